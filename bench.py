@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the teuk-kokkos RK4 hot path on B200.
+
+Workload (one "step" = one classical RK4 step of every solve in a batch):
+plain FP64 linear Kerr ringdown, a = 0.7, M = 1, L = 1, nr = 1025, SBP
+D10-5, m = -4..4, ell <= 16 (ntheta = 25), seeded Gaussian pulses in
+ell = 2, m = +-2 (centre 8M, width 0.8M, amplitude 1e-3) plus seeded
+1e-6 band-projected noise, CFL 0.25.  Each GPU advances a batch of
+``--batch`` such solves (weak scaling: per-GPU work fixed as N grows, no
+collective on the data path).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0).  ``value`` is whole-job grid-point updates/s
+(steps * modes * nr * ntheta per solve, the reference's metric) from CUDA
+events on the engine's stream, max over ranks; ``e2e`` is the same metric
+through the C ABI with host buffers (initial-state upload from pinned host
+memory and a per-step device->host read of every solve's endpoint waveform
+inside the timed region).  ``--impl reference`` times the reference's own
+CPU implementation (teuk-kokkos headers built against the Kokkos-API host
+shim, all host threads) on one solve of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "teuk-kokkos_b200"))
+
+METRIC = ("grid-point updates/s, p99 latency: batched split-prec vs plain "
+          "FP64 @<=1e-9 err")
+UNIT = "grid-point updates/s"
+FALLBACK_HBM_GBS = 6650.0
+PASSES_PER_STEP = 14  # compulsory modal passes of the fused stage schedule
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse_args():
+    p = argparse.ArgumentParser(description=__doc__,
+                                formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--batch", type=int, default=64,
+                   help="solves per GPU (default 64: 405 MB of state, > L2)")
+    p.add_argument("--cpu-seconds", type=float, default=15.0,
+                   help="target length of the CPU-baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def workload_config(batch: int):
+    from teuk_b200 import workloads as wl
+    config, pulse, dt = wl.kerr_ringdown()
+    return {
+        "workload": "kerr_ringdown a=0.7 M=1 L=1 nr=1025 d10-5 m=-4..4 "
+                    "ell<=16 ntheta=25 cfl=0.25",
+        "solves_per_gpu": batch,
+        "dt": dt,
+        "dissipation": config.dissipation,
+        "grid_points_per_solve": wl.grid_points(config),
+        "storage": "band (modal) coefficients, complex128",
+        "l2": f"inputs larger than L2: {batch} solves x "
+              f"{wl.modal_values(config) * 16 / 1e6:.1f} MB state per buffer",
+    }, config, pulse, dt
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_id: str | None):
+        self.samples = []
+        self.proc = None
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}",
+               "--format=csv,noheader,nounits", "-lms", "200"]
+        if device_id:
+            cmd += ["-i", device_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        sm_max = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for name, flag in zip(names, s[5:9]):
+                if flag.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(sm_max) if sm_max else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def device_uuid(torch, device: int):
+    try:
+        uuid = str(torch.cuda.get_device_properties(device).uuid)
+        return uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+    except Exception:
+        return None
+
+
+def measured_hbm_peak():
+    path = REPO / "MEASURED_PEAKS.json"
+    try:
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def recorded_traffic(algorithmic_bytes_per_launch: float):
+    """DRAM bytes per stage launch from the committed ncu summary, scaled
+    to this launch by the units processed."""
+    path = REPO / "profiles" / "stage_kernel_traffic.json"
+    try:
+        data = json.loads(path.read_text())
+        per_unit = data["dram_bytes_per_launch"] / data["algorithmic_bytes_per_launch"]
+        return per_unit * algorithmic_bytes_per_launch
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------- CPU side
+def cpu_reference_run(config, pulse, dt, seconds: float, warmup: int = 1,
+                      steps: int | None = None):
+    """Reference implementation on the host (oracle/_ref, all threads), else
+    the C restatement (port).  Returns (grid-point updates/s, description)."""
+    sys.path.insert(0, str(REPO / "tests"))
+    import oracle_bindings as ob
+    from teuk_b200 import workloads as wl
+
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("TEUK_SHIM_NUM_THREADS", str(threads))
+    if ob.ref_available(threads=True):
+        pipe = ob.RefPipeline(config, threads=True)
+        pipe.initialize_gaussian(pulse)
+        kind, cores = "reference", int(os.environ["TEUK_SHIM_NUM_THREADS"])
+    else:
+        import teuk_b200 as tb
+        pipe = ob.OraclePipeline(config)
+        state = np.zeros(config.shape(), dtype=np.complex128)
+        pipe.set_state(state + wl.band_noise(config, 1, 1e-3))
+        kind, cores = "port", 1
+    pipe.step(0.0, dt, warmup)
+    if steps is None:
+        t0 = time.perf_counter()
+        pipe.step(0.0, dt, 1)
+        one = time.perf_counter() - t0
+        steps = max(1, min(1000, int(seconds / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    pipe.step(0.0, dt, steps)
+    elapsed = time.perf_counter() - t0
+    value = wl.grid_points(config) * steps / elapsed
+    return value, {"kind": kind, "cores": cores,
+                   "sample": f"{steps} RK4 steps of one solve of the same "
+                             f"workload ({wl.grid_points(config)} grid points)",
+                   "seconds": elapsed, "steps": steps}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    meta, config, pulse, dt = workload_config(args.batch)
+    # Each reference "step" is one RK4 step of one solve (bounded sample).
+    value, info = cpu_reference_run(config, pulse, dt, 0.0,
+                                    warmup=args.warmup, steps=args.steps)
+    meta = dict(meta)
+    meta["solves_per_gpu"] = 1
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * info["seconds"] / info["steps"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded Gaussian pulses)",
+        "config": meta, "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["cores"],
+                         "kind": info["kind"], "sample": info["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU side
+def build_batch(tb, wl, config, pulse, batch_size, seed0, pinned):
+    """A batch of `batch_size` copies of the workload with seeded amplitudes
+    and noise.  Initial states are linear combinations of two unit-amplitude
+    Gaussian states (the system is linear) plus the seeded noise; they are
+    written into the pinned host tensor `pinned` (batch, *shape)."""
+    import torch
+    probe = tb.Pipeline(config)
+    units = []
+    for m in (2, -2):
+        probe.initialize_gaussian(tb.GaussianPulse(center=pulse.center,
+                                                   width=pulse.width,
+                                                   modes=[(2, m, 1.0)]))
+        units.append(probe.get_state())
+    probe.close()
+    batch = tb.Batch([config] * batch_size)
+    rng = np.random.Generator(np.random.PCG64(seed0))
+    for i in range(batch_size):
+        a = 1e-3 * complex(rng.standard_normal(), rng.standard_normal())
+        b = 1e-3 * complex(rng.standard_normal(), rng.standard_normal())
+        state = a * units[0] + b * units[1] + wl.band_noise(config, seed0 + i)
+        pinned[i].copy_(torch.from_numpy(state))
+        batch.set_state(i, pinned[i])
+    return batch
+
+
+def b200_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    import teuk_b200 as tb
+    from teuk_b200 import workloads as wl
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    meta, config, pulse, dt = workload_config(args.batch)
+    shape = config.shape()
+    B = args.batch
+    pinned = torch.empty((B, *shape), dtype=torch.complex128, pin_memory=True)
+    batch = build_batch(tb, wl, config, pulse, B, 1000 * (rank + 1), pinned)
+    stream = torch.cuda.Stream()
+    batch.set_stream(stream.cuda_stream)
+    dts = [dt] * B
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # warm-up (graph capture happens here)
+    batch.step(dts, steps=max(args.warmup, 0), graph=True)
+    batch.synchronize()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(device_uuid(torch, local))
+    barrier()
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    batch.step(dts, steps=args.steps, graph=True)
+    end.record(stream)
+    end.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    ms = start.elapsed_time(end)
+    elapsed = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(elapsed, op=dist.ReduceOp.MAX)
+    ms_max = float(elapsed.item())
+    gp = wl.grid_points(config)
+    value = world * B * gp * args.steps / (ms_max / 1e3)
+    launches_per_step = batch.launches_per_step()
+
+    # roofline of the stage kernel (four launches per RK4 step)
+    modal = wl.modal_values(config) * B
+    bytes_per_step = PASSES_PER_STEP * 16 * modal
+    launches = launches_per_step * args.steps
+    per_launch_s = (ms / 1e3) / launches
+    algorithmic_per_launch = bytes_per_step / launches_per_step
+    achieved = algorithmic_per_launch / per_launch_s / 1e9
+    peak, peak_kind = measured_hbm_peak()
+    traffic = recorded_traffic(algorithmic_per_launch)
+
+    # end-to-end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        n_end = batch.endpoint_modal_count()
+        waveform = torch.empty(n_end, dtype=torch.complex128, pin_memory=True)
+        barrier()
+        torch.cuda.synchronize()
+        e_start = torch.cuda.Event(enable_timing=True)
+        e_end = torch.cuda.Event(enable_timing=True)
+        e_start.record(stream)
+        for i in range(B):
+            batch.set_state(i, pinned[i])
+        for _ in range(args.steps):
+            batch.step(dts, steps=1, graph=True)
+            batch.endpoint_modal(waveform)
+        e_end.record(stream)
+        e_end.synchronize()
+        barrier()
+        e_ms = torch.tensor([e_start.elapsed_time(e_end)], dtype=torch.float64,
+                            device="cuda")
+        if world > 1:
+            dist.all_reduce(e_ms, op=dist.ReduceOp.MAX)
+        e_ms = float(e_ms.item())
+        state_bytes = wl.state_bytes(config) * B
+        e2e = {"value": world * B * gp * args.steps / (e_ms / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": (state_bytes + 8 * B) / args.steps,
+               "d2h_bytes_per_step": 16 * n_end,
+               "ms_per_step": e_ms / args.steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        value_cpu, info = cpu_reference_run(config, pulse, dt, args.cpu_seconds)
+        cpu = {"value": value_cpu, "unit": UNIT, "cores": info["cores"],
+               "kind": info["kind"], "sample": info["sample"]}
+
+    if rank == 0:
+        meta = dict(meta)
+        meta["parallelism"] = f"{world} GPU x {B} independent solves (no collective)"
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Gaussian pulses + band noise)",
+            "config": meta,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic,
+                         "kernel": "stage_kernel<D10-5, free-damped>",
+                         "peak_source": f"{peak_kind} hbm_gbs",
+                         "algorithmic_bytes_per_launch": algorithmic_per_launch},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    batch.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        b200_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,258 @@
+/*
+ * teuk_b200.h -- C ABI of the B200 (sm_100a) engine for the teuk-kokkos RK4
+ * right-hand-side hot path: the spin -2 Teukolsky spatial pipeline
+ * (SBP radial operators, fixed-m spin-weighted-harmonic transforms with the
+ * implicit Kerr ell-coupling, band projection) and its classical RK4 stage
+ * update.
+ *
+ * Every entry point replaces one member of the reference's C++ interface:
+ *
+ *   teuk_b200_create            SpatialPipeline::SpatialPipeline
+ *                               (include/teuk/spatial_pipeline.hpp:163-363)
+ *   teuk_b200_destroy           ~SpatialPipeline
+ *   teuk_b200_shape             SpatialPipelineStorage::snapshot_shape
+ *                               (include/teuk/pipeline_storage.hpp:114-117)
+ *   teuk_b200_set_state         Kokkos::deep_copy into storage().state()
+ *                               (include/teuk/pipeline_bands.hpp:215-231)
+ *   teuk_b200_get_state         deep_copy out of storage().state()
+ *                               (include/teuk/pipeline_checkpoint.hpp:820-830)
+ *   teuk_b200_evaluate_rhs      SpatialPipeline::evaluate_rhs_at_time
+ *                               (include/teuk/spatial_pipeline.hpp:458-588)
+ *   teuk_b200_step              SpatialPipeline::step, repeated
+ *                               (include/teuk/spatial_pipeline.hpp:590-620;
+ *                               include/teuk/device_rk4.hpp:84-128)
+ *   teuk_b200_initialize_gaussian
+ *                               initialize_compactified_gaussian_pulse
+ *                               (include/teuk/pipeline_initial_data.hpp:211-339)
+ *   teuk_b200_sample_endpoint   EndpointWaveformSampler::sample
+ *                               (include/teuk/waveform_output.hpp:75-160)
+ *   teuk_b200_get_activation / teuk_b200_restore_activation /
+ *   teuk_b200_reset_activation  SpatialPipeline::source_activation_state /
+ *                               restore_source_activation /
+ *                               reset_source_activation
+ *                               (include/teuk/spatial_pipeline.hpp:386-420)
+ *   teuk_b200_last_error        the std::invalid_argument / runtime_error
+ *                               message the reference would throw
+ *
+ * Batched variants (teuk_b200_batch_*) pack many independent solves of
+ * uneven shape into one set of stage launches; they have no single
+ * counterpart in the reference, whose driver runs one pipeline per process
+ * (include/teuk/solver_driver.hpp:86-353).
+ *
+ * Conventions.  State arrays are complex128 stored as interleaved
+ * (real, imag) doubles in the reference's (mode, field, radial, theta)
+ * order with theta contiguous and 13 fields (include/teuk/fields.hpp:27-28,
+ * include/teuk/pipeline_storage.hpp:18-33).  A `memory` argument says
+ * whether a pointer is host (TEUK_B200_HOST) or CUDA device
+ * (TEUK_B200_DEVICE) memory.  Every call returns TEUK_B200_OK or a negative
+ * status; teuk_b200_last_error() then holds the message (thread-local).
+ * No call falls back to a CPU implementation: when the CUDA kernels cannot
+ * run, create fails with TEUK_B200_ERR_CUDA.
+ */
+#ifndef TEUK_B200_H
+#define TEUK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TEUK_B200_ABI_VERSION 1
+
+enum teuk_b200_status {
+  TEUK_B200_OK = 0,
+  TEUK_B200_ERR_INVALID_ARGUMENT = -1, /* std::invalid_argument */
+  TEUK_B200_ERR_RUNTIME = -2,          /* std::runtime_error */
+  TEUK_B200_ERR_CUDA = -3,             /* CUDA launch / allocation failure */
+  TEUK_B200_ERR_UNSUPPORTED = -4,      /* valid reference input not yet
+                                          built on the B200 path */
+  TEUK_B200_ERR_OUT_OF_MEMORY = -5
+};
+
+enum teuk_b200_memory { TEUK_B200_HOST = 0, TEUK_B200_DEVICE = 1 };
+
+/* include/teuk/radial_discretization.hpp:17 */
+enum teuk_b200_discretization {
+  TEUK_B200_D42 = 0,
+  TEUK_B200_D84 = 1,
+  TEUK_B200_D105 = 2
+};
+
+/* include/teuk/teukolsky.hpp:148-151 */
+enum teuk_b200_reduction {
+  TEUK_B200_FREE_DAMPED = 0,
+  TEUK_B200_STAGE_CONSTRAINED = 1
+};
+
+/* include/teuk/spatial_pipeline.hpp:40-53 */
+enum teuk_b200_source_mode {
+  TEUK_B200_SOURCE_DISABLED = 0,
+  TEUK_B200_SOURCE_CONSTRAINT_AWARE = 1,
+  TEUK_B200_SOURCE_UNRESTRICTED = 2
+};
+
+/* Field slots of the 13-field state (include/teuk/pipeline_storage.hpp:18-33) */
+enum teuk_b200_field {
+  TEUK_B200_FIRST_P = 0,
+  TEUK_B200_FIRST_Q = 1,
+  TEUK_B200_FIRST_PSI = 2,
+  TEUK_B200_FIELD_COUNT = 13
+};
+
+enum teuk_b200_boundary { TEUK_B200_SCRI = 0, TEUK_B200_HORIZON = 1 };
+
+/* Constructor arguments of SpatialPipeline plus the ModeRegistry lists
+ * (include/teuk/modes.hpp:42-80).  Mode lists may be given in any order;
+ * they are sorted and checked exactly like ModeRegistry does. */
+typedef struct teuk_b200_config {
+  int abi_version; /* TEUK_B200_ABI_VERSION */
+  double mass;
+  double spin;
+  double compactification_length;
+  int radial_points;  /* nr: uniform grid on [0, L^2 / r_+] */
+  int theta_nodes;    /* Gauss-Legendre nodes */
+  int ell_max_first;  /* PipelineAngularBands::ell_max_first */
+  int ell_max_second; /* PipelineAngularBands::ell_max_second */
+  int mode_count;
+  const int* modes;   /* stored signed m */
+  int parent_count;
+  const int* parents; /* first-order modes */
+  int target_count;
+  const int* targets; /* second-order modes */
+  double reduction_damping;
+  double dissipation;
+  int reduction;      /* enum teuk_b200_reduction */
+  int discretization; /* enum teuk_b200_discretization */
+  int source_mode;    /* enum teuk_b200_source_mode */
+  double source_start_time;
+  double normalized_constraint_tolerance;
+  int required_consecutive_passes;
+} teuk_b200_config;
+
+/* SourceActivationState (include/teuk/source_activation.hpp) */
+typedef struct teuk_b200_activation {
+  int active;
+  double activation_time;
+  int consecutive_passes;
+  double last_eligibility_time;
+} teuk_b200_activation;
+
+/* GaussianPulseMode / PipelineGaussianPulse
+ * (include/teuk/pipeline_initial_data.hpp:24-57).  center and width are
+ * compactified radii (not fractions of R_H). */
+typedef struct teuk_b200_gaussian_mode {
+  int ell;
+  int m;
+  double amplitude_real;
+  double amplitude_imag;
+} teuk_b200_gaussian_mode;
+
+typedef struct teuk_b200_gaussian {
+  double center;
+  double width;
+  int compact_support;
+  int mode_count;
+  const teuk_b200_gaussian_mode* modes;
+} teuk_b200_gaussian;
+
+/* One endpoint waveform record (include/teuk/waveform_output.hpp:23-32). */
+typedef struct teuk_b200_waveform_record {
+  int boundary; /* enum teuk_b200_boundary */
+  int order;    /* 1 = first-order field, 2 = second-order field */
+  int m;
+  int ell;
+  double rescaled_real;
+  double rescaled_imag;
+  double endpoint_real;
+  double endpoint_imag;
+} teuk_b200_waveform_record;
+
+typedef struct teuk_b200_pipeline teuk_b200_pipeline;
+typedef struct teuk_b200_batch teuk_b200_batch;
+
+const char* teuk_b200_last_error(void);
+int teuk_b200_abi_version(void);
+
+/* ---- single pipeline (one solve) ------------------------------------- */
+int teuk_b200_create(const teuk_b200_config* config,
+                     teuk_b200_pipeline** out);
+int teuk_b200_destroy(teuk_b200_pipeline* pipeline);
+/* shape[4] = {modes, 13, radial, theta} */
+int teuk_b200_shape(const teuk_b200_pipeline* pipeline, size_t shape[4]);
+/* Values count = modes*13*radial*theta complex numbers. */
+int teuk_b200_set_state(teuk_b200_pipeline* pipeline, const double* state,
+                        size_t complex_count, int memory);
+int teuk_b200_get_state(teuk_b200_pipeline* pipeline, double* state,
+                        size_t complex_count, int memory);
+/* RHS of a caller-supplied stage (same layout).  Stage fields that lie
+ * outside the retained fixed-m bands are projected onto them first; every
+ * stage the pipeline itself produces is already in band. */
+int teuk_b200_evaluate_rhs(teuk_b200_pipeline* pipeline, const double* stage,
+                           double* output, size_t complex_count, double time,
+                           int memory);
+/* Advance `steps` classical RK4 steps of size dt from `time`. */
+int teuk_b200_step(teuk_b200_pipeline* pipeline, double time, double dt,
+                   int steps);
+int teuk_b200_initialize_gaussian(teuk_b200_pipeline* pipeline,
+                                  const teuk_b200_gaussian* pulse);
+/* Records for the scri then horizon endpoints of the first-order field and
+ * then the second-order field, in the reference's order.  `capacity` is the
+ * number of records `out` can hold; `count` receives the number written. */
+int teuk_b200_sample_endpoint(teuk_b200_pipeline* pipeline,
+                              teuk_b200_waveform_record* out,
+                              size_t capacity, size_t* count);
+int teuk_b200_get_activation(const teuk_b200_pipeline* pipeline,
+                             teuk_b200_activation* out);
+int teuk_b200_restore_activation(teuk_b200_pipeline* pipeline,
+                                 const teuk_b200_activation* state);
+int teuk_b200_reset_activation(teuk_b200_pipeline* pipeline);
+/* Bind the pipeline's launches to a caller cudaStream_t (NULL = the
+ * pipeline's own stream). */
+int teuk_b200_set_stream(teuk_b200_pipeline* pipeline, void* cuda_stream);
+int teuk_b200_synchronize(teuk_b200_pipeline* pipeline);
+/* Device bytes held by one pipeline built from `config` (admission). */
+int teuk_b200_footprint_bytes(const teuk_b200_config* config,
+                              size_t* bytes);
+
+/* ---- batched solves: one set of stage launches for all instances ----- */
+int teuk_b200_batch_create(const teuk_b200_config* configs, int count,
+                           teuk_b200_batch** out);
+int teuk_b200_batch_destroy(teuk_b200_batch* batch);
+int teuk_b200_batch_size(const teuk_b200_batch* batch, int* count);
+int teuk_b200_batch_shape(const teuk_b200_batch* batch, int instance,
+                          size_t shape[4]);
+int teuk_b200_batch_set_state(teuk_b200_batch* batch, int instance,
+                              const double* state, size_t complex_count,
+                              int memory);
+int teuk_b200_batch_get_state(teuk_b200_batch* batch, int instance,
+                              double* state, size_t complex_count,
+                              int memory);
+int teuk_b200_batch_initialize_gaussian(teuk_b200_batch* batch, int instance,
+                                        const teuk_b200_gaussian* pulse);
+/* One RK4 step of size dt[i] for every instance i, `steps` times.  With
+ * graph != 0 the four stage launches of a step are replayed from a
+ * captured CUDA graph. */
+int teuk_b200_batch_step(teuk_b200_batch* batch, const double* dt, int steps,
+                         int graph);
+int teuk_b200_batch_sample_endpoint(teuk_b200_batch* batch, int instance,
+                                    teuk_b200_waveform_record* out,
+                                    size_t capacity, size_t* count);
+/* Per-instance endpoint Psi modal coefficients gathered on the device for
+ * every instance at once: (instance, boundary, mode, ell) complex values in
+ * the batch's packed order; `count` receives the complex count. */
+int teuk_b200_batch_endpoint_modal(teuk_b200_batch* batch, double* out,
+                                   size_t capacity, size_t* count,
+                                   int memory);
+int teuk_b200_batch_set_stream(teuk_b200_batch* batch, void* cuda_stream);
+int teuk_b200_batch_synchronize(teuk_b200_batch* batch);
+/* Kernel launches issued per RK4 step (for launch accounting). */
+int teuk_b200_batch_launches_per_step(const teuk_b200_batch* batch,
+                                      int* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TEUK_B200_H */

@@ -1,0 +1,338 @@
+// Reference-side C ABI: test infrastructure, never linked into the product.
+//
+// Wraps the unmodified teuk-kokkos headers (compiled against the Kokkos-API
+// host shim in oracle/kokkos_shim) behind the same entry points that
+// include/teuk_b200.h declares for the B200 engine, with a teuk_ref_ prefix.
+// Tests and the CPU baseline of bench.py call both libraries with identical
+// arguments. Built by oracle/Makefile into oracle/_ref/libteuk_ref*.so; it
+// needs the reference include tree only at build time.
+#include <Kokkos_Core.hpp>
+
+#include <algorithm>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "teuk/diagnostics.hpp"
+#include "teuk/pipeline_bands.hpp"
+#include "teuk/pipeline_initial_data.hpp"
+#include "teuk/spatial_pipeline.hpp"
+#include "teuk/waveform_output.hpp"
+#include "teuk_b200.h"
+
+namespace {
+
+thread_local std::string last_error;
+
+int fail(const int code, const std::string& message) {
+  last_error = message;
+  return code;
+}
+
+template <class Body>
+int guarded(Body&& body) {
+  try {
+    body();
+    return TEUK_B200_OK;
+  } catch (const std::invalid_argument& error) {
+    return fail(TEUK_B200_ERR_INVALID_ARGUMENT, error.what());
+  } catch (const std::out_of_range& error) {
+    return fail(TEUK_B200_ERR_INVALID_ARGUMENT, error.what());
+  } catch (const std::exception& error) {
+    return fail(TEUK_B200_ERR_RUNTIME, error.what());
+  }
+}
+
+std::vector<int> list(const int* values, const int count) {
+  if (count < 0 || (count > 0 && values == nullptr)) {
+    throw std::invalid_argument("mode list pointer/count mismatch");
+  }
+  return std::vector<int>(values, values + count);
+}
+
+teuk::RadialDiscretization discretization(const int value) {
+  switch (value) {
+    case TEUK_B200_D42: return teuk::RadialDiscretization::D42;
+    case TEUK_B200_D84: return teuk::RadialDiscretization::D84;
+    case TEUK_B200_D105: return teuk::RadialDiscretization::D105;
+  }
+  throw std::invalid_argument("unknown radial discretization");
+}
+
+teuk::SecondOrderSourcePolicy policy(const teuk_b200_config& c) {
+  switch (c.source_mode) {
+    case TEUK_B200_SOURCE_DISABLED:
+      return teuk::SecondOrderSourcePolicy::disabled();
+    case TEUK_B200_SOURCE_CONSTRAINT_AWARE:
+      return {teuk::SecondOrderSourceMode::ConstraintAware,
+              c.source_start_time, c.normalized_constraint_tolerance,
+              c.required_consecutive_passes};
+    case TEUK_B200_SOURCE_UNRESTRICTED:
+      return {teuk::SecondOrderSourceMode::Unrestricted, c.source_start_time,
+              c.normalized_constraint_tolerance,
+              c.required_consecutive_passes};
+  }
+  throw std::invalid_argument("unknown source mode");
+}
+
+}  // namespace
+
+struct teuk_ref_pipeline {
+  explicit teuk_ref_pipeline(const teuk_b200_config& c)
+      : registry(list(c.modes, c.mode_count), list(c.parents, c.parent_count),
+                 list(c.targets, c.target_count)),
+        horizon(c.compactification_length * c.compactification_length /
+                teuk::outer_horizon_radius(c.mass, c.spin)),
+        pipeline(execution, registry,
+                 teuk::UniformRadialGrid(
+                     static_cast<std::size_t>(c.radial_points), 0.0, horizon),
+                 teuk::PipelineAngularBands{c.ell_max_first, c.ell_max_second},
+                 c.theta_nodes,
+                 teuk::KerrParameters{c.mass, c.spin,
+                                      c.compactification_length},
+                 c.reduction_damping, c.dissipation,
+                 c.reduction == TEUK_B200_STAGE_CONSTRAINED
+                     ? teuk::ReductionEvolution::StageConstrained
+                     : teuk::ReductionEvolution::FreeDamped,
+                 "ref_pipeline", policy(c), discretization(c.discretization)),
+        sampler(registry, {c.ell_max_first, c.ell_max_second}, c.theta_nodes,
+                c.compactification_length, horizon),
+        ell_max_first(c.ell_max_first),
+        background{c.mass, c.spin, c.compactification_length},
+        scratch("ref_scratch_state", registry.size(),
+                teuk::point_pipeline_field_count,
+                static_cast<std::size_t>(c.radial_points),
+                static_cast<std::size_t>(c.theta_nodes)),
+        scratch_out("ref_scratch_rhs", registry.size(),
+                    teuk::point_pipeline_field_count,
+                    static_cast<std::size_t>(c.radial_points),
+                    static_cast<std::size_t>(c.theta_nodes)) {}
+
+  teuk::ExecutionSpace execution;
+  teuk::ModeRegistry registry;
+  double horizon;
+  teuk::SpatialPipeline pipeline;
+  teuk::EndpointWaveformSampler sampler;
+  int ell_max_first;
+  teuk::KerrParameters background;
+  teuk::FieldView scratch;
+  teuk::FieldView scratch_out;
+};
+
+namespace {
+
+std::size_t value_count(const teuk_ref_pipeline& p) {
+  return p.pipeline.storage().value_count();
+}
+
+void check_count(const teuk_ref_pipeline& p, const std::size_t count) {
+  if (count != value_count(p)) {
+    throw std::invalid_argument("state complex count does not match shape");
+  }
+}
+
+void copy_in(const teuk::FieldView& view, const double* values) {
+  auto* data = view.data();
+  for (std::size_t i = 0; i < view.size(); ++i) {
+    data[i] = teuk::Complex(values[2 * i], values[2 * i + 1]);
+  }
+}
+
+void copy_out(const teuk::FieldView& view, double* values) {
+  const auto* data = view.data();
+  for (std::size_t i = 0; i < view.size(); ++i) {
+    values[2 * i] = data[i].real();
+    values[2 * i + 1] = data[i].imag();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* teuk_ref_last_error(void) { return last_error.c_str(); }
+
+const char* teuk_ref_backend(void) {
+  return teuk::ExecutionSpace::name();
+}
+
+int teuk_ref_create(const teuk_b200_config* config, teuk_ref_pipeline** out) {
+  if (config == nullptr || out == nullptr) {
+    return fail(TEUK_B200_ERR_INVALID_ARGUMENT, "null argument");
+  }
+  return guarded([&] { *out = new teuk_ref_pipeline(*config); });
+}
+
+int teuk_ref_destroy(teuk_ref_pipeline* p) {
+  delete p;
+  return TEUK_B200_OK;
+}
+
+int teuk_ref_shape(const teuk_ref_pipeline* p, size_t shape[4]) {
+  const auto s = p->pipeline.storage().snapshot_shape();
+  shape[0] = s.modes;
+  shape[1] = s.fields;
+  shape[2] = s.radial;
+  shape[3] = s.theta;
+  return TEUK_B200_OK;
+}
+
+int teuk_ref_set_state(teuk_ref_pipeline* p, const double* state,
+                       size_t count, int) {
+  return guarded([&] {
+    check_count(*p, count);
+    copy_in(p->pipeline.storage().state(), state);
+  });
+}
+
+int teuk_ref_get_state(teuk_ref_pipeline* p, double* state, size_t count,
+                       int) {
+  return guarded([&] {
+    check_count(*p, count);
+    copy_out(p->pipeline.storage().state(), state);
+  });
+}
+
+int teuk_ref_evaluate_rhs(teuk_ref_pipeline* p, const double* stage,
+                          double* output, size_t count, double time, int) {
+  return guarded([&] {
+    check_count(*p, count);
+    copy_in(p->scratch, stage);
+    p->pipeline.evaluate_rhs_at_time(p->execution, p->scratch,
+                                     p->scratch_out, time);
+    copy_out(p->scratch_out, output);
+  });
+}
+
+int teuk_ref_step(teuk_ref_pipeline* p, double time, double dt, int steps) {
+  return guarded([&] {
+    for (int i = 0; i < steps; ++i) {
+      p->pipeline.step(p->execution, time, dt);
+      time += dt;
+    }
+  });
+}
+
+int teuk_ref_initialize_gaussian(teuk_ref_pipeline* p,
+                                 const teuk_b200_gaussian* pulse) {
+  return guarded([&] {
+    teuk::PipelineGaussianPulse gaussian;
+    gaussian.center = pulse->center;
+    gaussian.width = pulse->width;
+    gaussian.compact_support = pulse->compact_support != 0;
+    for (int i = 0; i < pulse->mode_count; ++i) {
+      gaussian.modes.push_back(
+          {pulse->modes[i].ell, pulse->modes[i].m,
+           teuk::Complex(pulse->modes[i].amplitude_real,
+                         pulse->modes[i].amplitude_imag)});
+    }
+    teuk::initialize_compactified_gaussian_pulse(
+        p->execution, p->pipeline, p->registry, p->ell_max_first,
+        p->background, gaussian);
+  });
+}
+
+int teuk_ref_sample_endpoint(teuk_ref_pipeline* p,
+                             teuk_b200_waveform_record* out, size_t capacity,
+                             size_t* count) {
+  return guarded([&] {
+    const auto records =
+        p->sampler.sample(p->execution, p->pipeline.storage().state(), 0, 0.0);
+    if (records.size() > capacity) {
+      throw std::invalid_argument("waveform record capacity is too small");
+    }
+    for (std::size_t i = 0; i < records.size(); ++i) {
+      out[i].boundary = records[i].boundary == teuk::WaveformBoundary::Scri
+                            ? TEUK_B200_SCRI
+                            : TEUK_B200_HORIZON;
+      out[i].order = records[i].perturbative_order;
+      out[i].m = records[i].m;
+      out[i].ell = records[i].ell;
+      out[i].rescaled_real = records[i].rescaled.real();
+      out[i].rescaled_imag = records[i].rescaled.imag();
+      out[i].endpoint_real = records[i].endpoint_waveform.real();
+      out[i].endpoint_imag = records[i].endpoint_waveform.imag();
+    }
+    *count = records.size();
+  });
+}
+
+int teuk_ref_get_activation(const teuk_ref_pipeline* p,
+                            teuk_b200_activation* out) {
+  const auto s = p->pipeline.source_activation_state();
+  out->active = s.active ? 1 : 0;
+  out->activation_time = s.activation_time;
+  out->consecutive_passes = s.consecutive_passes;
+  out->last_eligibility_time = s.last_eligibility_time;
+  return TEUK_B200_OK;
+}
+
+// Project a (modes,13,radial,theta) host state onto the retained bands with
+// the reference's own routine (include/teuk/pipeline_bands.hpp).
+int teuk_ref_project_to_bands(teuk_ref_pipeline* p, double* state,
+                              size_t count) {
+  return guarded([&] {
+    check_count(*p, count);
+    copy_in(p->scratch, state);
+    teuk::project_pipeline_state_to_retained_bands(
+        p->scratch, p->registry, p->pipeline.angular_bands());
+    copy_out(p->scratch, state);
+  });
+}
+
+// Gauss-Legendre nodes / weights and one fixed-(s,m) synthesis and analysis
+// matrix pair exactly as the reference builds them
+// (include/teuk/angular.hpp:69-115,329-355), for KAT tests of the product's
+// host-side plan builder.
+int teuk_ref_gauss_legendre(int nodes, double* x, double* weights) {
+  return guarded([&] {
+    const auto grid = teuk::angular::gauss_legendre(nodes);
+    for (int i = 0; i < nodes; ++i) {
+      x[i] = grid.x[static_cast<std::size_t>(i)];
+      weights[i] = grid.weights[static_cast<std::size_t>(i)];
+    }
+  });
+}
+
+int teuk_ref_transform_matrices(int spin, int m, int ell_max, int nodes,
+                                double* synthesis, double* analysis,
+                                int* mode_count) {
+  return guarded([&] {
+    const teuk::angular::SpinWeightedTransform t(spin, m, ell_max, nodes);
+    const std::size_t modes = t.mode_count();
+    for (std::size_t j = 0; j < static_cast<std::size_t>(nodes); ++j) {
+      for (std::size_t l = 0; l < modes; ++l) {
+        synthesis[j * modes + l] = t.synthesis_matrix()(j, l);
+        analysis[l * static_cast<std::size_t>(nodes) + j] =
+            t.analysis_matrix()(l, j);
+      }
+    }
+    *mode_count = static_cast<int>(modes);
+  });
+}
+
+// Dense SBP first-derivative matrix h*D and norm weights H/h for n points
+// (include/teuk/sbp.hpp, sbp84.hpp, sbp105.hpp).
+int teuk_ref_sbp_matrix(int disc, int n, double* derivative, double* norm) {
+  return guarded([&] {
+    const auto d = discretization(disc);
+    const std::size_t count = static_cast<std::size_t>(n);
+    std::vector<double> unit(count);
+    for (std::size_t column = 0; column < count; ++column) {
+      std::fill(unit.begin(), unit.end(), 0.0);
+      unit[column] = 1.0;
+      for (std::size_t row = 0; row < count; ++row) {
+        derivative[row * count + column] =
+            teuk::radial_first_derivative_at(d, unit.data(), count, row, 1.0);
+      }
+    }
+    for (std::size_t row = 0; row < count; ++row) {
+      norm[row] = teuk::radial_norm_weight(d, count, row);
+    }
+  });
+}
+
+}  // extern "C"

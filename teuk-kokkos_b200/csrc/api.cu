@@ -1,0 +1,1035 @@
+// C ABI of the B200 engine (include/teuk_b200.h).  A pipeline is a batch of
+// one solve; a batch packs many independent solves of uneven shape into the
+// same four stage launches per RK4 step.  Host code here validates, plans,
+// owns device memory and orders launches on one CUDA stream; it never
+// computes a right-hand side itself.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <exception>
+#include <limits>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <numbers>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "kernels.h"
+#include "teuk_b200.h"
+
+namespace teuk_b200 {
+namespace {
+
+thread_local std::string g_last_error;
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct Unsupported : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+void check(const cudaError_t err, const char* what) {
+  if (err != cudaSuccess) {
+    throw CudaError(std::string(what) + ": " + cudaGetErrorString(err));
+  }
+}
+
+template <class Body>
+int guarded(Body&& body) {
+  try {
+    body();
+    return TEUK_B200_OK;
+  } catch (const std::invalid_argument& e) {
+    g_last_error = e.what();
+    return TEUK_B200_ERR_INVALID_ARGUMENT;
+  } catch (const std::out_of_range& e) {
+    g_last_error = e.what();
+    return TEUK_B200_ERR_INVALID_ARGUMENT;
+  } catch (const Unsupported& e) {
+    g_last_error = e.what();
+    return TEUK_B200_ERR_UNSUPPORTED;
+  } catch (const CudaError& e) {
+    g_last_error = e.what();
+    return TEUK_B200_ERR_CUDA;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return TEUK_B200_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return TEUK_B200_ERR_RUNTIME;
+  }
+}
+
+Config to_config(const teuk_b200_config& c) {
+  if (c.abi_version != TEUK_B200_ABI_VERSION) {
+    throw std::invalid_argument("teuk_b200_config.abi_version mismatch");
+  }
+  const auto list = [](const int* values, const int count) {
+    if (count < 0 || (count > 0 && values == nullptr)) {
+      throw std::invalid_argument("mode list pointer/count mismatch");
+    }
+    return std::vector<int>(values, values + count);
+  };
+  Config out;
+  out.mass = c.mass;
+  out.spin = c.spin;
+  out.length = c.compactification_length;
+  out.nr = c.radial_points;
+  out.ntheta = c.theta_nodes;
+  out.ell_max_first = c.ell_max_first;
+  out.ell_max_second = c.ell_max_second;
+  out.modes = list(c.modes, c.mode_count);
+  out.parents = list(c.parents, c.parent_count);
+  out.targets = list(c.targets, c.target_count);
+  out.damping = c.reduction_damping;
+  out.dissipation = c.dissipation;
+  out.reduction = c.reduction;
+  out.disc = c.discretization;
+  out.source_mode = c.source_mode;
+  out.source_start_time = c.source_start_time;
+  out.constraint_tolerance = c.normalized_constraint_tolerance;
+  out.required_passes = c.required_consecutive_passes;
+  if (out.source_mode < 0 || out.source_mode > 2) {
+    throw std::invalid_argument("unsupported second-order source mode");
+  }
+  return out;
+}
+
+void ensure_constants_on_current_device() {
+  static std::mutex mutex;
+  static bool uploaded[128] = {};
+  int device = 0;
+  check(cudaGetDevice(&device), "cudaGetDevice");
+  std::lock_guard<std::mutex> lock(mutex);
+  if (device >= 0 && device < 128 && uploaded[device]) return;
+  check(upload_sbp_constants(build_sbp_constants()), "upload SBP constants");
+  if (device >= 0 && device < 128) uploaded[device] = true;
+}
+
+template <class T>
+struct DeviceArray {
+  T* ptr = nullptr;
+  size_t count = 0;
+  DeviceArray() = default;
+  DeviceArray(const DeviceArray&) = delete;
+  DeviceArray& operator=(const DeviceArray&) = delete;
+  DeviceArray(DeviceArray&& other) noexcept
+      : ptr(other.ptr), count(other.count) {
+    other.ptr = nullptr;
+    other.count = 0;
+  }
+  void allocate(const size_t n) {
+    release();
+    if (n == 0) return;
+    check(cudaMalloc(reinterpret_cast<void**>(&ptr), n * sizeof(T)),
+          "cudaMalloc");
+    count = n;
+  }
+  void release() {
+    if (ptr != nullptr) cudaFree(ptr);
+    ptr = nullptr;
+    count = 0;
+  }
+  ~DeviceArray() { release(); }
+};
+
+constexpr int kTargetTileRows = 64;
+constexpr size_t kSmemBudget = 200 * 1024;
+
+int slab_halo(const int disc, const int reduction) {
+  const DiscInfo info = disc_info(disc);
+  return reduction == 1 ? std::max(info.diss_order, 2 * info.interior_half)
+                        : info.diss_order;
+}
+
+}  // namespace
+
+struct Batch {
+  std::vector<InstancePlan> plans;
+  std::vector<std::vector<int>> instance_segments;  // segment ids
+  std::vector<InstanceDesc> h_inst;
+  std::vector<SegmentDesc> h_seg;
+  std::vector<int> seg_mode;  // registry index of each segment's mode
+  std::vector<TileDesc> h_tiles;
+  std::vector<double> h_mat;
+  std::vector<double> h_trig;
+  std::vector<StageLaunch> groups;  // one per (disc, reduction)
+  std::vector<int> group_first_tile;
+  size_t total_complex = 0;
+  int max_ell = 1;
+
+  DeviceArray<double2> y, kA, kB, acc;
+  DeviceArray<InstanceDesc> d_inst;
+  DeviceArray<SegmentDesc> d_seg;
+  DeviceArray<int> d_seg_mode;
+  DeviceArray<TileDesc> d_tiles;
+  DeviceArray<double> d_mat, d_trig;
+  DeviceArray<double2> d_nodal;     // one instance's nodal state
+  DeviceArray<double2> d_endpoint;  // gathered endpoint coefficients
+  DeviceArray<int> d_parent_mask;    // per instance, per registry mode
+  DeviceArray<int> d_flag;
+  std::vector<size_t> parent_mask_offset;
+  std::vector<DeviceArray<double2>> frozen_dev;  // per instance, or empty
+
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaStream_t graph_stream = nullptr;
+  bool dt_dirty = false;
+
+  ~Batch() {
+    if (graph_exec != nullptr) cudaGraphExecDestroy(graph_exec);
+    if (graph != nullptr) cudaGraphDestroy(graph);
+    if (own_stream != nullptr) cudaStreamDestroy(own_stream);
+  }
+
+  void build(const std::vector<Config>& configs) {
+    if (configs.empty()) {
+      throw std::invalid_argument("a batch needs at least one solve");
+    }
+    for (const Config& c : configs) {
+      if (c.source_mode != 0) {
+        throw Unsupported(
+            "second-order source policies are not built on the B200 path; "
+            "only the linear (disabled) pipeline runs here");
+      }
+      plans.push_back(build_instance_plan(c));
+    }
+    int device_count = 0;
+    check(cudaGetDeviceCount(&device_count), "cudaGetDeviceCount");
+    if (device_count <= 0) throw CudaError("no CUDA device is visible");
+    ensure_constants_on_current_device();
+
+    // Segments, matrices, trig tables.
+    long long offset = 0;
+    for (size_t i = 0; i < plans.size(); ++i) {
+      InstancePlan& plan = plans[i];
+      const Config& c = plan.config;
+      InstanceDesc d{};
+      d.mass = c.mass;
+      d.spin = c.spin;
+      d.length = c.length;
+      d.spacing = plan.spacing;
+      d.inv_spacing = 1.0 / plan.spacing;
+      d.damping = c.reduction == 0 ? c.damping : 0.0;
+      d.dissipation = c.dissipation;
+      d.dt = 0.0;
+      d.nr = c.nr;
+      d.ntheta = c.ntheta;
+      d.trig_offset = static_cast<int>(h_trig.size());
+      d.reduction = c.reduction;
+      d.disc = c.disc;
+      h_trig.insert(h_trig.end(), plan.sinv.begin(), plan.sinv.end());
+      h_trig.insert(h_trig.end(), plan.cosv.begin(), plan.cosv.end());
+      h_inst.push_back(d);
+      instance_segments.emplace_back();
+      for (ModePlan& mp : plan.modes) {
+        if (!mp.parent) continue;
+        SegmentDesc s{};
+        s.offset = offset;
+        s.instance = static_cast<int>(i);
+        s.m = mp.m;
+        s.n_ell = mp.n_ell;
+        s.ell_min = mp.ell_min;
+        s.row_stride = 3 * mp.n_ell;
+        s.mat_offset = static_cast<int>(h_mat.size());
+        const int ne = mp.n_ell, nt = c.ntheta;
+        // St[l][j] then At[j][l]
+        for (int l = 0; l < ne; ++l) {
+          for (int j = 0; j < nt; ++j) {
+            h_mat.push_back(mp.synthesis[static_cast<size_t>(j) * ne + l]);
+          }
+        }
+        for (int j = 0; j < nt; ++j) {
+          for (int l = 0; l < ne; ++l) {
+            h_mat.push_back(mp.analysis[static_cast<size_t>(l) * nt + j]);
+          }
+        }
+        mp.segment = static_cast<long long>(h_seg.size());
+        instance_segments.back().push_back(static_cast<int>(h_seg.size()));
+        h_seg.push_back(s);
+        seg_mode.push_back(mp.mode_index);
+        max_ell = std::max(max_ell, ne);
+        long long count = static_cast<long long>(c.nr) * 3 * ne;
+        count = (count + 15) / 16 * 16;  // 256-byte aligned segments
+        offset += count;
+      }
+    }
+    total_complex = static_cast<size_t>(offset);
+
+    // Radial tiles, grouped by (disc, reduction).
+    for (int disc = 0; disc < 3; ++disc) {
+      for (int red = 0; red < 2; ++red) {
+        StageLaunch g{};
+        g.disc = disc;
+        g.reduction = red;
+        const int first_tile = static_cast<int>(h_tiles.size());
+        const int H = slab_halo(disc, red);
+        const int HD = disc_info(disc).interior_half;
+        for (size_t s = 0; s < h_seg.size(); ++s) {
+          const InstanceDesc& in = h_inst[static_cast<size_t>(h_seg[s].instance)];
+          if (in.disc != disc || in.reduction != red) continue;
+          const int ne = h_seg[s].n_ell;
+          const int nr = in.nr;
+          int rows = std::min(kTargetTileRows, std::max(16, 1024 / ne));
+          int tiles = (nr + rows - 1) / rows;
+          tiles = std::max(1, std::min(tiles, nr / 16));
+          for (int t = 0; t < tiles; ++t) {
+            const int r0 = static_cast<int>(static_cast<long long>(nr) * t / tiles);
+            const int r1 =
+                static_cast<int>(static_cast<long long>(nr) * (t + 1) / tiles);
+            h_tiles.push_back({static_cast<int>(s), r0, r1, 0});
+            const int s0 = std::max(0, r0 - H), s1 = std::min(nr, r1 + H);
+            const int t0 = std::max(0, r0 - HD), t1 = std::min(nr, r1 + HD);
+            g.slab_capacity = std::max(g.slab_capacity, (s1 - s0) * 3 * ne);
+            g.dslab_capacity = std::max(g.dslab_capacity, (t1 - t0) * ne);
+            g.coef_rows = std::max(g.coef_rows, t1 - t0);
+          }
+          g.matrix_capacity =
+              std::max(g.matrix_capacity, ne * in.ntheta);
+          g.max_theta = std::max(g.max_theta, in.ntheta);
+          g.max_ell = std::max(g.max_ell, ne);
+        }
+        g.tile_count = static_cast<int>(h_tiles.size()) - first_tile;
+        if (g.tile_count > 0) {
+          if (stage_smem_bytes(g) > kSmemBudget) {
+            throw std::invalid_argument(
+                "solve shape exceeds the stage kernel's shared-memory tile");
+          }
+          groups.push_back(g);
+          group_first_tile.push_back(first_tile);
+        }
+      }
+    }
+
+    // Device allocations.
+    y.allocate(total_complex);
+    kA.allocate(total_complex);
+    kB.allocate(total_complex);
+    acc.allocate(total_complex);
+    check(cudaMemset(y.ptr, 0, total_complex * sizeof(double2)), "memset y");
+    d_inst.allocate(h_inst.size());
+    d_seg.allocate(h_seg.size());
+    d_seg_mode.allocate(seg_mode.size());
+    d_tiles.allocate(h_tiles.size());
+    d_mat.allocate(std::max<size_t>(h_mat.size(), 1));
+    d_trig.allocate(h_trig.size());
+    size_t nodal_max = 0;
+    for (const InstancePlan& plan : plans) {
+      nodal_max = std::max(nodal_max, plan.value_count());
+    }
+    d_nodal.allocate(nodal_max);
+    d_endpoint.allocate(std::max<size_t>(h_seg.size(), 1) * 2 *
+                        static_cast<size_t>(max_ell));
+    std::vector<int> mask;
+    for (const InstancePlan& plan : plans) {
+      parent_mask_offset.push_back(mask.size());
+      for (const ModePlan& mp : plan.modes) mask.push_back(mp.parent ? 1 : 0);
+    }
+    d_parent_mask.allocate(mask.size());
+    check(cudaMemcpy(d_parent_mask.ptr, mask.data(), mask.size() * sizeof(int),
+                     cudaMemcpyHostToDevice),
+          "upload parent mask");
+    d_flag.allocate(1);
+    frozen_dev.resize(plans.size());
+    check(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking),
+          "cudaStreamCreate");
+    stream = own_stream;
+    upload_descriptors();
+    check(cudaMemcpy(d_seg.ptr, h_seg.data(), h_seg.size() * sizeof(SegmentDesc),
+                     cudaMemcpyHostToDevice),
+          "upload segments");
+    check(cudaMemcpy(d_seg_mode.ptr, seg_mode.data(),
+                     seg_mode.size() * sizeof(int), cudaMemcpyHostToDevice),
+          "upload segment modes");
+    check(cudaMemcpy(d_tiles.ptr, h_tiles.data(),
+                     h_tiles.size() * sizeof(TileDesc), cudaMemcpyHostToDevice),
+          "upload tiles");
+    if (!h_mat.empty()) {
+      check(cudaMemcpy(d_mat.ptr, h_mat.data(), h_mat.size() * sizeof(double),
+                       cudaMemcpyHostToDevice),
+            "upload matrices");
+    }
+    check(cudaMemcpy(d_trig.ptr, h_trig.data(), h_trig.size() * sizeof(double),
+                     cudaMemcpyHostToDevice),
+          "upload trig");
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+      StageLaunch& g = groups[gi];
+      g.tiles = d_tiles.ptr + group_first_tile[gi];
+      g.instances = d_inst.ptr;
+      g.segments = d_seg.ptr;
+      g.matrices = d_mat.ptr;
+      g.trig = d_trig.ptr;
+      g.y = y.ptr;
+      g.kA = kA.ptr;
+      g.kB = kB.ptr;
+      g.acc = acc.ptr;
+    }
+  }
+
+  void upload_descriptors() {
+    check(cudaMemcpyAsync(d_inst.ptr, h_inst.data(),
+                          h_inst.size() * sizeof(InstanceDesc),
+                          cudaMemcpyHostToDevice, stream),
+          "upload instances");
+    dt_dirty = false;
+  }
+
+  void check_instance(const int instance) const {
+    if (instance < 0 || instance >= static_cast<int>(plans.size())) {
+      throw std::out_of_range("batch instance index is out of range");
+    }
+  }
+
+  ConvertLaunch convert(const int instance) {
+    const InstancePlan& plan = plans[static_cast<size_t>(instance)];
+    ConvertLaunch c{};
+    c.modal = y.ptr;
+    const auto& segs = instance_segments[static_cast<size_t>(instance)];
+    c.segments = d_seg.ptr + (segs.empty() ? 0 : segs.front());
+    c.segment_modes = d_seg_mode.ptr + (segs.empty() ? 0 : segs.front());
+    c.matrices = d_mat.ptr;
+    c.segment_count = static_cast<int>(segs.size());
+    c.nr = plan.config.nr;
+    c.ntheta = plan.config.ntheta;
+    c.mode_count = static_cast<int>(plan.config.modes.size());
+    c.max_ell = max_ell;
+    return c;
+  }
+
+  void set_state(const int instance, const double* state, const size_t count,
+                 const int memory) {
+    check_instance(instance);
+    InstancePlan& plan = plans[static_cast<size_t>(instance)];
+    if (count != plan.value_count()) {
+      throw std::invalid_argument("state complex count does not match shape");
+    }
+    if (state == nullptr) throw std::invalid_argument("null state pointer");
+    const size_t bytes = count * sizeof(double2);
+    const double2* source = nullptr;
+    if (memory == TEUK_B200_HOST) {
+      check(cudaMemcpyAsync(d_nodal.ptr, state, bytes, cudaMemcpyHostToDevice,
+                            stream),
+            "set_state upload");
+      source = d_nodal.ptr;
+    } else if (memory == TEUK_B200_DEVICE) {
+      source = reinterpret_cast<const double2*>(state);
+    } else {
+      throw std::invalid_argument("unknown memory kind");
+    }
+    // Frozen planes (every field of a non-parent mode, fields 3..12 of a
+    // parent) never change in the linear pipeline; a device copy is kept
+    // only when one of them is non-zero.
+    check(cudaMemsetAsync(d_flag.ptr, 0, sizeof(int), stream), "flag reset");
+    check(launch_frozen_scan(source,
+                             d_parent_mask.ptr + parent_mask_offset[static_cast<size_t>(instance)],
+                             static_cast<int>(plan.config.modes.size()),
+                             plan.config.nr * plan.config.ntheta, d_flag.ptr,
+                             stream),
+          "frozen scan");
+    ConvertLaunch c = convert(instance);
+    c.nodal_in = source;
+    check(launch_nodal_to_modal(c, stream), "nodal_to_modal");
+    int flag = 0;
+    check(cudaMemcpyAsync(&flag, d_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost,
+                          stream),
+          "flag read");
+    check(cudaStreamSynchronize(stream), "set_state");
+    auto& frozen = frozen_dev[static_cast<size_t>(instance)];
+    if (flag != 0) {
+      if (frozen.count != count) frozen.allocate(count);
+      check(cudaMemcpyAsync(frozen.ptr, source, bytes, cudaMemcpyDeviceToDevice,
+                            stream),
+            "frozen copy");
+      check(cudaStreamSynchronize(stream), "frozen copy");
+    } else {
+      frozen.release();
+    }
+  }
+
+  // Full nodal state of `instance` into d_nodal: frozen planes from the
+  // device copy (zero when none is kept), evolved fields synthesized from
+  // `modal`.
+  void assemble_nodal(const int instance, double2* modal, const bool zero_frozen) {
+    InstancePlan& plan = plans[static_cast<size_t>(instance)];
+    const size_t bytes = plan.value_count() * sizeof(double2);
+    const auto& frozen = frozen_dev[static_cast<size_t>(instance)];
+    if (zero_frozen || frozen.ptr == nullptr) {
+      check(cudaMemsetAsync(d_nodal.ptr, 0, bytes, stream), "zero nodal");
+    } else {
+      check(cudaMemcpyAsync(d_nodal.ptr, frozen.ptr, bytes,
+                            cudaMemcpyDeviceToDevice, stream),
+            "frozen restore");
+    }
+    ConvertLaunch c = convert(instance);
+    c.modal = modal;
+    c.nodal_out = d_nodal.ptr;
+    check(launch_modal_to_nodal(c, stream), "modal_to_nodal");
+  }
+
+  void get_state(const int instance, double* out, const size_t count,
+                 const int memory) {
+    check_instance(instance);
+    InstancePlan& plan = plans[static_cast<size_t>(instance)];
+    if (count != plan.value_count()) {
+      throw std::invalid_argument("state complex count does not match shape");
+    }
+    if (out == nullptr) throw std::invalid_argument("null state pointer");
+    assemble_nodal(instance, y.ptr, false);
+    const size_t bytes = count * sizeof(double2);
+    check(cudaMemcpyAsync(out, d_nodal.ptr, bytes,
+                          memory == TEUK_B200_HOST ? cudaMemcpyDeviceToHost
+                                                   : cudaMemcpyDeviceToDevice,
+                          stream),
+          "get_state copy");
+    check(cudaStreamSynchronize(stream), "get_state");
+  }
+
+  void launch_stage_kind(const int kind, double2* input) {
+    for (StageLaunch g : groups) {
+      g.stage = kind;
+      if (input != nullptr) g.y = input;
+      check(launch_stage(g, stream), "stage kernel");
+    }
+  }
+
+  void evaluate_rhs(const int instance, const double* stage, double* out,
+                    const size_t count, const int memory) {
+    check_instance(instance);
+    if (plans.size() != 1) {
+      throw std::invalid_argument("evaluate_rhs needs a single-solve pipeline");
+    }
+    InstancePlan& plan = plans[static_cast<size_t>(instance)];
+    if (count != plan.value_count()) {
+      throw std::invalid_argument("state complex count does not match shape");
+    }
+    const size_t bytes = count * sizeof(double2);
+    const double2* source = reinterpret_cast<const double2*>(stage);
+    if (memory == TEUK_B200_HOST) {
+      check(cudaMemcpyAsync(d_nodal.ptr, stage, bytes, cudaMemcpyHostToDevice,
+                            stream),
+            "evaluate_rhs upload");
+      source = d_nodal.ptr;
+    }
+    ConvertLaunch c = convert(instance);
+    c.nodal_in = source;
+    c.modal = kB.ptr;
+    check(launch_nodal_to_modal(c, stream), "nodal_to_modal");
+    launch_stage_kind(kRhsOnly, kB.ptr);
+    assemble_nodal(instance, kA.ptr, true);
+    check(cudaMemcpyAsync(out, d_nodal.ptr, bytes,
+                          memory == TEUK_B200_HOST ? cudaMemcpyDeviceToHost
+                                                   : cudaMemcpyDeviceToDevice,
+                          stream),
+          "evaluate_rhs copy");
+    check(cudaStreamSynchronize(stream), "evaluate_rhs");
+  }
+
+  void set_dt(const std::vector<double>& dt) {
+    for (size_t i = 0; i < h_inst.size(); ++i) {
+      if (!std::isfinite(dt[i]) || !(dt[i] > 0.0)) {
+        throw std::invalid_argument(
+            "pipeline step requires finite positive time data");
+      }
+      if (h_inst[i].dt != dt[i]) {
+        h_inst[i].dt = dt[i];
+        dt_dirty = true;
+      }
+    }
+    if (dt_dirty) upload_descriptors();
+  }
+
+  void record_step() {
+    launch_stage_kind(kStage1, nullptr);
+    launch_stage_kind(kStage2, nullptr);
+    launch_stage_kind(kStage3, nullptr);
+    launch_stage_kind(kStage4, nullptr);
+  }
+
+  void step(const std::vector<double>& dt, const int steps, const bool use_graph) {
+    if (steps < 0) throw std::invalid_argument("step count must be nonnegative");
+    set_dt(dt);
+    if (!use_graph) {
+      for (int s = 0; s < steps; ++s) record_step();
+      check(cudaGetLastError(), "step");
+      return;
+    }
+    if (graph_exec == nullptr || graph_stream != stream) {
+      if (graph_exec != nullptr) cudaGraphExecDestroy(graph_exec);
+      if (graph != nullptr) cudaGraphDestroy(graph);
+      graph_exec = nullptr;
+      graph = nullptr;
+      check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal),
+            "begin capture");
+      try {
+        record_step();
+      } catch (...) {
+        cudaGraph_t discard = nullptr;
+        cudaStreamEndCapture(stream, &discard);
+        if (discard != nullptr) cudaGraphDestroy(discard);
+        throw;
+      }
+      check(cudaStreamEndCapture(stream, &graph), "end capture");
+      check(cudaGraphInstantiate(&graph_exec, graph, 0), "graph instantiate");
+      graph_stream = stream;
+    }
+    for (int s = 0; s < steps; ++s) {
+      check(cudaGraphLaunch(graph_exec, stream), "graph launch");
+    }
+  }
+
+  void endpoint_modal(double* out, const size_t capacity, size_t* count,
+                      const int memory) {
+    const size_t n = h_seg.size() * 2 * static_cast<size_t>(max_ell);
+    if (count != nullptr) *count = n;
+    if (out == nullptr) return;
+    if (capacity < n) {
+      throw std::invalid_argument("endpoint buffer capacity is too small");
+    }
+    check(launch_endpoint_gather(y.ptr, d_seg.ptr, d_inst.ptr,
+                                 static_cast<int>(h_seg.size()), max_ell,
+                                 d_endpoint.ptr, stream),
+          "endpoint gather");
+    check(cudaMemcpyAsync(out, d_endpoint.ptr, n * sizeof(double2),
+                          memory == TEUK_B200_HOST ? cudaMemcpyDeviceToHost
+                                                   : cudaMemcpyDeviceToDevice,
+                          stream),
+          "endpoint copy");
+    if (memory == TEUK_B200_HOST) {
+      check(cudaStreamSynchronize(stream), "endpoint sync");
+    }
+  }
+
+  void sample_endpoint(const int instance, teuk_b200_waveform_record* out,
+                       const size_t capacity, size_t* count) {
+    check_instance(instance);
+    const InstancePlan& plan = plans[static_cast<size_t>(instance)];
+    const Config& c = plan.config;
+    const int ne_max = max_ell;
+    std::vector<double2> gathered(h_seg.size() * 2 * static_cast<size_t>(ne_max));
+    size_t n = 0;
+    endpoint_modal(reinterpret_cast<double*>(gathered.data()), gathered.size(),
+                   &n, TEUK_B200_HOST);
+    std::vector<teuk_b200_waveform_record> records;
+    const double scale[2] = {c.length * c.length, plan.horizon};
+    // first-order field: modal coefficients straight from the band storage
+    for (int boundary = 0; boundary < 2; ++boundary) {
+      for (const ModePlan& mp : plan.modes) {
+        if (!mp.parent) continue;
+        const size_t base =
+            (static_cast<size_t>(mp.segment) * 2 + static_cast<size_t>(boundary)) *
+            static_cast<size_t>(ne_max);
+        for (int l = 0; l < mp.n_ell; ++l) {
+          const double2 v = gathered[base + static_cast<size_t>(l)];
+          records.push_back({boundary, 1, mp.m, mp.ell_min + l, v.x, v.y,
+                             scale[boundary] * v.x, scale[boundary] * v.y});
+        }
+      }
+    }
+    // second-order field: frozen in the linear pipeline; analyze the stored
+    // endpoint values with the target band's transform.
+    const int nt = c.ntheta;
+    const auto& frozen = frozen_dev[static_cast<size_t>(instance)];
+    std::vector<double2> slice(static_cast<size_t>(nt));
+    for (int boundary = 0; boundary < 2; ++boundary) {
+      const int r = boundary == 0 ? 0 : c.nr - 1;
+      for (const ModePlan& mp : plan.modes) {
+        if (!std::binary_search(c.targets.begin(), c.targets.end(), mp.m)) {
+          continue;
+        }
+        std::fill(slice.begin(), slice.end(), make_double2(0.0, 0.0));
+        if (frozen.ptr != nullptr) {
+          const size_t offset =
+              ((static_cast<size_t>(mp.mode_index) * kFieldCount + 12) *
+                   static_cast<size_t>(c.nr) +
+               static_cast<size_t>(r)) *
+              static_cast<size_t>(nt);
+          check(cudaMemcpy(slice.data(), frozen.ptr + offset,
+                           static_cast<size_t>(nt) * sizeof(double2),
+                           cudaMemcpyDeviceToHost),
+                "second-order endpoint slice");
+        }
+        const int ell_min = std::max(2, std::abs(mp.m));
+        const double pi = std::numbers::pi_v<double>;
+        for (int ell = ell_min; ell <= c.ell_max_second; ++ell) {
+          double re = 0.0, im = 0.0;
+          for (int j = 0; j < nt; ++j) {
+            const double a = 2.0 * pi * plan.weights[static_cast<size_t>(j)] *
+                             spin_weighted_harmonic_theta(
+                                 ell, mp.m, kSpinWeight,
+                                 plan.theta[static_cast<size_t>(j)]);
+            re += a * slice[static_cast<size_t>(j)].x;
+            im += a * slice[static_cast<size_t>(j)].y;
+          }
+          records.push_back({boundary, 2, mp.m, ell, re, im,
+                             scale[boundary] * re, scale[boundary] * im});
+        }
+      }
+    }
+    if (count != nullptr) *count = records.size();
+    if (records.size() > capacity) {
+      throw std::invalid_argument("waveform record capacity is too small");
+    }
+    std::copy(records.begin(), records.end(), out);
+  }
+
+  size_t device_bytes() const {
+    return 4 * total_complex * sizeof(double2) + d_nodal.count * sizeof(double2) +
+           h_mat.size() * sizeof(double) + h_trig.size() * sizeof(double) +
+           h_tiles.size() * sizeof(TileDesc) + h_seg.size() * sizeof(SegmentDesc) +
+           d_endpoint.count * sizeof(double2);
+  }
+};
+
+}  // namespace teuk_b200
+
+using teuk_b200::Batch;
+using teuk_b200::guarded;
+
+struct teuk_b200_batch {
+  std::unique_ptr<Batch> batch;
+};
+struct teuk_b200_pipeline {
+  std::unique_ptr<Batch> batch;
+};
+
+namespace {
+
+void require(const bool condition, const char* message) {
+  if (!condition) throw std::invalid_argument(message);
+}
+
+void fill_shape(const teuk_b200::InstancePlan& plan, size_t shape[4]) {
+  shape[0] = plan.config.modes.size();
+  shape[1] = teuk_b200::kFieldCount;
+  shape[2] = static_cast<size_t>(plan.config.nr);
+  shape[3] = static_cast<size_t>(plan.config.ntheta);
+}
+
+void restore_activation(teuk_b200::InstancePlan& plan,
+                        const teuk_b200_activation& s) {
+  // SpatialPipeline::validate_source_activation_state
+  // (include/teuk/spatial_pipeline.hpp:1225-1235)
+  if (s.consecutive_passes < 0 || !std::isfinite(s.activation_time) ||
+      !std::isfinite(s.last_eligibility_time) ||
+      (s.active != 0 && s.activation_time < 0.0) ||
+      (s.active == 0 && s.activation_time != -1.0) ||
+      s.last_eligibility_time < -1.0) {
+    throw std::invalid_argument("invalid second-order source activation state");
+  }
+  plan.active = s.active != 0 ? 1 : 0;
+  plan.activation_time = s.activation_time;
+  plan.consecutive_passes = s.consecutive_passes;
+  plan.last_eligibility_time = s.last_eligibility_time;
+}
+
+void reset_activation(teuk_b200::InstancePlan& plan) {
+  plan.active = 0;
+  plan.activation_time = -1.0;
+  plan.consecutive_passes = 0;
+  plan.last_eligibility_time = -1.0;
+  const auto& c = plan.config;
+  if (c.source_mode == TEUK_B200_SOURCE_UNRESTRICTED &&
+      c.source_start_time == 0.0) {
+    plan.active = 1;
+    plan.activation_time = 0.0;
+    plan.consecutive_passes = c.required_passes;
+  }
+}
+
+void initialize_gaussian(Batch& b, const int instance,
+                         const teuk_b200_gaussian* pulse) {
+  b.check_instance(instance);
+  require(pulse != nullptr, "null Gaussian pulse");
+  require(pulse->mode_count >= 0 &&
+              (pulse->mode_count == 0 || pulse->modes != nullptr),
+          "Gaussian mode list pointer/count mismatch");
+  std::vector<int> ell, m;
+  std::vector<double> re, im;
+  for (int i = 0; i < pulse->mode_count; ++i) {
+    ell.push_back(pulse->modes[i].ell);
+    m.push_back(pulse->modes[i].m);
+    re.push_back(pulse->modes[i].amplitude_real);
+    im.push_back(pulse->modes[i].amplitude_imag);
+  }
+  auto& plan = b.plans[static_cast<size_t>(instance)];
+  std::vector<double> nodal;
+  teuk_b200::gaussian_initial_state(plan, pulse->center, pulse->width,
+                                    pulse->compact_support != 0, ell, m, re,
+                                    im, nodal);
+  b.set_state(instance, nodal.data(), plan.value_count(), TEUK_B200_HOST);
+  reset_activation(plan);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* teuk_b200_last_error(void) {
+  return teuk_b200::g_last_error.c_str();
+}
+
+int teuk_b200_abi_version(void) { return TEUK_B200_ABI_VERSION; }
+
+int teuk_b200_create(const teuk_b200_config* config,
+                     teuk_b200_pipeline** out) {
+  return guarded([&] {
+    require(config != nullptr && out != nullptr, "null argument");
+    auto p = std::make_unique<teuk_b200_pipeline>();
+    p->batch = std::make_unique<Batch>();
+    p->batch->build({teuk_b200::to_config(*config)});
+    *out = p.release();
+  });
+}
+
+int teuk_b200_destroy(teuk_b200_pipeline* pipeline) {
+  delete pipeline;
+  return TEUK_B200_OK;
+}
+
+int teuk_b200_shape(const teuk_b200_pipeline* p, size_t shape[4]) {
+  return guarded([&] {
+    require(p != nullptr && shape != nullptr, "null argument");
+    fill_shape(p->batch->plans[0], shape);
+  });
+}
+
+int teuk_b200_set_state(teuk_b200_pipeline* p, const double* state,
+                        size_t count, int memory) {
+  return guarded([&] {
+    require(p != nullptr, "null pipeline");
+    p->batch->set_state(0, state, count, memory);
+  });
+}
+
+int teuk_b200_get_state(teuk_b200_pipeline* p, double* state, size_t count,
+                        int memory) {
+  return guarded([&] {
+    require(p != nullptr, "null pipeline");
+    p->batch->get_state(0, state, count, memory);
+  });
+}
+
+int teuk_b200_evaluate_rhs(teuk_b200_pipeline* p, const double* stage,
+                           double* output, size_t count, double time,
+                           int memory) {
+  return guarded([&] {
+    require(p != nullptr && stage != nullptr && output != nullptr,
+            "null argument");
+    require(std::isfinite(time), "stage time must be finite");
+    p->batch->evaluate_rhs(0, stage, output, count, memory);
+  });
+}
+
+int teuk_b200_step(teuk_b200_pipeline* p, double time, double dt, int steps) {
+  return guarded([&] {
+    require(p != nullptr, "null pipeline");
+    if (!std::isfinite(time) || !std::isfinite(dt) || time < 0.0 ||
+        !(dt > 0.0)) {
+      throw std::invalid_argument(
+          "pipeline step requires finite positive time data");
+    }
+    p->batch->step({dt}, steps, false);
+    teuk_b200::check(cudaStreamSynchronize(p->batch->stream), "step");
+  });
+}
+
+int teuk_b200_initialize_gaussian(teuk_b200_pipeline* p,
+                                  const teuk_b200_gaussian* pulse) {
+  return guarded([&] {
+    require(p != nullptr, "null pipeline");
+    initialize_gaussian(*p->batch, 0, pulse);
+  });
+}
+
+int teuk_b200_sample_endpoint(teuk_b200_pipeline* p,
+                              teuk_b200_waveform_record* out,
+                              size_t capacity, size_t* count) {
+  return guarded([&] {
+    require(p != nullptr, "null pipeline");
+    p->batch->sample_endpoint(0, out, capacity, count);
+  });
+}
+
+int teuk_b200_get_activation(const teuk_b200_pipeline* p,
+                             teuk_b200_activation* out) {
+  return guarded([&] {
+    require(p != nullptr && out != nullptr, "null argument");
+    const auto& plan = p->batch->plans[0];
+    out->active = plan.active;
+    out->activation_time = plan.activation_time;
+    out->consecutive_passes = plan.consecutive_passes;
+    out->last_eligibility_time = plan.last_eligibility_time;
+  });
+}
+
+int teuk_b200_restore_activation(teuk_b200_pipeline* p,
+                                 const teuk_b200_activation* state) {
+  return guarded([&] {
+    require(p != nullptr && state != nullptr, "null argument");
+    restore_activation(p->batch->plans[0], *state);
+  });
+}
+
+int teuk_b200_reset_activation(teuk_b200_pipeline* p) {
+  return guarded([&] {
+    require(p != nullptr, "null pipeline");
+    reset_activation(p->batch->plans[0]);
+  });
+}
+
+int teuk_b200_set_stream(teuk_b200_pipeline* p, void* cuda_stream) {
+  return guarded([&] {
+    require(p != nullptr, "null pipeline");
+    p->batch->stream = cuda_stream != nullptr
+                           ? static_cast<cudaStream_t>(cuda_stream)
+                           : p->batch->own_stream;
+  });
+}
+
+int teuk_b200_synchronize(teuk_b200_pipeline* p) {
+  return guarded([&] {
+    require(p != nullptr, "null pipeline");
+    teuk_b200::check(cudaStreamSynchronize(p->batch->stream), "synchronize");
+  });
+}
+
+int teuk_b200_footprint_bytes(const teuk_b200_config* config, size_t* bytes) {
+  return guarded([&] {
+    require(config != nullptr && bytes != nullptr, "null argument");
+    const auto plan =
+        teuk_b200::build_instance_plan(teuk_b200::to_config(*config));
+    size_t complex_count = 0;
+    size_t matrix = 0;
+    for (const auto& mp : plan.modes) {
+      if (!mp.parent) continue;
+      size_t count = static_cast<size_t>(plan.config.nr) * 3 *
+                     static_cast<size_t>(mp.n_ell);
+      complex_count += (count + 15) / 16 * 16;
+      matrix += 2 * static_cast<size_t>(mp.n_ell * plan.config.ntheta);
+    }
+    *bytes = 4 * complex_count * sizeof(double2) + matrix * sizeof(double) +
+             plan.value_count() * sizeof(double2);
+  });
+}
+
+int teuk_b200_batch_create(const teuk_b200_config* configs, int count,
+                           teuk_b200_batch** out) {
+  return guarded([&] {
+    require(configs != nullptr && out != nullptr && count > 0,
+            "null argument or empty batch");
+    std::vector<teuk_b200::Config> list;
+    for (int i = 0; i < count; ++i) {
+      list.push_back(teuk_b200::to_config(configs[i]));
+    }
+    auto b = std::make_unique<teuk_b200_batch>();
+    b->batch = std::make_unique<Batch>();
+    b->batch->build(list);
+    *out = b.release();
+  });
+}
+
+int teuk_b200_batch_destroy(teuk_b200_batch* batch) {
+  delete batch;
+  return TEUK_B200_OK;
+}
+
+int teuk_b200_batch_size(const teuk_b200_batch* b, int* count) {
+  return guarded([&] {
+    require(b != nullptr && count != nullptr, "null argument");
+    *count = static_cast<int>(b->batch->plans.size());
+  });
+}
+
+int teuk_b200_batch_shape(const teuk_b200_batch* b, int instance,
+                          size_t shape[4]) {
+  return guarded([&] {
+    require(b != nullptr && shape != nullptr, "null argument");
+    b->batch->check_instance(instance);
+    fill_shape(b->batch->plans[static_cast<size_t>(instance)], shape);
+  });
+}
+
+int teuk_b200_batch_set_state(teuk_b200_batch* b, int instance,
+                              const double* state, size_t count, int memory) {
+  return guarded([&] {
+    require(b != nullptr, "null batch");
+    b->batch->set_state(instance, state, count, memory);
+  });
+}
+
+int teuk_b200_batch_get_state(teuk_b200_batch* b, int instance,
+                              double* state, size_t count, int memory) {
+  return guarded([&] {
+    require(b != nullptr, "null batch");
+    b->batch->get_state(instance, state, count, memory);
+  });
+}
+
+int teuk_b200_batch_initialize_gaussian(teuk_b200_batch* b, int instance,
+                                        const teuk_b200_gaussian* pulse) {
+  return guarded([&] {
+    require(b != nullptr, "null batch");
+    initialize_gaussian(*b->batch, instance, pulse);
+  });
+}
+
+int teuk_b200_batch_step(teuk_b200_batch* b, const double* dt, int steps,
+                         int graph) {
+  return guarded([&] {
+    require(b != nullptr && dt != nullptr, "null argument");
+    std::vector<double> list(dt, dt + b->batch->plans.size());
+    b->batch->step(list, steps, graph != 0);
+  });
+}
+
+int teuk_b200_batch_sample_endpoint(teuk_b200_batch* b, int instance,
+                                    teuk_b200_waveform_record* out,
+                                    size_t capacity, size_t* count) {
+  return guarded([&] {
+    require(b != nullptr, "null batch");
+    b->batch->sample_endpoint(instance, out, capacity, count);
+  });
+}
+
+int teuk_b200_batch_endpoint_modal(teuk_b200_batch* b, double* out,
+                                   size_t capacity, size_t* count,
+                                   int memory) {
+  return guarded([&] {
+    require(b != nullptr, "null batch");
+    b->batch->endpoint_modal(out, capacity, count, memory);
+  });
+}
+
+int teuk_b200_batch_set_stream(teuk_b200_batch* b, void* cuda_stream) {
+  return guarded([&] {
+    require(b != nullptr, "null batch");
+    b->batch->stream = cuda_stream != nullptr
+                           ? static_cast<cudaStream_t>(cuda_stream)
+                           : b->batch->own_stream;
+  });
+}
+
+int teuk_b200_batch_synchronize(teuk_b200_batch* b) {
+  return guarded([&] {
+    require(b != nullptr, "null batch");
+    teuk_b200::check(cudaStreamSynchronize(b->batch->stream), "synchronize");
+  });
+}
+
+int teuk_b200_batch_launches_per_step(const teuk_b200_batch* b,
+                                      int* launches) {
+  return guarded([&] {
+    require(b != nullptr && launches != nullptr, "null argument");
+    *launches = 4 * static_cast<int>(b->batch->groups.size());
+  });
+}
+
+}  // extern "C"

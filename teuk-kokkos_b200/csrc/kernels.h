@@ -1,0 +1,82 @@
+// Launch interface of the CUDA kernels (kernels.cu) used by the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "engine.h"
+
+namespace teuk_b200 {
+
+// RK stage selector of stage_kernel.  kRhsOnly evaluates k = f(y) into kA
+// without touching y / kB / acc (evaluate_rhs).
+enum StageKind : int {
+  kStage1 = 1,
+  kStage2 = 2,
+  kStage3 = 3,
+  kStage4 = 4,
+  kRhsOnly = 5
+};
+
+struct StageLaunch {
+  double2* y;
+  double2* kA;
+  double2* kB;
+  double2* acc;
+  const InstanceDesc* instances;
+  const SegmentDesc* segments;
+  const TileDesc* tiles;  // tiles of this launch group
+  const double* matrices;
+  const double* trig;
+  int tile_count;
+  int disc;
+  int reduction;  // 0 free damped, 1 stage constrained
+  int stage;
+  // shared-memory carve-up capacities (elements), host-computed per group
+  int slab_capacity;   // double2
+  int dslab_capacity;  // double2
+  int matrix_capacity; // doubles per matrix
+  int coef_rows;       // rows of coefficient records
+  int max_theta;
+  int max_ell;
+};
+
+// Dynamic shared memory bytes for one launch description.
+size_t stage_smem_bytes(const StageLaunch& launch);
+cudaError_t upload_sbp_constants(const SbpConstants& constants);
+cudaError_t launch_stage(const StageLaunch& launch, cudaStream_t stream);
+
+// Nodal (m,13,r,theta) complex array of one instance <-> modal segments.
+struct ConvertLaunch {
+  const double2* nodal_in;  // nodal -> modal source
+  double2* nodal_out;       // modal -> nodal destination
+  double2* modal;           // state buffer base
+  const SegmentDesc* segments;
+  const int* segment_modes;  // registry index of each listed segment
+  const double* matrices;
+  int segment_count;
+  int nr;
+  int ntheta;
+  int mode_count;  // registry modes of the instance
+  int max_ell;
+};
+cudaError_t launch_nodal_to_modal(const ConvertLaunch& launch,
+                                  cudaStream_t stream);
+cudaError_t launch_modal_to_nodal(const ConvertLaunch& launch,
+                                  cudaStream_t stream);
+
+// Sets *flag to 1 when any value of a frozen (mode, field) plane of the
+// nodal state is non-zero.  parent_mask[mode] is 1 for parent modes, whose
+// first three fields are evolved (not frozen).
+cudaError_t launch_frozen_scan(const double2* nodal, const int* parent_mask,
+                               int modes, int plane_values, int* flag,
+                               cudaStream_t stream);
+
+// Gather psi modal coefficients at r = 0 and r = nr-1 of every segment into
+// out[(2 * segment + boundary) * max_ell + ell].
+cudaError_t launch_endpoint_gather(const double2* y,
+                                   const SegmentDesc* segments,
+                                   const InstanceDesc* instances,
+                                   int segment_count, int max_ell,
+                                   double2* out, cudaStream_t stream);
+
+}  // namespace teuk_b200

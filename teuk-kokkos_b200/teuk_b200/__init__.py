@@ -1,0 +1,504 @@
+"""Python host binding of the B200 teuk-kokkos RK4 engine (ctypes over the
+C ABI declared in include/teuk_b200.h).
+
+The classes mirror the reference's C++ interface: ``Pipeline`` is
+``teuk::SpatialPipeline`` (include/teuk/spatial_pipeline.hpp:144-1364) for one
+solve and ``Batch`` packs many solves into one set of stage launches.  State
+arrays are complex128 in the reference's (mode, field, radial, theta) order.
+Arrays may be numpy (host) or torch CUDA tensors (device).  There is no CPU
+fallback: importing this module fails when libteuk_b200.so is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Iterable, Sequence
+
+import numpy as np
+
+_PACKAGE = Path(__file__).resolve().parent.parent
+LIBRARY_PATH = _PACKAGE / "lib" / "libteuk_b200.so"
+
+OK = 0
+ERR_INVALID_ARGUMENT = -1
+ERR_RUNTIME = -2
+ERR_CUDA = -3
+ERR_UNSUPPORTED = -4
+ERR_OUT_OF_MEMORY = -5
+
+HOST = 0
+DEVICE = 1
+
+D42, D84, D105 = 0, 1, 2
+FREE_DAMPED, STAGE_CONSTRAINED = 0, 1
+SOURCE_DISABLED, SOURCE_CONSTRAINT_AWARE, SOURCE_UNRESTRICTED = 0, 1, 2
+FIELD_COUNT = 13
+SCRI, HORIZON = 0, 1
+
+DISCRETIZATION_NAMES = {"d4-2": D42, "d8-4": D84, "d10-5": D105}
+
+
+class TeukError(RuntimeError):
+    """Raised for any non-zero status; ``status`` holds the code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+class InvalidArgument(TeukError, ValueError):
+    """std::invalid_argument in the reference."""
+
+
+class Unsupported(TeukError):
+    """A valid reference input that the B200 path does not run yet."""
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_int),
+        ("mass", ctypes.c_double),
+        ("spin", ctypes.c_double),
+        ("compactification_length", ctypes.c_double),
+        ("radial_points", ctypes.c_int),
+        ("theta_nodes", ctypes.c_int),
+        ("ell_max_first", ctypes.c_int),
+        ("ell_max_second", ctypes.c_int),
+        ("mode_count", ctypes.c_int),
+        ("modes", ctypes.POINTER(ctypes.c_int)),
+        ("parent_count", ctypes.c_int),
+        ("parents", ctypes.POINTER(ctypes.c_int)),
+        ("target_count", ctypes.c_int),
+        ("targets", ctypes.POINTER(ctypes.c_int)),
+        ("reduction_damping", ctypes.c_double),
+        ("dissipation", ctypes.c_double),
+        ("reduction", ctypes.c_int),
+        ("discretization", ctypes.c_int),
+        ("source_mode", ctypes.c_int),
+        ("source_start_time", ctypes.c_double),
+        ("normalized_constraint_tolerance", ctypes.c_double),
+        ("required_consecutive_passes", ctypes.c_int),
+    ]
+
+
+class Activation(ctypes.Structure):
+    _fields_ = [
+        ("active", ctypes.c_int),
+        ("activation_time", ctypes.c_double),
+        ("consecutive_passes", ctypes.c_int),
+        ("last_eligibility_time", ctypes.c_double),
+    ]
+
+
+class _GaussianMode(ctypes.Structure):
+    _fields_ = [
+        ("ell", ctypes.c_int),
+        ("m", ctypes.c_int),
+        ("amplitude_real", ctypes.c_double),
+        ("amplitude_imag", ctypes.c_double),
+    ]
+
+
+class _Gaussian(ctypes.Structure):
+    _fields_ = [
+        ("center", ctypes.c_double),
+        ("width", ctypes.c_double),
+        ("compact_support", ctypes.c_int),
+        ("mode_count", ctypes.c_int),
+        ("modes", ctypes.POINTER(_GaussianMode)),
+    ]
+
+
+class WaveformRecord(ctypes.Structure):
+    _fields_ = [
+        ("boundary", ctypes.c_int),
+        ("order", ctypes.c_int),
+        ("m", ctypes.c_int),
+        ("ell", ctypes.c_int),
+        ("rescaled_real", ctypes.c_double),
+        ("rescaled_imag", ctypes.c_double),
+        ("endpoint_real", ctypes.c_double),
+        ("endpoint_imag", ctypes.c_double),
+    ]
+
+
+ABI_VERSION = 1
+
+
+@dataclass
+class SolveConfig:
+    """SpatialPipeline constructor arguments + ModeRegistry lists."""
+
+    mass: float = 1.0
+    spin: float = 0.0
+    compactification_length: float = 1.0
+    radial_points: int = 65
+    theta_nodes: int = 7
+    ell_max_first: int = 4
+    ell_max_second: int = 4
+    modes: Sequence[int] = (-2, 2)
+    parents: Sequence[int] | None = None
+    targets: Sequence[int] | None = None
+    reduction_damping: float = 0.1
+    dissipation: float = 0.0
+    reduction: int = FREE_DAMPED
+    discretization: int = D42
+    source_mode: int = SOURCE_DISABLED
+    source_start_time: float = 0.0
+    normalized_constraint_tolerance: float = 0.0
+    required_consecutive_passes: int = 1
+
+    @property
+    def horizon_radius(self) -> float:
+        r_plus = self.mass + math.sqrt(self.mass * self.mass - self.spin * self.spin)
+        return self.compactification_length ** 2 / r_plus
+
+    @property
+    def spacing(self) -> float:
+        return self.horizon_radius / (self.radial_points - 1)
+
+    def parent_list(self):
+        return list(self.modes if self.parents is None else self.parents)
+
+    def target_list(self):
+        return list(self.modes if self.targets is None else self.targets)
+
+    def shape(self):
+        return (len(self.modes), FIELD_COUNT, self.radial_points, self.theta_nodes)
+
+    def value_count(self) -> int:
+        return int(np.prod(self.shape()))
+
+    def to_struct(self):
+        """ctypes struct plus the arrays it points into (keep them alive)."""
+        modes = (ctypes.c_int * len(self.modes))(*self.modes)
+        parents_list = self.parent_list()
+        targets_list = self.target_list()
+        parents = (ctypes.c_int * len(parents_list))(*parents_list)
+        targets = (ctypes.c_int * len(targets_list))(*targets_list)
+        s = _Config(
+            ABI_VERSION, self.mass, self.spin, self.compactification_length,
+            self.radial_points, self.theta_nodes, self.ell_max_first,
+            self.ell_max_second, len(self.modes), modes, len(parents_list),
+            parents, len(targets_list), targets, self.reduction_damping,
+            self.dissipation, self.reduction, self.discretization,
+            self.source_mode, self.source_start_time,
+            self.normalized_constraint_tolerance,
+            self.required_consecutive_passes)
+        return s, (modes, parents, targets)
+
+
+@dataclass
+class GaussianPulse:
+    """PipelineGaussianPulse (include/teuk/pipeline_initial_data.hpp:29-57);
+    center/width are compactified radii."""
+
+    center: float
+    width: float
+    modes: Sequence[tuple] = field(default_factory=lambda: [(2, 2, 1e-3 + 0j)])
+    compact_support: bool = False
+
+    def to_struct(self):
+        items = (_GaussianMode * len(self.modes))()
+        for i, (ell, m, amp) in enumerate(self.modes):
+            amp = complex(amp)
+            items[i] = _GaussianMode(int(ell), int(m), amp.real, amp.imag)
+        return _Gaussian(self.center, self.width, int(self.compact_support),
+                         len(self.modes), items), items
+
+
+def _load() -> ctypes.CDLL:
+    if not LIBRARY_PATH.exists():
+        raise ImportError(
+            f"{LIBRARY_PATH} is missing: build it with "
+            "`python teuk-kokkos_b200/build.py` (no CPU fallback exists)")
+    lib = ctypes.CDLL(str(LIBRARY_PATH))
+    P = ctypes.c_void_p
+    D = ctypes.c_double
+    I = ctypes.c_int
+    SZ = ctypes.c_size_t
+    DP = ctypes.POINTER(ctypes.c_double)
+    sig = {
+        "teuk_b200_last_error": ([], ctypes.c_char_p),
+        "teuk_b200_abi_version": ([], I),
+        "teuk_b200_create": ([ctypes.POINTER(_Config), ctypes.POINTER(P)], I),
+        "teuk_b200_destroy": ([P], I),
+        "teuk_b200_shape": ([P, ctypes.POINTER(SZ)], I),
+        "teuk_b200_set_state": ([P, P, SZ, I], I),
+        "teuk_b200_get_state": ([P, P, SZ, I], I),
+        "teuk_b200_evaluate_rhs": ([P, P, P, SZ, D, I], I),
+        "teuk_b200_step": ([P, D, D, I], I),
+        "teuk_b200_initialize_gaussian": ([P, ctypes.POINTER(_Gaussian)], I),
+        "teuk_b200_sample_endpoint": ([P, ctypes.POINTER(WaveformRecord), SZ,
+                                       ctypes.POINTER(SZ)], I),
+        "teuk_b200_get_activation": ([P, ctypes.POINTER(Activation)], I),
+        "teuk_b200_restore_activation": ([P, ctypes.POINTER(Activation)], I),
+        "teuk_b200_reset_activation": ([P], I),
+        "teuk_b200_set_stream": ([P, P], I),
+        "teuk_b200_synchronize": ([P], I),
+        "teuk_b200_footprint_bytes": ([ctypes.POINTER(_Config),
+                                       ctypes.POINTER(SZ)], I),
+        "teuk_b200_batch_create": ([ctypes.POINTER(_Config), I,
+                                    ctypes.POINTER(P)], I),
+        "teuk_b200_batch_destroy": ([P], I),
+        "teuk_b200_batch_size": ([P, ctypes.POINTER(I)], I),
+        "teuk_b200_batch_shape": ([P, I, ctypes.POINTER(SZ)], I),
+        "teuk_b200_batch_set_state": ([P, I, P, SZ, I], I),
+        "teuk_b200_batch_get_state": ([P, I, P, SZ, I], I),
+        "teuk_b200_batch_initialize_gaussian": ([P, I,
+                                                 ctypes.POINTER(_Gaussian)], I),
+        "teuk_b200_batch_step": ([P, DP, I, I], I),
+        "teuk_b200_batch_sample_endpoint": ([P, I,
+                                             ctypes.POINTER(WaveformRecord),
+                                             SZ, ctypes.POINTER(SZ)], I),
+        "teuk_b200_batch_endpoint_modal": ([P, P, SZ, ctypes.POINTER(SZ), I], I),
+        "teuk_b200_batch_set_stream": ([P, P], I),
+        "teuk_b200_batch_synchronize": ([P], I),
+        "teuk_b200_batch_launches_per_step": ([P, ctypes.POINTER(I)], I),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    return lib
+
+
+_lib = _load()
+EXPORTED_SYMBOLS = [n for n in dir(_lib) if n.startswith("teuk_b200_")]
+
+
+def library() -> ctypes.CDLL:
+    return _lib
+
+
+def _check(status: int):
+    if status == OK:
+        return
+    message = _lib.teuk_b200_last_error().decode()
+    if status == ERR_INVALID_ARGUMENT:
+        raise InvalidArgument(status, message)
+    if status == ERR_UNSUPPORTED:
+        raise Unsupported(status, message)
+    raise TeukError(status, message)
+
+
+def _pointer(array, writable: bool, count: int):
+    """(pointer, memory kind, keepalive) for a complex128 buffer."""
+    try:
+        import torch
+    except ImportError:  # pragma: no cover - torch is in the image
+        torch = None
+    if torch is not None and isinstance(array, torch.Tensor):
+        if array.dtype != torch.complex128 or not array.is_contiguous():
+            raise ValueError("state tensors must be contiguous complex128")
+        if array.numel() != count:
+            raise ValueError("state tensor size does not match the shape")
+        kind = DEVICE if array.is_cuda else HOST
+        return ctypes.c_void_p(array.data_ptr()), kind, array
+    arr = np.asarray(array)
+    if arr.dtype != np.complex128 or not arr.flags.c_contiguous:
+        raise ValueError("state arrays must be C-contiguous complex128")
+    if writable and not arr.flags.writeable:
+        raise ValueError("output array is read-only")
+    if arr.size != count:
+        raise ValueError("state array size does not match the shape")
+    return ctypes.c_void_p(arr.ctypes.data), HOST, arr
+
+
+def _records(buffer, count):
+    out = []
+    for i in range(count):
+        r = buffer[i]
+        out.append({
+            "boundary": "scri" if r.boundary == SCRI else "horizon",
+            "order": r.order, "m": r.m, "ell": r.ell,
+            "rescaled": complex(r.rescaled_real, r.rescaled_imag),
+            "endpoint": complex(r.endpoint_real, r.endpoint_imag),
+        })
+    return out
+
+
+def footprint_bytes(config: SolveConfig) -> int:
+    s, keep = config.to_struct()
+    out = ctypes.c_size_t()
+    _check(_lib.teuk_b200_footprint_bytes(ctypes.byref(s), ctypes.byref(out)))
+    return out.value
+
+
+class Pipeline:
+    """One solve (teuk::SpatialPipeline)."""
+
+    def __init__(self, config: SolveConfig):
+        self.config = config
+        s, keep = config.to_struct()
+        handle = ctypes.c_void_p()
+        _check(_lib.teuk_b200_create(ctypes.byref(s), ctypes.byref(handle)))
+        self._handle = handle
+
+    def close(self):
+        if getattr(self, "_handle", None):
+            _lib.teuk_b200_destroy(self._handle)
+            self._handle = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def shape(self):
+        dims = (ctypes.c_size_t * 4)()
+        _check(_lib.teuk_b200_shape(self._handle, dims))
+        return tuple(int(d) for d in dims)
+
+    def set_state(self, state):
+        ptr, kind, _keep = _pointer(state, False, self.config.value_count())
+        _check(_lib.teuk_b200_set_state(self._handle, ptr,
+                                        self.config.value_count(), kind))
+
+    def get_state(self, out=None):
+        if out is None:
+            out = np.zeros(self.shape, dtype=np.complex128)
+        ptr, kind, _keep = _pointer(out, True, self.config.value_count())
+        _check(_lib.teuk_b200_get_state(self._handle, ptr,
+                                        self.config.value_count(), kind))
+        return out
+
+    def evaluate_rhs(self, stage, out=None, time: float = 0.0):
+        if out is None:
+            out = np.zeros(self.shape, dtype=np.complex128)
+        src, kind, _k1 = _pointer(stage, False, self.config.value_count())
+        dst, kind2, _k2 = _pointer(out, True, self.config.value_count())
+        if kind != kind2:
+            raise ValueError("stage and output must live in the same memory")
+        _check(_lib.teuk_b200_evaluate_rhs(self._handle, src, dst,
+                                           self.config.value_count(), time,
+                                           kind))
+        return out
+
+    def step(self, time: float, dt: float, steps: int = 1):
+        _check(_lib.teuk_b200_step(self._handle, time, dt, steps))
+
+    def initialize_gaussian(self, pulse: GaussianPulse):
+        s, keep = pulse.to_struct()
+        _check(_lib.teuk_b200_initialize_gaussian(self._handle, ctypes.byref(s)))
+
+    def sample_endpoint(self):
+        count = ctypes.c_size_t()
+        cap = 4 * len(self.config.modes) * (self.config.ell_max_first +
+                                             self.config.ell_max_second + 2)
+        buf = (WaveformRecord * cap)()
+        _check(_lib.teuk_b200_sample_endpoint(self._handle, buf, cap,
+                                              ctypes.byref(count)))
+        return _records(buf, count.value)
+
+    def activation(self) -> Activation:
+        a = Activation()
+        _check(_lib.teuk_b200_get_activation(self._handle, ctypes.byref(a)))
+        return a
+
+    def restore_activation(self, a: Activation):
+        _check(_lib.teuk_b200_restore_activation(self._handle, ctypes.byref(a)))
+
+    def reset_activation(self):
+        _check(_lib.teuk_b200_reset_activation(self._handle))
+
+    def synchronize(self):
+        _check(_lib.teuk_b200_synchronize(self._handle))
+
+
+class Batch:
+    """Many independent solves advanced by the same stage launches."""
+
+    def __init__(self, configs: Iterable[SolveConfig]):
+        self.configs = list(configs)
+        structs = (_Config * len(self.configs))()
+        keep = []
+        for i, c in enumerate(self.configs):
+            s, k = c.to_struct()
+            structs[i] = s
+            keep.append(k)
+        handle = ctypes.c_void_p()
+        _check(_lib.teuk_b200_batch_create(structs, len(self.configs),
+                                           ctypes.byref(handle)))
+        self._handle = handle
+
+    def close(self):
+        if getattr(self, "_handle", None):
+            _lib.teuk_b200_batch_destroy(self._handle)
+            self._handle = None
+
+    __del__ = close
+
+    def __len__(self):
+        return len(self.configs)
+
+    def set_state(self, instance: int, state):
+        n = self.configs[instance].value_count()
+        ptr, kind, _keep = _pointer(state, False, n)
+        _check(_lib.teuk_b200_batch_set_state(self._handle, instance, ptr, n,
+                                              kind))
+
+    def get_state(self, instance: int, out=None):
+        c = self.configs[instance]
+        if out is None:
+            out = np.zeros(c.shape(), dtype=np.complex128)
+        ptr, kind, _keep = _pointer(out, True, c.value_count())
+        _check(_lib.teuk_b200_batch_get_state(self._handle, instance, ptr,
+                                              c.value_count(), kind))
+        return out
+
+    def initialize_gaussian(self, instance: int, pulse: GaussianPulse):
+        s, keep = pulse.to_struct()
+        _check(_lib.teuk_b200_batch_initialize_gaussian(self._handle, instance,
+                                                        ctypes.byref(s)))
+
+    def step(self, dt, steps: int = 1, graph: bool = True):
+        dts = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, dtype=np.float64),
+                                                   (len(self.configs),)))
+        _check(_lib.teuk_b200_batch_step(
+            self._handle, dts.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+            steps, int(graph)))
+
+    def sample_endpoint(self, instance: int):
+        c = self.configs[instance]
+        cap = 4 * len(c.modes) * (c.ell_max_first + c.ell_max_second + 2)
+        buf = (WaveformRecord * cap)()
+        count = ctypes.c_size_t()
+        _check(_lib.teuk_b200_batch_sample_endpoint(self._handle, instance, buf,
+                                                    cap, ctypes.byref(count)))
+        return _records(buf, count.value)
+
+    def endpoint_modal_count(self) -> int:
+        count = ctypes.c_size_t()
+        _check(_lib.teuk_b200_batch_endpoint_modal(self._handle, None, 0,
+                                                   ctypes.byref(count), HOST))
+        return count.value
+
+    def endpoint_modal(self, out=None):
+        n = self.endpoint_modal_count()
+        if out is None:
+            out = np.zeros(n, dtype=np.complex128)
+        ptr, kind, _keep = _pointer(out, True, n)
+        count = ctypes.c_size_t()
+        _check(_lib.teuk_b200_batch_endpoint_modal(self._handle, ptr, n,
+                                                   ctypes.byref(count), kind))
+        return out
+
+    def set_stream(self, stream_handle: int | None):
+        _check(_lib.teuk_b200_batch_set_stream(
+            self._handle, ctypes.c_void_p(stream_handle or 0)))
+
+    def synchronize(self):
+        _check(_lib.teuk_b200_batch_synchronize(self._handle))
+
+    def launches_per_step(self) -> int:
+        n = ctypes.c_int()
+        _check(_lib.teuk_b200_batch_launches_per_step(self._handle,
+                                                      ctypes.byref(n)))
+        return n.value
