@@ -1,0 +1,88 @@
+"""The drop-in boundary on a host without a GPU.
+
+* libteuk_b200.so loads and exports every entry point include/teuk_b200.h
+  declares;
+* construction-time validation reproduces the reference's
+  std::invalid_argument cases before any device work;
+* a valid configuration fails loudly (status TEUK_B200_ERR_CUDA) when no
+  CUDA device is usable: there is no CPU fallback;
+* the C++ facade (include/teuk_b200.hpp) compiles against the library and
+  maps status codes to the reference's exception types.
+"""
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+import teuk_b200 as tb
+from cases import CASES
+from conftest import cuda_available
+
+REPO = Path(__file__).resolve().parent.parent
+HEADER = REPO / "include" / "teuk_b200.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"\b(teuk_b200_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_header_symbols_are_exported():
+    names = declared_functions()
+    assert len(names) >= 30
+    out = subprocess.run(["nm", "-D", "--defined-only", str(tb.LIBRARY_PATH)],
+                         capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r"\bT (teuk_b200_\w+)", out))
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+    lib = tb.library()
+    for name in names:
+        assert hasattr(lib, name)
+
+
+def test_abi_version():
+    assert tb.library().teuk_b200_abi_version() == tb.ABI_VERSION
+
+
+@pytest.mark.parametrize("change,message", [
+    ({"radial_points": 12, "discretization": tb.D105},
+     "too small for selected discretization"),
+    ({"theta_nodes": 8}, "exact-product padding"),
+    ({"modes": (-2, 2, 3)}, "closed under m -> -m"),
+    ({"modes": (-2, 2, 2)}, "duplicate mode"),
+    ({"dissipation": -1.0}, "dissipation must be nonnegative"),
+    ({"parents": (-3, 3)}, "is not stored"),
+    ({"ell_max_first": 2}, "exact-product padding"),
+    ({"spin": 1.5}, "Kerr parameters"),
+])
+def test_reference_validation_before_device_work(change, message):
+    config = tb.SolveConfig(**{**CASES["schw_d84"].__dict__, **change})
+    with pytest.raises(tb.InvalidArgument, match=re.escape(message)):
+        tb.Pipeline(config)
+
+
+def test_second_order_policies_are_reported_unsupported_or_fail_on_cuda():
+    config = tb.SolveConfig(**{**CASES["schw_d84"].__dict__,
+                               "source_mode": tb.SOURCE_UNRESTRICTED})
+    with pytest.raises(tb.TeukError):
+        tb.Pipeline(config)
+
+
+@pytest.mark.skipif(cuda_available(), reason="host has a GPU")
+def test_no_cpu_fallback_without_gpu():
+    with pytest.raises(tb.TeukError) as info:
+        tb.Pipeline(CASES["schw_d84"])
+    assert info.value.status == tb.ERR_CUDA
+
+
+def test_cpp_facade_compiles_and_maps_exceptions(tmp_path):
+    exe = tmp_path / "facade_check"
+    subprocess.run(["g++", "-std=c++20", "-O1", "-I", str(REPO / "include"),
+                    str(REPO / "tests" / "cpp" / "facade_check.cpp"),
+                    str(tb.LIBRARY_PATH), f"-Wl,-rpath,{tb.LIBRARY_PATH.parent}",
+                    "-o", str(exe)], check=True)
+    run = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert run.stdout.count("invalid_argument:") == 2
+    expected = 0 if cuda_available() else 3
+    assert run.returncode == expected, run.stdout + run.stderr

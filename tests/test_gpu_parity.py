@@ -156,7 +156,8 @@ def test_device_pointers_round_trip(require_gpu):
     gpu.get_state(dev)
     assert np.array_equal(dev.cpu().numpy(), host)
     gpu.set_state(dev)
-    assert relative_error(gpu.get_state(), host) < 1e-14
+    # nodal -> band -> nodal applies S A once more: ~1e-14 rounding
+    assert relative_error(gpu.get_state(), host) < 1e-12
     rhs_dev = torch.zeros_like(dev)
     gpu.evaluate_rhs(dev, rhs_dev)
     rhs_host = gpu.evaluate_rhs(host)

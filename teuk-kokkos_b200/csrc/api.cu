@@ -139,7 +139,7 @@ struct DeviceArray {
   ~DeviceArray() { release(); }
 };
 
-constexpr int kTargetTileRows = 64;
+constexpr int kTargetTileRows = 48;
 constexpr size_t kSmemBudget = 200 * 1024;
 
 int slab_halo(const int disc, const int reduction) {
@@ -195,12 +195,16 @@ struct Batch {
       throw std::invalid_argument("a batch needs at least one solve");
     }
     for (const Config& c : configs) {
+      // The reference's construction-time validation runs first, so invalid
+      // inputs report the same error whatever their source policy.
+      plans.push_back(build_instance_plan(c));
+    }
+    for (const Config& c : configs) {
       if (c.source_mode != 0) {
         throw Unsupported(
             "second-order source policies are not built on the B200 path; "
             "only the linear (disabled) pipeline runs here");
       }
-      plans.push_back(build_instance_plan(c));
     }
     int device_count = 0;
     check(cudaGetDeviceCount(&device_count), "cudaGetDeviceCount");
@@ -278,7 +282,7 @@ struct Batch {
           if (in.disc != disc || in.reduction != red) continue;
           const int ne = h_seg[s].n_ell;
           const int nr = in.nr;
-          int rows = std::min(kTargetTileRows, std::max(16, 1024 / ne));
+          int rows = std::min(kTargetTileRows, std::max(16, 720 / ne));
           int tiles = (nr + rows - 1) / rows;
           tiles = std::max(1, std::min(tiles, nr / 16));
           for (int t = 0; t < tiles; ++t) {

@@ -27,7 +27,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kCoefCount = 9;
+constexpr int kCoefCount = 10;
 
 template <int DISC>
 struct DiscTraits;
@@ -81,6 +81,7 @@ __device__ void row_coefficients(const InstanceDesc& in, const int m,
   out[6] = -(2.0 * a * mm * R2 / L2);
   out[7] = -2.0 * R * ((1.0 + s) * M / L2 - a2 * R / L4);
   out[8] = -(2.0 * a * mm * R / L2);
+  out[9] = 1.0 / out[0];
 }
 
 // h * (D v)(r): v(q) = base[(q - s0) * stride], q in the resident slab.
@@ -145,14 +146,262 @@ __device__ __forceinline__ double2 sbp_dissipation(const double2* base,
   return acc;
 }
 
+// Shared-memory geometry of one launch group (padded strides chosen so the
+// 8x4 / 4x8 fragment loads of the FP64 MMA hit 32 distinct banks).
+struct SmemLayout {
+  int ne4, ne8, nt4, nt8;  // padded ell / theta extents
+  int xs;                  // stride of the per-warp band staging rows
+  int ts;                  // stride of the per-warp nodal staging columns
+  int ss;                  // synthesis matrix row stride
+  int as;                  // analysis matrix row stride
+  __host__ __device__ static int round_up(const int v, const int m) {
+    return (v + m - 1) / m * m;
+  }
+  __host__ __device__ static int bank_stride(const int v) {
+    return 16 * ((v + 15) / 16) + 4;
+  }
+  __host__ __device__ explicit SmemLayout(const StageLaunch& p) {
+    ne4 = round_up(p.max_ell, 4);
+    ne8 = round_up(p.max_ell, 8);
+    nt4 = round_up(p.max_theta, 4);
+    nt8 = round_up(p.max_theta, 8);
+    xs = bank_stride(ne4);
+    ts = bank_stride(nt8);
+    ss = bank_stride(ne4);
+    as = bank_stride(nt4);
+  }
+  // double counts
+  __host__ __device__ int warp_x() const { return 16 * xs; }
+  __host__ __device__ int warp_t() const { return 8 * ts; }
+  __host__ __device__ int synthesis() const { return nt8 * ss; }
+  __host__ __device__ int analysis() const { return ne8 * as; }
+};
+
+// D = A * B + D for one 8x8x4 FP64 tile (mma.sync m8n8k4, FP64 tensor path).
+__device__ __forceinline__ void dmma(double& c0, double& c1, const double a,
+                                     const double b) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, "
+      "{%0,%1};\n"
+      : "+d"(c0), "+d"(c1)
+      : "d"(a), "d"(b));
+}
+
+// psi_t = A diag(1/C_T) S (P + 2K Q - G0 psi) - i A diag(2 s a cos/C_T) S psi
+// for rows [t0, t1) of one tile, four rows per warp iteration:
+//   synthesis  C(j, col) = S(j, l) X(l, col), col = (row, {v1.re, v1.im,
+//              psi.re, psi.im})            -> pointwise t_j on the nodes
+//   analysis   psi_t(l, col2) = A(l, j) T(j, col2), col2 = (row, re/im).
+__device__ void psi_t_transforms(const SmemLayout& L, const int ne,
+                                 const int nt, const int t0, const int t1,
+                                 const double2* u, const int s0, const int rs,
+                                 const double2* qcol, const int qstride,
+                                 const int qbase, const double* coef,
+                                 const double* Sm, const double* Am,
+                                 const double* sinv, const double* cosv,
+                                 const double spin, double* xw, double* tw,
+                                 double2* psit, const int warp,
+                                 const int lane) {
+  const double a2 = spin * spin;
+  const double sa2 = 2.0 * (static_cast<double>(kSpinWeight) * spin);
+  const int rows = t1 - t0;
+  const int quad = lane & 3;
+  const int group = lane >> 2;
+  for (int b0 = warp * 4; b0 < rows; b0 += kWarps * 4) {
+    // stage the band vectors of four rows: v1 = P + 2K Q - G0 psi, psi
+    for (int idx = lane; idx < 4 * L.ne4; idx += 32) {
+      const int rho = idx / L.ne4;
+      const int l = idx - rho * L.ne4;
+      const int rr = b0 + rho;
+      double2 v1 = make_double2(0.0, 0.0), psi = make_double2(0.0, 0.0);
+      if (rr < rows && l < ne) {
+        const int r = t0 + rr;
+        const double* cf = coef + rr * kCoefCount;
+        const double2* row = u + (r - s0) * rs;
+        const double2 Q = qcol[(r - qbase) * qstride + l];
+        psi = row[2 * ne + l];
+        v1 = csub(cadd(row[l], cscale(2.0 * cf[1], Q)),
+                  cmul(make_double2(cf[3], cf[4]), psi));
+      }
+      xw[(rho * 4 + 0) * L.xs + l] = v1.x;
+      xw[(rho * 4 + 1) * L.xs + l] = v1.y;
+      xw[(rho * 4 + 2) * L.xs + l] = psi.x;
+      xw[(rho * 4 + 3) * L.xs + l] = psi.y;
+    }
+    __syncwarp();
+    // synthesis on the nodes and the pointwise Kerr factor
+    for (int mt = 0; mt < L.nt8 / 8; ++mt) {
+      double acc[2][2];
+#pragma unroll
+      for (int n = 0; n < 2; ++n) acc[n][0] = acc[n][1] = 0.0;
+      for (int ks = 0; ks < L.ne4 / 4; ++ks) {
+        const double a = Sm[(mt * 8 + group) * L.ss + ks * 4 + quad];
+#pragma unroll
+        for (int n = 0; n < 2; ++n) {
+          const double b = xw[(n * 8 + group) * L.xs + ks * 4 + quad];
+          dmma(acc[n][0], acc[n][1], a, b);
+        }
+      }
+      const int j = mt * 8 + group;
+      // 1 / C_T for the two rows this lane finishes, issued before the
+      // shuffles so the reciprocals overlap them
+      double inv[2], gam = 0.0;
+      const bool node = j < nt;
+      if (node) gam = sa2 * cosv[j];
+#pragma unroll
+      for (int n = 0; n < 2; ++n) {
+        const int rr = b0 + 2 * n + (quad >> 1);
+        inv[n] = 0.0;
+        if (rr < rows && node) {
+          inv[n] = 1.0 / (coef[rr * kCoefCount] - a2 * sinv[j] * sinv[j]);
+        }
+      }
+#pragma unroll
+      for (int n = 0; n < 2; ++n) {
+        // lane quad 0/2 holds a_j of a row, quad 1/3 holds b_j of that row
+        const double o0 = __shfl_xor_sync(0xffffffffu, acc[n][0], 1);
+        const double o1 = __shfl_xor_sync(0xffffffffu, acc[n][1], 1);
+        if ((quad & 1) == 0) {
+          const int rho = 2 * n + (quad >> 1);
+          tw[(rho * 2 + 0) * L.ts + j] = (acc[n][0] + gam * o1) * inv[n];
+          tw[(rho * 2 + 1) * L.ts + j] = (acc[n][1] - gam * o0) * inv[n];
+        }
+      }
+    }
+    __syncwarp();
+    // analysis back onto the band
+    for (int mt = 0; mt < L.ne8 / 8; ++mt) {
+      // two accumulator pairs (even / odd K steps) halve the MMA chain
+      double c0 = 0.0, c1 = 0.0, d0 = 0.0, d1 = 0.0;
+      const int ksteps = L.nt4 / 4;
+      int ks = 0;
+      for (; ks + 1 < ksteps; ks += 2) {
+        const double a = Am[(mt * 8 + group) * L.as + ks * 4 + quad];
+        const double b = tw[group * L.ts + ks * 4 + quad];
+        const double a2n = Am[(mt * 8 + group) * L.as + ks * 4 + 4 + quad];
+        const double b2n = tw[group * L.ts + ks * 4 + 4 + quad];
+        dmma(c0, c1, a, b);
+        dmma(d0, d1, a2n, b2n);
+      }
+      if (ks < ksteps) {
+        const double a = Am[(mt * 8 + group) * L.as + ks * 4 + quad];
+        const double b = tw[group * L.ts + ks * 4 + quad];
+        dmma(c0, c1, a, b);
+      }
+      c0 += d0;
+      c1 += d1;
+      const int l = mt * 8 + group;
+      const int rr = b0 + quad;
+      if (rr < rows && l < ne) psit[rr * ne + l] = make_double2(c0, c1);
+    }
+    __syncwarp();
+  }
+}
+
+// The same psi_t on the FP64 CUDA cores: one warp per row, lanes over the
+// Gauss-Legendre nodes for the synthesis and over ell for the analysis.
+__device__ void psi_t_scalar(const SmemLayout& L, const int ne, const int nt,
+                             const int t0, const int t1, const double2* u,
+                             const int s0, const int rs, const double2* qcol,
+                             const int qstride, const int qbase,
+                             const double* coef, const double* Sm,
+                             const double* Am, const double* sinv,
+                             const double* cosv, const double spin,
+                             double* xw, double* tw, double2* psit,
+                             const int warp, const int lane) {
+  const double a2 = spin * spin;
+  const double sa2 = 2.0 * (static_cast<double>(kSpinWeight) * spin);
+  double2* v1 = reinterpret_cast<double2*>(xw);
+  double2* tj = reinterpret_cast<double2*>(tw);
+  for (int rr = warp; rr < t1 - t0; rr += kWarps) {
+    const int r = t0 + rr;
+    const double* cf = coef + rr * kCoefCount;
+    const double2* row = u + (r - s0) * rs;
+    const double2 G0 = make_double2(cf[3], cf[4]);
+    for (int l = lane; l < ne; l += 32) {
+      const double2 Q = qcol[(r - qbase) * qstride + l];
+      v1[l] = csub(cadd(row[l], cscale(2.0 * cf[1], Q)),
+                   cmul(G0, row[2 * ne + l]));
+    }
+    __syncwarp();
+    for (int j = lane; j < nt; j += 32) {
+      double2 sa = make_double2(0.0, 0.0);
+      double2 sb = make_double2(0.0, 0.0);
+      for (int l = 0; l < ne; ++l) {
+        const double s = Sm[j * L.ss + l];
+        sa = cfma(s, v1[l], sa);
+        sb = cfma(s, row[2 * ne + l], sb);
+      }
+      const double gamma = sa2 * cosv[j];
+      const double ct = cf[0] - a2 * sinv[j] * sinv[j];
+      tj[j] = make_double2((sa.x + gamma * sb.y) / ct,
+                           (sa.y - gamma * sb.x) / ct);
+    }
+    __syncwarp();
+    for (int l = lane; l < ne; l += 32) {
+      double2 acc = make_double2(0.0, 0.0);
+      for (int j = 0; j < nt; ++j) acc = cfma(Am[l * L.as + j], tj[j], acc);
+      psit[rr * ne + l] = acc;
+    }
+    __syncwarp();
+  }
+}
+
+#ifndef TEUK_TRANSFORM_MMA
+#define TEUK_TRANSFORM_MMA 1
+#endif
+
+// Register window of RB output rows plus a halo of H rows on each side.
+template <int RB, int H>
+__device__ __forceinline__ void load_window(double2 (&w)[RB + 2 * H],
+                                            const double2* col,
+                                            const int stride, const int base,
+                                            const int ra) {
+#pragma unroll
+  for (int i = 0; i < RB + 2 * H; ++i) {
+    w[i] = col[(ra - H + i - base) * stride];
+  }
+}
+
+template <int DISC, int RB, int H>
+__device__ __forceinline__ double2 window_derivative(
+    const double2 (&w)[RB + 2 * H], const int i) {
+  using T = DiscTraits<DISC>;
+  double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+  for (int k = T::HALF; k >= 1; --k) {
+    acc = cfma(c_sbp.interior[DISC][k], csub(w[i + H + k], w[i + H - k]), acc);
+  }
+  return acc;
+}
+
+template <int DISC, int RB, int H>
+__device__ __forceinline__ double2 window_dissipation(
+    const double2 (&w)[RB + 2 * H], const int i) {
+  using T = DiscTraits<DISC>;
+  double2 acc = cscale(c_sbp.diss_interior[DISC][0], w[i + H]);
+#pragma unroll
+  for (int k = 1; k <= T::P; ++k) {
+    acc = cfma(c_sbp.diss_interior[DISC][k], cadd(w[i + H + k], w[i + H - k]),
+               acc);
+  }
+  return acc;
+}
+
+#ifndef TEUK_ROW_BLOCK
+#define TEUK_ROW_BLOCK 2
+#endif
+constexpr int kRowBlock = TEUK_ROW_BLOCK;
+
 template <int DISC, int SC>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
     stage_kernel(const StageLaunch p) {
   using T = DiscTraits<DISC>;
   extern __shared__ double2 smem[];
   const TileDesc tile = p.tiles[blockIdx.x];
   const SegmentDesc seg = p.segments[tile.segment];
   const InstanceDesc in = p.instances[seg.instance];
+  const SmemLayout L(p);
   const int nr = in.nr;
   const int ne = seg.n_ell;
   const int nt = in.ntheta;
@@ -166,15 +415,17 @@ __global__ void __launch_bounds__(kThreads)
   const int lane = tid & 31;
   const int warp = tid >> 5;
 
-  double2* u = smem;                                   // slab rows x rs
-  double2* psit = u + p.slab_capacity;                 // t-rows x ne
-  double2* qeff = psit + p.dslab_capacity;             // t-rows x ne (SC)
-  double2* wbuf = qeff + (SC ? p.dslab_capacity : 0);  // warps x (nt + ne)
-  double* St = reinterpret_cast<double*>(wbuf + kWarps * (p.max_theta + p.max_ell));
-  double* At = St + p.matrix_capacity;
-  double* sinv = At + p.matrix_capacity;
-  double* cosv = sinv + p.max_theta;
-  double* coef = cosv + p.max_theta;  // t-rows x kCoefCount
+  double2* u = smem;                        // slab rows x rs
+  double2* psit = u + p.slab_capacity;      // t-rows x ne
+  double2* qeff = psit + p.dslab_capacity;  // t-rows x ne (SC)
+  double* dbase = reinterpret_cast<double*>(qeff + (SC ? p.dslab_capacity : 0));
+  double* xw = dbase + warp * (L.warp_x() + L.warp_t());
+  double* tw = xw + L.warp_x();
+  double* Sm = dbase + kWarps * (L.warp_x() + L.warp_t());
+  double* Am = Sm + L.synthesis();
+  double* sinv = Am + L.analysis();
+  double* cosv = sinv + L.nt8;
+  double* coef = cosv + L.nt8;  // t-rows x kCoefCount
 
   // ---- phase 0: RK stage input over the slab, matrices, coefficients
   {
@@ -182,28 +433,62 @@ __global__ void __launch_bounds__(kThreads)
     const int count = (s1 - s0) * rs;
     const double hdt = 0.5 * in.dt;
     const double2* __restrict__ y = p.y + base;
-    if (p.stage == kStage1 || p.stage == kRhsOnly) {
-      for (int i = tid; i < count; i += kThreads) u[i] = __ldg(y + i);
-    } else if (p.stage == kStage4) {
-      const double2* __restrict__ k = p.kA + base;
-      for (int i = tid; i < count; i += kThreads) u[i] = __ldg(k + i);
+    constexpr int U = 4;
+    if (p.stage == kStage1 || p.stage == kRhsOnly || p.stage == kStage4) {
+      const double2* __restrict__ src = p.stage == kStage4 ? p.kA + base : y;
+      for (int i0 = tid; i0 < count; i0 += kThreads * U) {
+        double2 v[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+          const int i = i0 + k * kThreads;
+          if (i < count) v[k] = __ldg(src + i);
+        }
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+          const int i = i0 + k * kThreads;
+          if (i < count) u[i] = v[k];
+        }
+      }
     } else {
-      const double2* __restrict__ k = (p.stage == kStage2 ? p.kA : p.kB) + base;
-      for (int i = tid; i < count; i += kThreads) {
-        const double2 yv = __ldg(y + i);
-        const double2 kv = __ldg(k + i);
-        u[i] = make_double2(yv.x + hdt * kv.x, yv.y + hdt * kv.y);
+      const double2* __restrict__ kk =
+          (p.stage == kStage2 ? p.kA : p.kB) + base;
+      for (int i0 = tid; i0 < count; i0 += kThreads * U) {
+        double2 yv[U], kv[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+          const int i = i0 + k * kThreads;
+          if (i < count) {
+            yv[k] = __ldg(y + i);
+            kv[k] = __ldg(kk + i);
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+          const int i = i0 + k * kThreads;
+          if (i < count) {
+            u[i] = make_double2(yv[k].x + hdt * kv[k].x,
+                                yv[k].y + hdt * kv[k].y);
+          }
+        }
       }
     }
-    const double* S = p.matrices + seg.mat_offset;  // St[l][j]
-    const double* A = S + ne * nt;                  // At[j][l]
-    for (int i = tid; i < ne * nt; i += kThreads) {
-      St[i] = S[i];
-      At[i] = A[i];
-    }
-    for (int j = tid; j < nt; j += kThreads) {
-      sinv[j] = p.trig[in.trig_offset + j];
-      cosv[j] = p.trig[in.trig_offset + nt + j];
+    if (in.spin != 0.0) {
+      const double* S = p.matrices + seg.mat_offset;  // St[l][j]
+      const double* A = S + ne * nt;                  // At[j][l]
+      for (int i = tid; i < L.nt8 * L.ne4; i += kThreads) {
+        const int j = i / L.ne4, l = i - (i / L.ne4) * L.ne4;
+        Sm[j * L.ss + l] = (j < nt && l < ne) ? S[l * nt + j] : 0.0;
+      }
+      for (int i = tid; i < L.ne8 * L.nt4; i += kThreads) {
+        const int l = i / L.nt4, j = i - (i / L.nt4) * L.nt4;
+        Am[l * L.as + j] = (j < nt && l < ne) ? A[j * ne + l] : 0.0;
+      }
+      for (int j = tid; j < L.nt8; j += kThreads) {
+        sinv[j] = j < nt ? p.trig[in.trig_offset + j] : 0.0;
+        cosv[j] = j < nt ? p.trig[in.trig_offset + nt + j] : 0.0;
+      }
+      // zero the nodal staging columns beyond the analysis K extent
+      for (int i = lane; i < L.warp_t(); i += 32) tw[i] = 0.0;
     }
     for (int r = t0 + tid; r < t1; r += kThreads) {
       row_coefficients(in, seg.m, r, coef + (r - t0) * kCoefCount);
@@ -232,8 +517,7 @@ __global__ void __launch_bounds__(kThreads)
   }
 
   // ---- phase 1: psi_t on rows [t0, t1)
-  const double a = in.spin;
-  if (a == 0.0) {
+  if (in.spin == 0.0) {
     for (int i = tid; i < (t1 - t0) * ne; i += kThreads) {
       const int rr = i / ne;
       const int l = i - rr * ne;
@@ -244,113 +528,187 @@ __global__ void __launch_bounds__(kThreads)
       const double2 psi = u[(r - s0) * rs + 2 * ne + l];
       const double2 G = make_double2(cf[3], cf[4]);
       const double2 num = csub(cadd(P, cscale(2.0 * cf[1], Q)), cmul(G, psi));
-      psit[i] = make_double2(num.x / cf[0], num.y / cf[0]);
+      psit[i] = cscale(cf[9], num);
     }
+  } else if (TEUK_TRANSFORM_MMA) {
+    psi_t_transforms(L, ne, nt, t0, t1, u, s0, rs, qcol, qstride, qbase, coef,
+                     Sm, Am, sinv, cosv, in.spin, xw, tw, psit, warp, lane);
   } else {
-    double2* v1 = wbuf + warp * (p.max_theta + p.max_ell);
-    double2* tj = v1 + p.max_ell;
-    const double a2 = a * a;
-    const double sa2 = 2.0 * (static_cast<double>(kSpinWeight) * a);
-    for (int rr = warp; rr < t1 - t0; rr += kWarps) {
-      const int r = t0 + rr;
-      const double* cf = coef + rr * kCoefCount;
-      const double2* row = u + (r - s0) * rs;
-      const double2 G0 = make_double2(cf[3], cf[4]);
-      for (int l = lane; l < ne; l += 32) {
-        const double2 Q = qcol[(r - qbase) * qstride + l];
-        v1[l] = csub(cadd(row[l], cscale(2.0 * cf[1], Q)),
-                     cmul(G0, row[2 * ne + l]));
-      }
-      __syncwarp();
-      for (int j = lane; j < nt; j += 32) {
-        double2 sa = make_double2(0.0, 0.0);
-        double2 sb = make_double2(0.0, 0.0);
-        for (int l = 0; l < ne; ++l) {
-          const double s = St[l * nt + j];
-          sa = cfma(s, v1[l], sa);
-          sb = cfma(s, row[2 * ne + l], sb);
-        }
-        // t_j = (a_j - i gamma_j b_j) / C_T_j, gamma_j = 2 s a cos(theta_j)
-        const double gamma = sa2 * cosv[j];
-        const double ct = cf[0] - a2 * sinv[j] * sinv[j];
-        tj[j] = make_double2((sa.x + gamma * sb.y) / ct,
-                             (sa.y - gamma * sb.x) / ct);
-      }
-      __syncwarp();
-      for (int l = lane; l < ne; l += 32) {
-        double2 acc = make_double2(0.0, 0.0);
-        for (int j = 0; j < nt; ++j) acc = cfma(At[j * ne + l], tj[j], acc);
-        psit[rr * ne + l] = acc;
-      }
-      __syncwarp();
-    }
+    psi_t_scalar(L, ne, nt, t0, t1, u, s0, rs, qcol, qstride, qbase, coef, Sm,
+                 Am, sinv, cosv, in.spin, xw, tw, psit, warp, lane);
   }
   __syncthreads();
 
   // ---- phase 2: RHS assembly and RK update on rows [r0, r1)
   const double inv_h = in.inv_spacing;
   const double diss_scale = in.dissipation * inv_h;
+  const bool dissipate = in.dissipation > 0.0;
   const double damping = in.damping;
   const double dt = in.dt;
   const double dt6 = in.dt / 6.0;
-  const int items = (r1 - r0) * ne;
-  for (int i = tid; i < items; i += kThreads) {
-    const int rr = i / ne;
-    const int l = i - rr * ne;
-    const int r = r0 + rr;
-    const double* cf = coef + (r - t0) * kCoefCount;
-    const double2* urow = u + (r - s0) * rs;
-    const double2 Qs = urow[ne + l];
-    const double2 psi = urow[2 * ne + l];
-    const double2 Qe = qcol[(r - qbase) * qstride + l];
-    const double2 dpsi =
-        cscale(inv_h, sbp_derivative<DISC>(u + 2 * ne + l, rs, s0, r, nr));
-    const double2 dq = cscale(inv_h, sbp_derivative<DISC>(qcol + l, qstride,
-                                                          qbase, r, nr));
-    const double2 dpsit =
-        cscale(inv_h, sbp_derivative<DISC>(psit + l, ne, t0, r, nr));
+  const int chunks = (r1 - r0 + kRowBlock - 1) / kRowBlock;
+  for (int item = tid; item < chunks * ne; item += kThreads) {
+    const int chunk = item / ne;
+    const int l = item - chunk * ne;
+    const int ra = r0 + chunk * kRowBlock;
+    const int rows = min(kRowBlock, r1 - ra);
     const int ell = seg.ell_min + l;
     const double lambda = -static_cast<double>((ell - kSpinWeight) *
                                                (ell + kSpinWeight + 1));
-    double2 kP = cscale(cf[2], dq);
-    kP = cadd(kP, cmul(make_double2(cf[5], cf[6]), Qe));
-    kP = cadd(kP, cmul(make_double2(cf[7], cf[8]), psi));
-    kP = cadd(kP, cscale(lambda, psi));
-    double2 kQ = csub(dpsit, cscale(damping, csub(Qs, dpsi)));
-    double2 kpsi = psit[(r - t0) * ne + l];
-    if (in.dissipation > 0.0) {
-      kP = cfma(diss_scale, sbp_dissipation<DISC>(u + l, rs, s0, r, nr), kP);
-      kQ = cfma(diss_scale, sbp_dissipation<DISC>(u + ne + l, rs, s0, r, nr),
-                kQ);
-      kpsi = cfma(diss_scale,
-                  sbp_dissipation<DISC>(u + 2 * ne + l, rs, s0, r, nr), kpsi);
-    }
-    const long long g = seg.offset + static_cast<long long>(r) * rs + l;
-    const double2 k[3] = {kP, kQ, kpsi};
+    double2 kP[kRowBlock], kQ[kRowBlock], kpsi[kRowBlock];
+    const bool interior =
+        rows == kRowBlock && ra >= T::BR && ra + kRowBlock + T::BR <= nr;
+    if (interior) {
+      {  // psi: D psi (constraint), dissipation, (c_psi + lambda) psi
+        double2 w[kRowBlock + 2 * T::P];
+        load_window<kRowBlock, T::P>(w, u + 2 * ne + l, rs, s0, ra);
 #pragma unroll
-    for (int f = 0; f < 3; ++f) {
-      const long long gi = g + f * ne;
-      switch (p.stage) {
-        case kStage1:
-        case kRhsOnly:
-          p.kA[gi] = k[f];
-          break;
-        case kStage2: {
-          const double2 k1 = p.kA[gi];
-          p.kB[gi] = k[f];
-          p.acc[gi] = cfma(2.0, k[f], k1);
-          break;
+        for (int i = 0; i < kRowBlock; ++i) {
+          const double* cf = coef + (ra + i - t0) * kCoefCount;
+          const double2 dpsi =
+              cscale(inv_h, window_derivative<DISC, kRowBlock, T::P>(w, i));
+          kQ[i] = cscale(damping, dpsi);
+          kpsi[i] = dissipate
+                        ? cscale(diss_scale,
+                                 window_dissipation<DISC, kRowBlock, T::P>(w, i))
+                        : make_double2(0.0, 0.0);
+          const double2 psi = w[i + T::P];
+          kP[i] = cadd(cmul(make_double2(cf[7], cf[8]), psi),
+                       cscale(lambda, psi));
         }
-        case kStage3: {
-          const double2 yv = p.y[gi];
-          const double2 acc = cfma(2.0, k[f], p.acc[gi]);
-          p.acc[gi] = cfma(dt6, acc, yv);
-          p.kA[gi] = cfma(dt, k[f], yv);
-          break;
+      }
+      {  // Q: -gamma Q, dissipation; free-damped: H_R D Q + q Q
+        double2 w[kRowBlock + 2 * T::P];
+        load_window<kRowBlock, T::P>(w, u + ne + l, rs, s0, ra);
+#pragma unroll
+        for (int i = 0; i < kRowBlock; ++i) {
+          const double* cf = coef + (ra + i - t0) * kCoefCount;
+          const double2 Q = w[i + T::P];
+          kQ[i] = csub(kQ[i], cscale(damping, Q));
+          if (dissipate) {
+            kQ[i] = cfma(diss_scale,
+                         window_dissipation<DISC, kRowBlock, T::P>(w, i),
+                         kQ[i]);
+          }
+          if (!SC) {
+            const double2 dq =
+                cscale(inv_h, window_derivative<DISC, kRowBlock, T::P>(w, i));
+            kP[i] = cadd(kP[i], cscale(cf[2], dq));
+            kP[i] = cadd(kP[i], cmul(make_double2(cf[5], cf[6]), Q));
+          }
         }
-        case kStage4:
-          p.y[gi] = cfma(dt6, k[f], p.acc[gi]);
-          break;
+      }
+      if (SC) {  // stage-constrained effective Q = D psi
+        double2 w[kRowBlock + 2 * T::HALF];
+        load_window<kRowBlock, T::HALF>(w, qeff + l, ne, t0, ra);
+#pragma unroll
+        for (int i = 0; i < kRowBlock; ++i) {
+          const double* cf = coef + (ra + i - t0) * kCoefCount;
+          const double2 dq = cscale(
+              inv_h, window_derivative<DISC, kRowBlock, T::HALF>(w, i));
+          kP[i] = cadd(kP[i], cscale(cf[2], dq));
+          kP[i] = cadd(kP[i], cmul(make_double2(cf[5], cf[6]), w[i + T::HALF]));
+        }
+      }
+      if (dissipate) {  // P: dissipation only
+        double2 w[kRowBlock + 2 * T::P];
+        load_window<kRowBlock, T::P>(w, u + l, rs, s0, ra);
+#pragma unroll
+        for (int i = 0; i < kRowBlock; ++i) {
+          kP[i] = cfma(diss_scale,
+                       window_dissipation<DISC, kRowBlock, T::P>(w, i), kP[i]);
+        }
+      }
+      {  // psi_t: D psi_t into Q_t, psi_t itself
+        double2 w[kRowBlock + 2 * T::HALF];
+        load_window<kRowBlock, T::HALF>(w, psit + l, ne, t0, ra);
+#pragma unroll
+        for (int i = 0; i < kRowBlock; ++i) {
+          kQ[i] = cadd(kQ[i], cscale(inv_h, window_derivative<DISC, kRowBlock,
+                                                              T::HALF>(w, i)));
+          kpsi[i] = cadd(kpsi[i], w[i + T::HALF]);
+        }
+      }
+    } else {
+      for (int i = 0; i < rows; ++i) {
+        const int r = ra + i;
+        const double* cf = coef + (r - t0) * kCoefCount;
+        const double2* urow = u + (r - s0) * rs;
+        const double2 Qs = urow[ne + l];
+        const double2 psi = urow[2 * ne + l];
+        const double2 Qe = qcol[(r - qbase) * qstride + l];
+        const double2 dpsi =
+            cscale(inv_h, sbp_derivative<DISC>(u + 2 * ne + l, rs, s0, r, nr));
+        const double2 dq = cscale(
+            inv_h, sbp_derivative<DISC>(qcol + l, qstride, qbase, r, nr));
+        const double2 dpsit =
+            cscale(inv_h, sbp_derivative<DISC>(psit + l, ne, t0, r, nr));
+        double2 P_t = cscale(cf[2], dq);
+        P_t = cadd(P_t, cmul(make_double2(cf[5], cf[6]), Qe));
+        P_t = cadd(P_t, cmul(make_double2(cf[7], cf[8]), psi));
+        P_t = cadd(P_t, cscale(lambda, psi));
+        double2 Q_t = csub(dpsit, cscale(damping, csub(Qs, dpsi)));
+        double2 psi_t = psit[(r - t0) * ne + l];
+        if (dissipate) {
+          P_t = cfma(diss_scale, sbp_dissipation<DISC>(u + l, rs, s0, r, nr),
+                     P_t);
+          Q_t = cfma(diss_scale,
+                     sbp_dissipation<DISC>(u + ne + l, rs, s0, r, nr), Q_t);
+          psi_t = cfma(diss_scale,
+                       sbp_dissipation<DISC>(u + 2 * ne + l, rs, s0, r, nr),
+                       psi_t);
+        }
+        kP[i] = P_t;
+        kQ[i] = Q_t;
+        kpsi[i] = psi_t;
+      }
+    }
+    // RK update: every own-row input is loaded before any store so the
+    // global loads are in flight together.
+    const long long g0 = seg.offset + static_cast<long long>(ra) * rs + l;
+    double2 in0[kRowBlock][3], in1[kRowBlock][3];
+    const double2* __restrict__ src0 =
+        p.stage == kStage2 ? p.kA : (p.stage == kStage3 ? p.y : p.acc);
+    const double2* __restrict__ src1 = p.acc;
+#pragma unroll
+    for (int i = 0; i < kRowBlock; ++i) {
+#pragma unroll
+      for (int f = 0; f < 3; ++f) {
+        in0[i][f] = make_double2(0.0, 0.0);
+        in1[i][f] = make_double2(0.0, 0.0);
+        if (i < rows && p.stage != kStage1 && p.stage != kRhsOnly) {
+          const long long gi = g0 + static_cast<long long>(i) * rs + f * ne;
+          in0[i][f] = src0[gi];
+          if (p.stage == kStage3) in1[i][f] = src1[gi];
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < kRowBlock; ++i) {
+      if (i >= rows) break;
+      const double2 k[3] = {kP[i], kQ[i], kpsi[i]};
+#pragma unroll
+      for (int f = 0; f < 3; ++f) {
+        const long long gi = g0 + static_cast<long long>(i) * rs + f * ne;
+        switch (p.stage) {
+          case kStage1:
+          case kRhsOnly:
+            p.kA[gi] = k[f];
+            break;
+          case kStage2:  // in0 = k1
+            p.kB[gi] = k[f];
+            p.acc[gi] = cfma(2.0, k[f], in0[i][f]);
+            break;
+          case kStage3: {  // in0 = y, in1 = k1 + 2 k2
+            const double2 acc = cfma(2.0, k[f], in1[i][f]);
+            p.acc[gi] = cfma(dt6, acc, in0[i][f]);
+            p.kA[gi] = cfma(dt, k[f], in0[i][f]);
+            break;
+          }
+          case kStage4:  // in0 = y + dt/6 (k1 + 2 k2 + 2 k3)
+            p.y[gi] = cfma(dt6, k[f], in0[i][f]);
+            break;
+        }
       }
     }
   }
@@ -476,13 +834,15 @@ __global__ void endpoint_gather_kernel(const double2* y,
 }  // namespace
 
 size_t stage_smem_bytes(const StageLaunch& p) {
+  const SmemLayout L(p);
   const size_t complex_count =
       static_cast<size_t>(p.slab_capacity) +
-      static_cast<size_t>(p.dslab_capacity) * (p.reduction == 1 ? 2 : 1) +
-      static_cast<size_t>(kWarps) * (p.max_theta + p.max_ell);
-  const size_t double_count = 2 * static_cast<size_t>(p.matrix_capacity) +
-                              2 * static_cast<size_t>(p.max_theta) +
-                              static_cast<size_t>(p.coef_rows) * kCoefCount;
+      static_cast<size_t>(p.dslab_capacity) * (p.reduction == 1 ? 2 : 1);
+  const size_t double_count =
+      static_cast<size_t>(kWarps) * (L.warp_x() + L.warp_t()) +
+      static_cast<size_t>(L.synthesis() + L.analysis()) +
+      2 * static_cast<size_t>(L.nt8) +
+      static_cast<size_t>(p.coef_rows) * kCoefCount;
   return complex_count * sizeof(double2) + double_count * sizeof(double);
 }
 

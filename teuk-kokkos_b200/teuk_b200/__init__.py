@@ -18,8 +18,13 @@ from typing import Iterable, Sequence
 
 import numpy as np
 
+import os
+
 _PACKAGE = Path(__file__).resolve().parent.parent
-LIBRARY_PATH = _PACKAGE / "lib" / "libteuk_b200.so"
+# TEUK_B200_LIBRARY selects another build of the same C ABI (for A/B timing
+# of build variants); the default is the in-tree library.
+LIBRARY_PATH = Path(os.environ.get("TEUK_B200_LIBRARY",
+                                   _PACKAGE / "lib" / "libteuk_b200.so"))
 
 OK = 0
 ERR_INVALID_ARGUMENT = -1
