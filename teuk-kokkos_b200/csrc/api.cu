@@ -140,6 +140,7 @@ struct DeviceArray {
 };
 
 constexpr int kTargetTileRows = 48;
+constexpr int kStageRowBlock = 2;  // rows per stage-kernel work item
 constexpr size_t kSmemBudget = 200 * 1024;
 
 int slab_halo(const int disc, const int reduction) {
@@ -282,7 +283,10 @@ struct Batch {
           if (in.disc != disc || in.reduction != red) continue;
           const int ne = h_seg[s].n_ell;
           const int nr = in.nr;
-          int rows = std::min(kTargetTileRows, std::max(16, 720 / ne));
+          // at most one (row pair, ell) work item per thread, so the stage
+          // kernel can park its results and stream the RK update
+          int rows = std::min(kTargetTileRows,
+                              std::max(16, (256 / ne) * kStageRowBlock));
           int tiles = (nr + rows - 1) / rows;
           tiles = std::max(1, std::min(tiles, nr / 16));
           for (int t = 0; t < tiles; ++t) {

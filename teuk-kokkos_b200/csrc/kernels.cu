@@ -298,6 +298,118 @@ __device__ void psi_t_transforms(const SmemLayout& L, const int ne,
   }
 }
 
+// psi_t_transforms for one padded shape known at compile time: the
+// synthesis and analysis A-fragments are loaded once per warp and stay in
+// registers for every row block.
+template <int MTS, int KSS, int MTA, int KSA>
+__device__ void psi_t_transforms_fixed(
+    const SmemLayout& L, const int ne, const int nt, const int t0,
+    const int t1, const double2* u, const int s0, const int rs,
+    const double2* qcol, const int qstride, const int qbase,
+    const double* coef, const double* Sm, const double* Am,
+    const double* sinv, const double* cosv, const double spin, double* xw,
+    double* tw, double2* psit, const int warp, const int lane) {
+  const double a2 = spin * spin;
+  const double sa2 = 2.0 * (static_cast<double>(kSpinWeight) * spin);
+  const int rows = t1 - t0;
+  const int quad = lane & 3;
+  const int group = lane >> 2;
+  double fs[MTS][KSS], fa[MTA][KSA];
+#pragma unroll
+  for (int mt = 0; mt < MTS; ++mt) {
+#pragma unroll
+    for (int ks = 0; ks < KSS; ++ks) {
+      fs[mt][ks] = Sm[(mt * 8 + group) * L.ss + ks * 4 + quad];
+    }
+  }
+#pragma unroll
+  for (int mt = 0; mt < MTA; ++mt) {
+#pragma unroll
+    for (int ks = 0; ks < KSA; ++ks) {
+      fa[mt][ks] = Am[(mt * 8 + group) * L.as + ks * 4 + quad];
+    }
+  }
+  for (int b0 = warp * 4; b0 < rows; b0 += kWarps * 4) {
+    for (int idx = lane; idx < 4 * L.ne4; idx += 32) {
+      const int rho = idx / L.ne4;
+      const int l = idx - rho * L.ne4;
+      const int rr = b0 + rho;
+      double2 v1 = make_double2(0.0, 0.0), psi = make_double2(0.0, 0.0);
+      if (rr < rows && l < ne) {
+        const int r = t0 + rr;
+        const double* cf = coef + rr * kCoefCount;
+        const double2* row = u + (r - s0) * rs;
+        const double2 Q = qcol[(r - qbase) * qstride + l];
+        psi = row[2 * ne + l];
+        v1 = csub(cadd(row[l], cscale(2.0 * cf[1], Q)),
+                  cmul(make_double2(cf[3], cf[4]), psi));
+      }
+      xw[(rho * 4 + 0) * L.xs + l] = v1.x;
+      xw[(rho * 4 + 1) * L.xs + l] = v1.y;
+      xw[(rho * 4 + 2) * L.xs + l] = psi.x;
+      xw[(rho * 4 + 3) * L.xs + l] = psi.y;
+    }
+    __syncwarp();
+    double bx[2][KSS];
+#pragma unroll
+    for (int n = 0; n < 2; ++n) {
+#pragma unroll
+      for (int ks = 0; ks < KSS; ++ks) {
+        bx[n][ks] = xw[(n * 8 + group) * L.xs + ks * 4 + quad];
+      }
+    }
+#pragma unroll
+    for (int mt = 0; mt < MTS; ++mt) {
+      double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+      for (int ks = 0; ks < KSS; ++ks) {
+#pragma unroll
+        for (int n = 0; n < 2; ++n) {
+          dmma(acc[n][0], acc[n][1], fs[mt][ks], bx[n][ks]);
+        }
+      }
+      const int j = mt * 8 + group;
+      double inv[2], gam = 0.0;
+      const bool node = j < nt;
+      if (node) gam = sa2 * cosv[j];
+#pragma unroll
+      for (int n = 0; n < 2; ++n) {
+        const int rr = b0 + 2 * n + (quad >> 1);
+        inv[n] = 0.0;
+        if (rr < rows && node) {
+          inv[n] = 1.0 / (coef[rr * kCoefCount] - a2 * sinv[j] * sinv[j]);
+        }
+      }
+#pragma unroll
+      for (int n = 0; n < 2; ++n) {
+        const double o0 = __shfl_xor_sync(0xffffffffu, acc[n][0], 1);
+        const double o1 = __shfl_xor_sync(0xffffffffu, acc[n][1], 1);
+        if ((quad & 1) == 0) {
+          const int rho = 2 * n + (quad >> 1);
+          tw[(rho * 2 + 0) * L.ts + j] = (acc[n][0] + gam * o1) * inv[n];
+          tw[(rho * 2 + 1) * L.ts + j] = (acc[n][1] - gam * o0) * inv[n];
+        }
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int mt = 0; mt < MTA; ++mt) {
+      double c[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+      for (int ks = 0; ks < KSA; ++ks) {
+        const double b = tw[group * L.ts + ks * 4 + quad];
+        dmma(c[ks & 1][0], c[ks & 1][1], fa[mt][ks], b);
+      }
+      const int l = mt * 8 + group;
+      const int rr = b0 + quad;
+      if (rr < rows && l < ne) {
+        psit[rr * ne + l] = make_double2(c[0][0] + c[1][0], c[0][1] + c[1][1]);
+      }
+    }
+    __syncwarp();
+  }
+}
+
 // The same psi_t on the FP64 CUDA cores: one warp per row, lanes over the
 // Gauss-Legendre nodes for the synthesis and over ell for the analysis.
 __device__ void psi_t_scalar(const SmemLayout& L, const int ne, const int nt,
@@ -433,7 +545,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     const int count = (s1 - s0) * rs;
     const double hdt = 0.5 * in.dt;
     const double2* __restrict__ y = p.y + base;
-    constexpr int U = 4;
+    constexpr int U = 8;
     if (p.stage == kStage1 || p.stage == kRhsOnly || p.stage == kStage4) {
       const double2* __restrict__ src = p.stage == kStage4 ? p.kA + base : y;
       for (int i0 = tid; i0 < count; i0 += kThreads * U) {
@@ -530,6 +642,12 @@ __global__ void __launch_bounds__(kThreads, 2)
       const double2 num = csub(cadd(P, cscale(2.0 * cf[1], Q)), cmul(G, psi));
       psit[i] = cscale(cf[9], num);
     }
+  } else if (TEUK_TRANSFORM_MMA && L.nt8 == 32 && L.ne4 == 16 &&
+             L.ne8 == 16 && L.nt4 == 28) {
+    psi_t_transforms_fixed<4, 4, 2, 7>(L, ne, nt, t0, t1, u, s0, rs, qcol,
+                                       qstride, qbase, coef, Sm, Am, sinv,
+                                       cosv, in.spin, xw, tw, psit, warp,
+                                       lane);
   } else if (TEUK_TRANSFORM_MMA) {
     psi_t_transforms(L, ne, nt, t0, t1, u, s0, rs, qcol, qstride, qbase, coef,
                      Sm, Am, sinv, cosv, in.spin, xw, tw, psit, warp, lane);
@@ -547,166 +665,238 @@ __global__ void __launch_bounds__(kThreads, 2)
   const double dt = in.dt;
   const double dt6 = in.dt / 6.0;
   const int chunks = (r1 - r0 + kRowBlock - 1) / kRowBlock;
-  for (int item = tid; item < chunks * ne; item += kThreads) {
-    const int chunk = item / ne;
-    const int l = item - chunk * ne;
-    const int ra = r0 + chunk * kRowBlock;
-    const int rows = min(kRowBlock, r1 - ra);
-    const int ell = seg.ell_min + l;
-    const double lambda = -static_cast<double>((ell - kSpinWeight) *
-                                               (ell + kSpinWeight + 1));
+  const int items = chunks * ne;
+  // With at most one work item per thread the stage results are parked in
+  // the slab (after every window has read it) and the RK update runs as one
+  // coalesced streaming pass over the tile's rows; otherwise each item
+  // updates its own rows directly.
+  const bool park = items <= kThreads;
+  for (int item0 = 0; item0 < items; item0 += kThreads) {
+    const int item = item0 + tid;
+    const bool active = item < items;
+    int l = 0, ra = r0, rows = 0;
     double2 kP[kRowBlock], kQ[kRowBlock], kpsi[kRowBlock];
-    const bool interior =
-        rows == kRowBlock && ra >= T::BR && ra + kRowBlock + T::BR <= nr;
-    if (interior) {
-      {  // psi: D psi (constraint), dissipation, (c_psi + lambda) psi
-        double2 w[kRowBlock + 2 * T::P];
-        load_window<kRowBlock, T::P>(w, u + 2 * ne + l, rs, s0, ra);
-#pragma unroll
-        for (int i = 0; i < kRowBlock; ++i) {
-          const double* cf = coef + (ra + i - t0) * kCoefCount;
-          const double2 dpsi =
-              cscale(inv_h, window_derivative<DISC, kRowBlock, T::P>(w, i));
-          kQ[i] = cscale(damping, dpsi);
-          kpsi[i] = dissipate
-                        ? cscale(diss_scale,
-                                 window_dissipation<DISC, kRowBlock, T::P>(w, i))
-                        : make_double2(0.0, 0.0);
-          const double2 psi = w[i + T::P];
-          kP[i] = cadd(cmul(make_double2(cf[7], cf[8]), psi),
-                       cscale(lambda, psi));
-        }
-      }
-      {  // Q: -gamma Q, dissipation; free-damped: H_R D Q + q Q
-        double2 w[kRowBlock + 2 * T::P];
-        load_window<kRowBlock, T::P>(w, u + ne + l, rs, s0, ra);
-#pragma unroll
-        for (int i = 0; i < kRowBlock; ++i) {
-          const double* cf = coef + (ra + i - t0) * kCoefCount;
-          const double2 Q = w[i + T::P];
-          kQ[i] = csub(kQ[i], cscale(damping, Q));
-          if (dissipate) {
-            kQ[i] = cfma(diss_scale,
-                         window_dissipation<DISC, kRowBlock, T::P>(w, i),
-                         kQ[i]);
-          }
-          if (!SC) {
-            const double2 dq =
+    if (active) {
+      const int chunk = item / ne;
+      l = item - chunk * ne;
+      ra = r0 + chunk * kRowBlock;
+      rows = min(kRowBlock, r1 - ra);
+      const int ell = seg.ell_min + l;
+      const double lambda = -static_cast<double>((ell - kSpinWeight) *
+                                                 (ell + kSpinWeight + 1));
+      const bool interior =
+          rows == kRowBlock && ra >= T::BR && ra + kRowBlock + T::BR <= nr;
+      if (interior) {
+        {  // psi: D psi (constraint), dissipation, (c_psi + lambda) psi
+          double2 w[kRowBlock + 2 * T::P];
+          load_window<kRowBlock, T::P>(w, u + 2 * ne + l, rs, s0, ra);
+  #pragma unroll
+          for (int i = 0; i < kRowBlock; ++i) {
+            const double* cf = coef + (ra + i - t0) * kCoefCount;
+            const double2 dpsi =
                 cscale(inv_h, window_derivative<DISC, kRowBlock, T::P>(w, i));
+            kQ[i] = cscale(damping, dpsi);
+            kpsi[i] = dissipate
+                          ? cscale(diss_scale,
+                                   window_dissipation<DISC, kRowBlock, T::P>(w, i))
+                          : make_double2(0.0, 0.0);
+            const double2 psi = w[i + T::P];
+            kP[i] = cadd(cmul(make_double2(cf[7], cf[8]), psi),
+                         cscale(lambda, psi));
+          }
+        }
+        {  // Q: -gamma Q, dissipation; free-damped: H_R D Q + q Q
+          double2 w[kRowBlock + 2 * T::P];
+          load_window<kRowBlock, T::P>(w, u + ne + l, rs, s0, ra);
+  #pragma unroll
+          for (int i = 0; i < kRowBlock; ++i) {
+            const double* cf = coef + (ra + i - t0) * kCoefCount;
+            const double2 Q = w[i + T::P];
+            kQ[i] = csub(kQ[i], cscale(damping, Q));
+            if (dissipate) {
+              kQ[i] = cfma(diss_scale,
+                           window_dissipation<DISC, kRowBlock, T::P>(w, i),
+                           kQ[i]);
+            }
+            if (!SC) {
+              const double2 dq =
+                  cscale(inv_h, window_derivative<DISC, kRowBlock, T::P>(w, i));
+              kP[i] = cadd(kP[i], cscale(cf[2], dq));
+              kP[i] = cadd(kP[i], cmul(make_double2(cf[5], cf[6]), Q));
+            }
+          }
+        }
+        if (SC) {  // stage-constrained effective Q = D psi
+          double2 w[kRowBlock + 2 * T::HALF];
+          load_window<kRowBlock, T::HALF>(w, qeff + l, ne, t0, ra);
+  #pragma unroll
+          for (int i = 0; i < kRowBlock; ++i) {
+            const double* cf = coef + (ra + i - t0) * kCoefCount;
+            const double2 dq = cscale(
+                inv_h, window_derivative<DISC, kRowBlock, T::HALF>(w, i));
             kP[i] = cadd(kP[i], cscale(cf[2], dq));
-            kP[i] = cadd(kP[i], cmul(make_double2(cf[5], cf[6]), Q));
+            kP[i] = cadd(kP[i], cmul(make_double2(cf[5], cf[6]), w[i + T::HALF]));
+          }
+        }
+        if (dissipate) {  // P: dissipation only
+          double2 w[kRowBlock + 2 * T::P];
+          load_window<kRowBlock, T::P>(w, u + l, rs, s0, ra);
+  #pragma unroll
+          for (int i = 0; i < kRowBlock; ++i) {
+            kP[i] = cfma(diss_scale,
+                         window_dissipation<DISC, kRowBlock, T::P>(w, i), kP[i]);
+          }
+        }
+        {  // psi_t: D psi_t into Q_t, psi_t itself
+          double2 w[kRowBlock + 2 * T::HALF];
+          load_window<kRowBlock, T::HALF>(w, psit + l, ne, t0, ra);
+  #pragma unroll
+          for (int i = 0; i < kRowBlock; ++i) {
+            kQ[i] = cadd(kQ[i], cscale(inv_h, window_derivative<DISC, kRowBlock,
+                                                                T::HALF>(w, i)));
+            kpsi[i] = cadd(kpsi[i], w[i + T::HALF]);
+          }
+        }
+      } else {
+        for (int i = 0; i < rows; ++i) {
+          const int r = ra + i;
+          const double* cf = coef + (r - t0) * kCoefCount;
+          const double2* urow = u + (r - s0) * rs;
+          const double2 Qs = urow[ne + l];
+          const double2 psi = urow[2 * ne + l];
+          const double2 Qe = qcol[(r - qbase) * qstride + l];
+          const double2 dpsi =
+              cscale(inv_h, sbp_derivative<DISC>(u + 2 * ne + l, rs, s0, r, nr));
+          const double2 dq = cscale(
+              inv_h, sbp_derivative<DISC>(qcol + l, qstride, qbase, r, nr));
+          const double2 dpsit =
+              cscale(inv_h, sbp_derivative<DISC>(psit + l, ne, t0, r, nr));
+          double2 P_t = cscale(cf[2], dq);
+          P_t = cadd(P_t, cmul(make_double2(cf[5], cf[6]), Qe));
+          P_t = cadd(P_t, cmul(make_double2(cf[7], cf[8]), psi));
+          P_t = cadd(P_t, cscale(lambda, psi));
+          double2 Q_t = csub(dpsit, cscale(damping, csub(Qs, dpsi)));
+          double2 psi_t = psit[(r - t0) * ne + l];
+          if (dissipate) {
+            P_t = cfma(diss_scale, sbp_dissipation<DISC>(u + l, rs, s0, r, nr),
+                       P_t);
+            Q_t = cfma(diss_scale,
+                       sbp_dissipation<DISC>(u + ne + l, rs, s0, r, nr), Q_t);
+            psi_t = cfma(diss_scale,
+                         sbp_dissipation<DISC>(u + 2 * ne + l, rs, s0, r, nr),
+                         psi_t);
+          }
+          kP[i] = P_t;
+          kQ[i] = Q_t;
+          kpsi[i] = psi_t;
+        }
+      }
+    }
+    if (park) {
+      __syncthreads();  // every window has finished reading the slab
+      if (active) {
+        for (int i = 0; i < rows; ++i) {
+          double2* dst = u + (ra + i - s0) * rs + l;
+          dst[0] = kP[i];
+          dst[ne] = kQ[i];
+          dst[2 * ne] = kpsi[i];
+        }
+      }
+    } else if (active) {
+        // RK update: every own-row input is loaded before any store so the
+        // global loads are in flight together.
+        const long long g0 = seg.offset + static_cast<long long>(ra) * rs + l;
+        double2 in0[kRowBlock][3], in1[kRowBlock][3];
+        const double2* __restrict__ src0 =
+            p.stage == kStage2 ? p.kA : (p.stage == kStage3 ? p.y : p.acc);
+        const double2* __restrict__ src1 = p.acc;
+    #pragma unroll
+        for (int i = 0; i < kRowBlock; ++i) {
+    #pragma unroll
+          for (int f = 0; f < 3; ++f) {
+            in0[i][f] = make_double2(0.0, 0.0);
+            in1[i][f] = make_double2(0.0, 0.0);
+            if (i < rows && p.stage != kStage1 && p.stage != kRhsOnly) {
+              const long long gi = g0 + static_cast<long long>(i) * rs + f * ne;
+              in0[i][f] = src0[gi];
+              if (p.stage == kStage3) in1[i][f] = src1[gi];
+            }
+          }
+        }
+    #pragma unroll
+        for (int i = 0; i < kRowBlock; ++i) {
+          if (i >= rows) break;
+          const double2 k[3] = {kP[i], kQ[i], kpsi[i]};
+    #pragma unroll
+          for (int f = 0; f < 3; ++f) {
+            const long long gi = g0 + static_cast<long long>(i) * rs + f * ne;
+            switch (p.stage) {
+              case kStage1:
+              case kRhsOnly:
+                p.kA[gi] = k[f];
+                break;
+              case kStage2:  // in0 = k1
+                p.kB[gi] = k[f];
+                p.acc[gi] = cfma(2.0, k[f], in0[i][f]);
+                break;
+              case kStage3: {  // in0 = y, in1 = k1 + 2 k2
+                const double2 acc = cfma(2.0, k[f], in1[i][f]);
+                p.acc[gi] = cfma(dt6, acc, in0[i][f]);
+                p.kA[gi] = cfma(dt, k[f], in0[i][f]);
+                break;
+              }
+              case kStage4:  // in0 = y + dt/6 (k1 + 2 k2 + 2 k3)
+                p.y[gi] = cfma(dt6, k[f], in0[i][f]);
+                break;
+            }
+          }
+        }
+    }
+  }
+  if (park) {
+    __syncthreads();
+    const int count = (r1 - r0) * rs;
+    const double2* kk = u + (r0 - s0) * rs;
+    const long long g0 = seg.offset + static_cast<long long>(r0) * rs;
+    constexpr int V = 4;
+    for (int i0 = tid; i0 < count; i0 += kThreads * V) {
+      double2 a[V], b[V];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const int i = i0 + v * kThreads;
+        a[v] = b[v] = make_double2(0.0, 0.0);
+        if (i < count) {
+          switch (p.stage) {
+            case kStage2: a[v] = p.kA[g0 + i]; break;
+            case kStage3: a[v] = p.y[g0 + i]; b[v] = p.acc[g0 + i]; break;
+            case kStage4: a[v] = p.acc[g0 + i]; break;
+            default: break;
           }
         }
       }
-      if (SC) {  // stage-constrained effective Q = D psi
-        double2 w[kRowBlock + 2 * T::HALF];
-        load_window<kRowBlock, T::HALF>(w, qeff + l, ne, t0, ra);
 #pragma unroll
-        for (int i = 0; i < kRowBlock; ++i) {
-          const double* cf = coef + (ra + i - t0) * kCoefCount;
-          const double2 dq = cscale(
-              inv_h, window_derivative<DISC, kRowBlock, T::HALF>(w, i));
-          kP[i] = cadd(kP[i], cscale(cf[2], dq));
-          kP[i] = cadd(kP[i], cmul(make_double2(cf[5], cf[6]), w[i + T::HALF]));
-        }
-      }
-      if (dissipate) {  // P: dissipation only
-        double2 w[kRowBlock + 2 * T::P];
-        load_window<kRowBlock, T::P>(w, u + l, rs, s0, ra);
-#pragma unroll
-        for (int i = 0; i < kRowBlock; ++i) {
-          kP[i] = cfma(diss_scale,
-                       window_dissipation<DISC, kRowBlock, T::P>(w, i), kP[i]);
-        }
-      }
-      {  // psi_t: D psi_t into Q_t, psi_t itself
-        double2 w[kRowBlock + 2 * T::HALF];
-        load_window<kRowBlock, T::HALF>(w, psit + l, ne, t0, ra);
-#pragma unroll
-        for (int i = 0; i < kRowBlock; ++i) {
-          kQ[i] = cadd(kQ[i], cscale(inv_h, window_derivative<DISC, kRowBlock,
-                                                              T::HALF>(w, i)));
-          kpsi[i] = cadd(kpsi[i], w[i + T::HALF]);
-        }
-      }
-    } else {
-      for (int i = 0; i < rows; ++i) {
-        const int r = ra + i;
-        const double* cf = coef + (r - t0) * kCoefCount;
-        const double2* urow = u + (r - s0) * rs;
-        const double2 Qs = urow[ne + l];
-        const double2 psi = urow[2 * ne + l];
-        const double2 Qe = qcol[(r - qbase) * qstride + l];
-        const double2 dpsi =
-            cscale(inv_h, sbp_derivative<DISC>(u + 2 * ne + l, rs, s0, r, nr));
-        const double2 dq = cscale(
-            inv_h, sbp_derivative<DISC>(qcol + l, qstride, qbase, r, nr));
-        const double2 dpsit =
-            cscale(inv_h, sbp_derivative<DISC>(psit + l, ne, t0, r, nr));
-        double2 P_t = cscale(cf[2], dq);
-        P_t = cadd(P_t, cmul(make_double2(cf[5], cf[6]), Qe));
-        P_t = cadd(P_t, cmul(make_double2(cf[7], cf[8]), psi));
-        P_t = cadd(P_t, cscale(lambda, psi));
-        double2 Q_t = csub(dpsit, cscale(damping, csub(Qs, dpsi)));
-        double2 psi_t = psit[(r - t0) * ne + l];
-        if (dissipate) {
-          P_t = cfma(diss_scale, sbp_dissipation<DISC>(u + l, rs, s0, r, nr),
-                     P_t);
-          Q_t = cfma(diss_scale,
-                     sbp_dissipation<DISC>(u + ne + l, rs, s0, r, nr), Q_t);
-          psi_t = cfma(diss_scale,
-                       sbp_dissipation<DISC>(u + 2 * ne + l, rs, s0, r, nr),
-                       psi_t);
-        }
-        kP[i] = P_t;
-        kQ[i] = Q_t;
-        kpsi[i] = psi_t;
-      }
-    }
-    // RK update: every own-row input is loaded before any store so the
-    // global loads are in flight together.
-    const long long g0 = seg.offset + static_cast<long long>(ra) * rs + l;
-    double2 in0[kRowBlock][3], in1[kRowBlock][3];
-    const double2* __restrict__ src0 =
-        p.stage == kStage2 ? p.kA : (p.stage == kStage3 ? p.y : p.acc);
-    const double2* __restrict__ src1 = p.acc;
-#pragma unroll
-    for (int i = 0; i < kRowBlock; ++i) {
-#pragma unroll
-      for (int f = 0; f < 3; ++f) {
-        in0[i][f] = make_double2(0.0, 0.0);
-        in1[i][f] = make_double2(0.0, 0.0);
-        if (i < rows && p.stage != kStage1 && p.stage != kRhsOnly) {
-          const long long gi = g0 + static_cast<long long>(i) * rs + f * ne;
-          in0[i][f] = src0[gi];
-          if (p.stage == kStage3) in1[i][f] = src1[gi];
-        }
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < kRowBlock; ++i) {
-      if (i >= rows) break;
-      const double2 k[3] = {kP[i], kQ[i], kpsi[i]};
-#pragma unroll
-      for (int f = 0; f < 3; ++f) {
-        const long long gi = g0 + static_cast<long long>(i) * rs + f * ne;
+      for (int v = 0; v < V; ++v) {
+        const int i = i0 + v * kThreads;
+        if (i >= count) break;
+        const double2 k = kk[i];
+        const long long g = g0 + i;
         switch (p.stage) {
           case kStage1:
           case kRhsOnly:
-            p.kA[gi] = k[f];
+            p.kA[g] = k;
             break;
-          case kStage2:  // in0 = k1
-            p.kB[gi] = k[f];
-            p.acc[gi] = cfma(2.0, k[f], in0[i][f]);
+          case kStage2:  // a = k1
+            p.kB[g] = k;
+            p.acc[g] = cfma(2.0, k, a[v]);
             break;
-          case kStage3: {  // in0 = y, in1 = k1 + 2 k2
-            const double2 acc = cfma(2.0, k[f], in1[i][f]);
-            p.acc[gi] = cfma(dt6, acc, in0[i][f]);
-            p.kA[gi] = cfma(dt, k[f], in0[i][f]);
+          case kStage3: {  // a = y, b = k1 + 2 k2
+            const double2 acc = cfma(2.0, k, b[v]);
+            p.acc[g] = cfma(dt6, acc, a[v]);
+            p.kA[g] = cfma(dt, k, a[v]);
             break;
           }
-          case kStage4:  // in0 = y + dt/6 (k1 + 2 k2 + 2 k3)
-            p.y[gi] = cfma(dt6, k[f], in0[i][f]);
+          case kStage4:  // a = y + dt/6 (k1 + 2 k2 + 2 k3)
+            p.y[g] = cfma(dt6, k, a[v]);
             break;
         }
       }
