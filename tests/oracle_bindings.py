@@ -143,6 +143,12 @@ class RefPipeline:
                                                       ctypes.byref(count)))
         return tb._records(buf, count.value)
 
+    def activation(self) -> tb.Activation:
+        a = tb.Activation()
+        self._check(self.lib.teuk_ref_get_activation(self._handle,
+                                                     ctypes.byref(a)))
+        return a
+
     def project_to_bands(self, state):
         arr = np.array(state, dtype=np.complex128, order="C", copy=True)
         self._check(self.lib.teuk_ref_project_to_bands(

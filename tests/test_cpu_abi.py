@@ -62,11 +62,37 @@ def test_reference_validation_before_device_work(change, message):
         tb.Pipeline(config)
 
 
-def test_second_order_policies_are_reported_unsupported_or_fail_on_cuda():
-    config = tb.SolveConfig(**{**CASES["schw_d84"].__dict__,
-                               "source_mode": tb.SOURCE_UNRESTRICTED})
-    with pytest.raises(tb.TeukError):
+SECOND_ORDER = tb.SolveConfig(**{**CASES["nonparent"].__dict__,
+                                 "source_mode": tb.SOURCE_UNRESTRICTED})
+
+
+@pytest.mark.skipif(cuda_available(), reason="host has a GPU")
+def test_second_order_has_no_cpu_fallback():
+    with pytest.raises(tb.TeukError) as info:
+        tb.Pipeline(SECOND_ORDER)
+    assert info.value.status == tb.ERR_CUDA
+
+
+@pytest.mark.parametrize("change,message", [
+    ({"targets": (-4, 0, 6)}, "is not stored"),
+    ({"normalized_constraint_tolerance": -1.0}, "source policy is invalid"),
+    ({"required_consecutive_passes": 0}, "source policy is invalid"),
+    ({"ell_max_second": 2}, "exact-product padding"),
+])
+def test_second_order_validation_before_device_work(change, message):
+    config = tb.SolveConfig(**{**SECOND_ORDER.__dict__, **change})
+    with pytest.raises(tb.InvalidArgument, match=re.escape(message)):
         tb.Pipeline(config)
+
+
+def test_second_order_footprint_counts_nodal_buffers():
+    nodal = tb.footprint_bytes(SECOND_ORDER)
+    points = (len(SECOND_ORDER.modes) * SECOND_ORDER.radial_points *
+              SECOND_ORDER.theta_nodes)
+    # at least the state, RK stage and four RK slopes of all 13 fields
+    assert nodal >= 6 * 13 * points * 16
+    linear = tb.footprint_bytes(CASES["nonparent"])
+    assert nodal > linear
 
 
 @pytest.mark.skipif(cuda_available(), reason="host has a GPU")

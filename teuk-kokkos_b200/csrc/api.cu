@@ -20,6 +20,7 @@
 
 #include "engine.h"
 #include "kernels.h"
+#include "second_order.h"
 #include "teuk_b200.h"
 
 namespace teuk_b200 {
@@ -55,6 +56,9 @@ int guarded(Body&& body) {
     g_last_error = e.what();
     return TEUK_B200_ERR_UNSUPPORTED;
   } catch (const CudaError& e) {
+    g_last_error = e.what();
+    return TEUK_B200_ERR_CUDA;
+  } catch (const DeviceError& e) {
     g_last_error = e.what();
     return TEUK_B200_ERR_CUDA;
   } catch (const std::bad_alloc&) {
@@ -203,8 +207,8 @@ struct Batch {
     for (const Config& c : configs) {
       if (c.source_mode != 0) {
         throw Unsupported(
-            "second-order source policies are not built on the B200 path; "
-            "only the linear (disabled) pipeline runs here");
+            "second-order source policies run through teuk_b200_create "
+            "(one nodal pipeline per solve), not through a batch");
       }
     }
     int device_count = 0;
@@ -705,13 +709,78 @@ struct teuk_b200_batch {
   std::unique_ptr<Batch> batch;
 };
 struct teuk_b200_pipeline {
+  // exactly one of the two is set: the band-storage batch of one solve for
+  // the linear policy, the nodal pipeline for second-order source policies
   std::unique_ptr<Batch> batch;
+  std::unique_ptr<teuk_b200::NodalPipeline> nodal;
 };
 
 namespace {
 
 void require(const bool condition, const char* message) {
   if (!condition) throw std::invalid_argument(message);
+}
+
+void require_device() {
+  int device_count = 0;
+  const cudaError_t err = cudaGetDeviceCount(&device_count);
+  if (err != cudaSuccess) {
+    throw teuk_b200::DeviceError(std::string("cudaGetDeviceCount: ") +
+                                 cudaGetErrorString(err));
+  }
+  if (device_count <= 0) {
+    throw teuk_b200::DeviceError("no CUDA device is visible");
+  }
+}
+
+// EndpointWaveformSampler::sample over a nodal state
+// (include/teuk/waveform_output.hpp:75-160): psi at the two radial ends,
+// analysed with the first-order band for parents and the second-order band
+// for targets.
+void sample_nodal_endpoint(teuk_b200::NodalPipeline& nodal,
+                           teuk_b200_waveform_record* out,
+                           const size_t capacity, size_t* count) {
+  using namespace teuk_b200;
+  const InstancePlan& plan = nodal.plan();
+  const Config& c = plan.config;
+  const int nt = c.ntheta;
+  const double pi = std::numbers::pi_v<double>;
+  const double scale[2] = {c.length * c.length, plan.horizon};
+  std::vector<teuk_b200_waveform_record> records;
+  std::vector<double2> slice;
+  for (int order = 1; order <= 2; ++order) {
+    const int field = order == 1 ? 2 : 12;
+    const std::vector<int>& members = order == 1 ? c.parents : c.targets;
+    const int ell_max = order == 1 ? c.ell_max_first : c.ell_max_second;
+    for (int boundary = 0; boundary < 2; ++boundary) {
+      nodal.endpoint_slice(field, boundary == 0 ? 0 : c.nr - 1, slice);
+      for (size_t mode = 0; mode < c.modes.size(); ++mode) {
+        const int m = c.modes[mode];
+        if (!std::binary_search(members.begin(), members.end(), m)) continue;
+        const int ell_min = std::max(2, std::abs(m));
+        for (int ell = ell_min; ell <= ell_max; ++ell) {
+          double re = 0.0, im = 0.0;
+          for (int j = 0; j < nt; ++j) {
+            const double a = 2.0 * pi * plan.weights[static_cast<size_t>(j)] *
+                             spin_weighted_harmonic_theta(
+                                 ell, m, kSpinWeight,
+                                 plan.theta[static_cast<size_t>(j)]);
+            const double2 v = slice[mode * static_cast<size_t>(nt) +
+                                    static_cast<size_t>(j)];
+            re += a * v.x;
+            im += a * v.y;
+          }
+          records.push_back({boundary, order, m, ell, re, im,
+                             scale[boundary] * re, scale[boundary] * im});
+        }
+      }
+    }
+  }
+  if (count != nullptr) *count = records.size();
+  if (records.size() > capacity) {
+    throw std::invalid_argument("waveform record capacity is too small");
+  }
+  std::copy(records.begin(), records.end(), out);
 }
 
 void fill_shape(const teuk_b200::InstancePlan& plan, size_t shape[4]) {
@@ -776,6 +845,28 @@ void initialize_gaussian(Batch& b, const int instance,
   reset_activation(plan);
 }
 
+void initialize_nodal_gaussian(teuk_b200::NodalPipeline& p,
+                               const teuk_b200_gaussian* pulse) {
+  require(pulse != nullptr, "null Gaussian pulse");
+  require(pulse->mode_count >= 0 &&
+              (pulse->mode_count == 0 || pulse->modes != nullptr),
+          "Gaussian mode list pointer/count mismatch");
+  std::vector<int> ell, m;
+  std::vector<double> re, im;
+  for (int i = 0; i < pulse->mode_count; ++i) {
+    ell.push_back(pulse->modes[i].ell);
+    m.push_back(pulse->modes[i].m);
+    re.push_back(pulse->modes[i].amplitude_real);
+    im.push_back(pulse->modes[i].amplitude_imag);
+  }
+  std::vector<double> nodal;
+  teuk_b200::gaussian_initial_state(p.plan(), pulse->center, pulse->width,
+                                    pulse->compact_support != 0, ell, m, re,
+                                    im, nodal);
+  p.set_state(nodal.data(), TEUK_B200_HOST);
+  p.reset_activation();
+}
+
 }  // namespace
 
 extern "C" {
@@ -791,8 +882,15 @@ int teuk_b200_create(const teuk_b200_config* config,
   return guarded([&] {
     require(config != nullptr && out != nullptr, "null argument");
     auto p = std::make_unique<teuk_b200_pipeline>();
-    p->batch = std::make_unique<Batch>();
-    p->batch->build({teuk_b200::to_config(*config)});
+    const teuk_b200::Config c = teuk_b200::to_config(*config);
+    if (c.source_mode != TEUK_B200_SOURCE_DISABLED) {
+      const teuk_b200::InstancePlan plan = teuk_b200::build_instance_plan(c);
+      require_device();
+      p->nodal = std::make_unique<teuk_b200::NodalPipeline>(plan);
+    } else {
+      p->batch = std::make_unique<Batch>();
+      p->batch->build({c});
+    }
     *out = p.release();
   });
 }
@@ -805,7 +903,7 @@ int teuk_b200_destroy(teuk_b200_pipeline* pipeline) {
 int teuk_b200_shape(const teuk_b200_pipeline* p, size_t shape[4]) {
   return guarded([&] {
     require(p != nullptr && shape != nullptr, "null argument");
-    fill_shape(p->batch->plans[0], shape);
+    fill_shape(p->nodal ? p->nodal->plan() : p->batch->plans[0], shape);
   });
 }
 
@@ -813,6 +911,13 @@ int teuk_b200_set_state(teuk_b200_pipeline* p, const double* state,
                         size_t count, int memory) {
   return guarded([&] {
     require(p != nullptr, "null pipeline");
+    if (p->nodal) {
+      require(count == p->nodal->value_count(),
+              "state complex count does not match shape");
+      require(state != nullptr, "null state pointer");
+      p->nodal->set_state(state, memory);
+      return;
+    }
     p->batch->set_state(0, state, count, memory);
   });
 }
@@ -821,6 +926,13 @@ int teuk_b200_get_state(teuk_b200_pipeline* p, double* state, size_t count,
                         int memory) {
   return guarded([&] {
     require(p != nullptr, "null pipeline");
+    if (p->nodal) {
+      require(count == p->nodal->value_count(),
+              "state complex count does not match shape");
+      require(state != nullptr, "null state pointer");
+      p->nodal->get_state(state, memory);
+      return;
+    }
     p->batch->get_state(0, state, count, memory);
   });
 }
@@ -832,6 +944,12 @@ int teuk_b200_evaluate_rhs(teuk_b200_pipeline* p, const double* stage,
     require(p != nullptr && stage != nullptr && output != nullptr,
             "null argument");
     require(std::isfinite(time), "stage time must be finite");
+    if (p->nodal) {
+      require(count == p->nodal->value_count(),
+              "state complex count does not match shape");
+      p->nodal->evaluate_rhs(stage, output, memory, time);
+      return;
+    }
     p->batch->evaluate_rhs(0, stage, output, count, memory);
   });
 }
@@ -844,6 +962,17 @@ int teuk_b200_step(teuk_b200_pipeline* p, double time, double dt, int steps) {
       throw std::invalid_argument(
           "pipeline step requires finite positive time data");
     }
+    if (p->nodal) {
+      require(steps >= 0, "step count must be nonnegative");
+      // the driver loop of the reference: time advances by dt per step
+      double t = time;
+      for (int s = 0; s < steps; ++s) {
+        p->nodal->step(t, dt);
+        t += dt;
+      }
+      teuk_b200::check(cudaStreamSynchronize(p->nodal->stream()), "step");
+      return;
+    }
     p->batch->step({dt}, steps, false);
     teuk_b200::check(cudaStreamSynchronize(p->batch->stream), "step");
   });
@@ -853,6 +982,10 @@ int teuk_b200_initialize_gaussian(teuk_b200_pipeline* p,
                                   const teuk_b200_gaussian* pulse) {
   return guarded([&] {
     require(p != nullptr, "null pipeline");
+    if (p->nodal) {
+      initialize_nodal_gaussian(*p->nodal, pulse);
+      return;
+    }
     initialize_gaussian(*p->batch, 0, pulse);
   });
 }
@@ -862,6 +995,10 @@ int teuk_b200_sample_endpoint(teuk_b200_pipeline* p,
                               size_t capacity, size_t* count) {
   return guarded([&] {
     require(p != nullptr, "null pipeline");
+    if (p->nodal) {
+      sample_nodal_endpoint(*p->nodal, out, capacity, count);
+      return;
+    }
     p->batch->sample_endpoint(0, out, capacity, count);
   });
 }
@@ -870,6 +1007,14 @@ int teuk_b200_get_activation(const teuk_b200_pipeline* p,
                              teuk_b200_activation* out) {
   return guarded([&] {
     require(p != nullptr && out != nullptr, "null argument");
+    if (p->nodal) {
+      const auto s = p->nodal->activation();
+      out->active = s.active ? 1 : 0;
+      out->activation_time = s.activation_time;
+      out->consecutive_passes = s.consecutive_passes;
+      out->last_eligibility_time = s.last_eligibility_time;
+      return;
+    }
     const auto& plan = p->batch->plans[0];
     out->active = plan.active;
     out->activation_time = plan.activation_time;
@@ -882,6 +1027,15 @@ int teuk_b200_restore_activation(teuk_b200_pipeline* p,
                                  const teuk_b200_activation* state) {
   return guarded([&] {
     require(p != nullptr && state != nullptr, "null argument");
+    if (p->nodal) {
+      teuk_b200::InstancePlan scratch = p->nodal->plan();
+      restore_activation(scratch, *state);  // validates like the reference
+      p->nodal->restore_activation({scratch.active != 0,
+                                    scratch.activation_time,
+                                    scratch.consecutive_passes,
+                                    scratch.last_eligibility_time});
+      return;
+    }
     restore_activation(p->batch->plans[0], *state);
   });
 }
@@ -889,6 +1043,10 @@ int teuk_b200_restore_activation(teuk_b200_pipeline* p,
 int teuk_b200_reset_activation(teuk_b200_pipeline* p) {
   return guarded([&] {
     require(p != nullptr, "null pipeline");
+    if (p->nodal) {
+      p->nodal->reset_activation();
+      return;
+    }
     reset_activation(p->batch->plans[0]);
   });
 }
@@ -896,6 +1054,10 @@ int teuk_b200_reset_activation(teuk_b200_pipeline* p) {
 int teuk_b200_set_stream(teuk_b200_pipeline* p, void* cuda_stream) {
   return guarded([&] {
     require(p != nullptr, "null pipeline");
+    if (p->nodal) {
+      p->nodal->set_stream(static_cast<cudaStream_t>(cuda_stream));
+      return;
+    }
     p->batch->stream = cuda_stream != nullptr
                            ? static_cast<cudaStream_t>(cuda_stream)
                            : p->batch->own_stream;
@@ -905,7 +1067,9 @@ int teuk_b200_set_stream(teuk_b200_pipeline* p, void* cuda_stream) {
 int teuk_b200_synchronize(teuk_b200_pipeline* p) {
   return guarded([&] {
     require(p != nullptr, "null pipeline");
-    teuk_b200::check(cudaStreamSynchronize(p->batch->stream), "synchronize");
+    teuk_b200::check(cudaStreamSynchronize(p->nodal ? p->nodal->stream()
+                                                     : p->batch->stream),
+                     "synchronize");
   });
 }
 
@@ -914,6 +1078,10 @@ int teuk_b200_footprint_bytes(const teuk_b200_config* config, size_t* bytes) {
     require(config != nullptr && bytes != nullptr, "null argument");
     const auto plan =
         teuk_b200::build_instance_plan(teuk_b200::to_config(*config));
+    if (plan.config.source_mode != TEUK_B200_SOURCE_DISABLED) {
+      *bytes = teuk_b200::nodal_footprint_bytes(plan);
+      return;
+    }
     size_t complex_count = 0;
     size_t matrix = 0;
     for (const auto& mp : plan.modes) {

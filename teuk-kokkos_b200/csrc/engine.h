@@ -154,6 +154,8 @@ void gauss_legendre(int nodes, std::vector<double>& x,
 double spin_weighted_harmonic_theta(int ell, int m, int spin, double theta);
 double outer_horizon_radius(double mass, double spin);
 SbpConstants build_sbp_constants();
+// Diagonal SBP norm weight H_ii / h (include/teuk/radial_discretization.hpp).
+double sbp_norm_weight(int disc, int n, int index);
 // Dense h*D row for host-side use (initial data): value of the SBP first
 // derivative of `line` (stride 2 doubles for complex parts) at `row`.
 void sbp_derivative_line(int disc, const double* line_re_im, int n,

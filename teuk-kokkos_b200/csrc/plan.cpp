@@ -210,6 +210,10 @@ const int binomial_difference[3][7] = {
 
 }  // namespace
 
+double sbp_norm_weight(const int disc, const int n, const int index) {
+  return norm_weight(disc, n, index);
+}
+
 SbpConstants build_sbp_constants() {
   SbpConstants c{};
   for (int disc = 0; disc < 3; ++disc) {

@@ -1,0 +1,113 @@
+// Second-order (quadratic-source) pipeline on the GPU: the stage graph of
+// SpatialPipeline::evaluate_rhs_at_time for the ConstraintAware and
+// Unrestricted source policies (include/teuk/spatial_pipeline.hpp:517-587),
+// its RK4 step with the source-activation latch (:590-620, :1225-1310).
+//
+// Storage follows the reference: every field lives nodally on the
+// Gauss-Legendre grid in (mode, slot, radial, theta) order, because the
+// quadratic source multiplies fields of different m pointwise.  Each angular
+// operator of a SignedModeAngularCoordinator (project, Laplacian, eth,
+// eth') is one fused launch over all modes and radial rows.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <stdexcept>
+#include <vector>
+
+#include "engine.h"
+
+namespace teuk_b200 {
+
+// One SignedModeAngularCoordinator: (spin, boost, ell_max, active modes).
+struct AngularCoordinator {
+  int spin = 0;
+  int boost = 0;
+  int ell_max = 0;
+  std::vector<int> active;  // per registry mode: 1 if it has resources
+  // per registry mode, offsets into the matrix pool (0 when inactive)
+  std::vector<int> analysis;        // A_s   [ne_s][nt]
+  std::vector<int> synthesis;       // S_s   [nt][ne_s]
+  std::vector<int> raised;          // S_s+1 [nt][ne_s+1]
+  std::vector<int> lowered;         // S_s-1 [nt][ne_s-1]
+  std::vector<int> n_ell, ell_min;  // source band
+  std::vector<int> n_ell_up, ell_min_up, n_ell_down, ell_min_down;
+};
+
+struct SourceActivation {
+  bool active = false;
+  double activation_time = -1.0;
+  int consecutive_passes = 0;
+  double last_eligibility_time = -1.0;
+};
+
+struct ConstraintNorms {
+  double absolute_maximum[3] = {0, 0, 0};
+  double normalized_maximum[3] = {0, 0, 0};
+  double weighted_rms[3] = {0, 0, 0};
+  double normalized_weighted[3] = {0, 0, 0};
+  double controlling_normalized = 0.0;
+  bool all_finite = true;
+};
+
+// Uploads the SBP tables used by the nodal kernels to the current device.
+cudaError_t upload_nodal_sbp_constants();
+
+// A CUDA runtime failure inside the nodal pipeline.
+struct DeviceError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+// Device bytes a NodalPipeline allocates for `plan`.
+std::size_t nodal_footprint_bytes(const InstancePlan& plan);
+
+class NodalPipeline {
+ public:
+  struct Buffers;
+  explicit NodalPipeline(const InstancePlan& plan);
+  ~NodalPipeline();
+  NodalPipeline(const NodalPipeline&) = delete;
+  NodalPipeline& operator=(const NodalPipeline&) = delete;
+
+  const InstancePlan& plan() const { return plan_; }
+  size_t value_count() const { return plan_.value_count(); }
+  void set_stream(cudaStream_t stream);
+  cudaStream_t stream() const { return stream_; }
+
+  void set_state(const double* state, int memory);
+  void get_state(double* state, int memory);
+  void evaluate_rhs(const double* stage, double* out, int memory,
+                    double time);
+  void step(double time, double dt);
+  void reset_activation();
+  void restore_activation(const SourceActivation& s);
+  SourceActivation activation() const { return activation_; }
+  const ConstraintNorms& constraint_norms() const { return norms_; }
+  // Endpoint psi of the first-order (field 2) or second-order (field 12)
+  // state: (mode, theta) nodal values at radial index `radial`.
+  void endpoint_slice(int field, int radial, std::vector<double2>& out);
+
+ private:
+  void build_coordinators();
+  void evaluate(const double2* stage, double2* out);
+  void consider_activation(double accepted_time);
+  void advance_fixed(double time, double dt);
+  ConstraintNorms sample_constraints();
+  void sync_check(const char* what);
+
+  InstancePlan plan_;
+  std::vector<int> pair_index1_, pair_index2_, pair_offsets_, targets_;
+  std::vector<AngularCoordinator> coordinators_;
+  // per coordinator: pool offsets of the Laplacian / raising / lowering
+  // diagonals of each registry mode
+  std::vector<int> coordinator_diag_[10][3];
+  std::vector<double> matrices_;
+  SourceActivation activation_;
+  ConstraintNorms norms_;
+  cudaStream_t own_stream_ = nullptr;
+  cudaStream_t stream_ = nullptr;
+  std::unique_ptr<Buffers> buf_;
+};
+
+}  // namespace teuk_b200
