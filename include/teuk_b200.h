@@ -33,6 +33,9 @@
  *                               (include/teuk/spatial_pipeline.hpp:386-420)
  *   teuk_b200_last_error        the std::invalid_argument / runtime_error
  *                               message the reference would throw
+ *   teuk_b200_step_static_scratch
+ *                               no counterpart: teuk_b200_step with its RK
+ *                               slopes in a static device array
  *
  * Batched variants (teuk_b200_batch_*) pack many independent solves of
  * uneven shape into one set of stage launches; they have no single
@@ -195,6 +198,25 @@ int teuk_b200_evaluate_rhs(teuk_b200_pipeline* pipeline, const double* stage,
 /* Advance `steps` classical RK4 steps of size dt from `time`. */
 int teuk_b200_step(teuk_b200_pipeline* pipeline, double time, double dt,
                    int steps);
+/* Same steps as teuk_b200_step without allocating device memory: the three
+ * RK slope buffers come from one static device array of 3 x 524,288
+ * complex128 values (24 MiB) instead of the pipeline's own.  No counterpart
+ * in the reference, which always steps through a workspace it allocated.
+ * - For callers that cannot allocate at step time (a framework allocator
+ *   that already holds the device, a latency budget without room for a
+ *   driver allocation call).
+ * - Linear (disabled-source) pipelines whose band state holds at most
+ *   524,288 complex values; larger ones, and second-order pipelines, are
+ *   rejected (TEUK_B200_ERR_INVALID_ARGUMENT / _UNSUPPORTED) before any
+ *   device work.
+ * - The first call on each device resolves the array's address (a module
+ *   load); make it once before any stream capture.
+ * - The array is shared by every pipeline on a device: calls that overlap
+ *   in time on one device (other threads, other streams) race on it.
+ *   Serialize them.
+ * - Nothing in the array needs to start at zero. */
+int teuk_b200_step_static_scratch(teuk_b200_pipeline* pipeline, double time,
+                                  double dt, int steps);
 int teuk_b200_initialize_gaussian(teuk_b200_pipeline* pipeline,
                                   const teuk_b200_gaussian* pulse);
 /* Records for the scri then horizon endpoints of the first-order field and

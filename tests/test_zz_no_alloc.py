@@ -1,0 +1,72 @@
+"""Allocation-free RK4 steps (teuk_b200_step_static_scratch) on the GPU.
+
+The entry point runs the same stage kernels as teuk_b200_step with the RK
+slope buffers taken from the library's static device array.  Two calls in a
+row must reproduce teuk_b200_step on an identically initialised pipeline.
+This file is named to be collected last and depends on no other test.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import teuk_b200 as tb
+from cases import CASES, pulse_for, relative_error, step_size
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def _twins(config, seed=3):
+    a, b = tb.Pipeline(config), tb.Pipeline(config)
+    pulse = pulse_for(config, seed)
+    a.initialize_gaussian(pulse)
+    b.initialize_gaussian(pulse)
+    return a, b
+
+
+@pytest.mark.parametrize("name", ["kerr_d105", "kerr_d42_sc"])
+def test_two_static_scratch_calls_match_step(require_gpu, name):
+    config = CASES[name]
+    reference, static = _twins(config)
+    dt = step_size(config)
+    reference.step(0.0, dt, 3)
+    static.step_static_scratch(0.0, dt, 3)
+    assert relative_error(static.get_state(), reference.get_state()) < TOL
+    reference.step(3 * dt, dt, 2)
+    static.step_static_scratch(3 * dt, dt, 2)
+    assert relative_error(static.get_state(), reference.get_state()) < TOL
+
+
+def test_static_scratch_call_allocates_no_device_memory(require_gpu):
+    import torch
+
+    config = CASES["kerr_d105"]
+    _, static = _twins(config)
+    dt = step_size(config)
+    static.step_static_scratch(0.0, dt, 1)  # first call: symbol lookup
+    free_before, _ = torch.cuda.mem_get_info()
+    static.step_static_scratch(dt, dt, 4)
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
+
+
+def test_static_scratch_rejects_band_state_beyond_capacity(require_gpu):
+    # 387 band values per radial row x 1500 rows = 580,500 > 524,288
+    config = dataclasses.replace(CASES["kerr_d105"], radial_points=1500)
+    pipeline = tb.Pipeline(config)
+    pipeline.initialize_gaussian(pulse_for(config, 3))
+    before = pipeline.get_state()
+    with pytest.raises(tb.InvalidArgument,
+                       match="exceeds the static scratch capacity"):
+        pipeline.step_static_scratch(0.0, step_size(config), 1)
+    assert np.array_equal(pipeline.get_state(), before)
+
+
+def test_static_scratch_rejects_second_order_pipelines(require_gpu):
+    config = dataclasses.replace(CASES["nonparent"],
+                                 source_mode=tb.SOURCE_UNRESTRICTED)
+    pipeline = tb.Pipeline(config)
+    with pytest.raises(tb.Unsupported, match="linear"):
+        pipeline.step_static_scratch(0.0, step_size(config), 1)

@@ -21,6 +21,7 @@
 #include "engine.h"
 #include "kernels.h"
 #include "second_order.h"
+#include "static_scratch.h"
 #include "teuk_b200.h"
 
 namespace teuk_b200 {
@@ -597,6 +598,30 @@ struct Batch {
     }
   }
 
+  // RK4 steps whose three slope buffers (k1 / stage-4 input, k2, weighted
+  // sum) are slopes[0, stride), [stride, 2 stride), [2 stride, 3 stride)
+  // instead of kA / kB / acc.  Launches only: no allocation, no graph.
+  void step_with_slopes(const std::vector<double>& dt, const int steps,
+                        double2* slopes, const size_t stride) {
+    if (steps < 0) throw std::invalid_argument("step count must be nonnegative");
+    if (total_complex > stride) {
+      throw std::invalid_argument("slope buffers are smaller than the band state");
+    }
+    set_dt(dt);
+    for (int s = 0; s < steps; ++s) {
+      for (const int kind : {kStage1, kStage2, kStage3, kStage4}) {
+        for (StageLaunch g : groups) {
+          g.stage = kind;
+          g.kA = slopes;
+          g.kB = slopes + stride;
+          g.acc = slopes + 2 * stride;
+          check(launch_stage(g, stream), "stage kernel");
+        }
+      }
+    }
+    check(cudaGetLastError(), "step");
+  }
+
   void endpoint_modal(double* out, const size_t capacity, size_t* count,
                       const int memory) {
     const size_t n = h_seg.size() * 2 * static_cast<size_t>(max_ell);
@@ -975,6 +1000,36 @@ int teuk_b200_step(teuk_b200_pipeline* p, double time, double dt, int steps) {
     }
     p->batch->step({dt}, steps, false);
     teuk_b200::check(cudaStreamSynchronize(p->batch->stream), "step");
+  });
+}
+
+int teuk_b200_step_static_scratch(teuk_b200_pipeline* p, double time,
+                                  double dt, int steps) {
+  return guarded([&] {
+    require(p != nullptr, "null pipeline");
+    if (p->nodal) {
+      throw teuk_b200::Unsupported(
+          "static-scratch steps cover the linear (disabled-source) pipeline "
+          "only");
+    }
+    if (!std::isfinite(time) || !std::isfinite(dt) || time < 0.0 ||
+        !(dt > 0.0)) {
+      throw std::invalid_argument(
+          "pipeline step requires finite positive time data");
+    }
+    Batch& b = *p->batch;
+    if (b.total_complex > teuk_b200::kStaticSlopeCapacity) {
+      throw std::invalid_argument(
+          "band state of " + std::to_string(b.total_complex) +
+          " complex values exceeds the static scratch capacity of " +
+          std::to_string(teuk_b200::kStaticSlopeCapacity) +
+          " per slope buffer; use teuk_b200_step");
+    }
+    double2* slopes = nullptr;
+    teuk_b200::check(teuk_b200::static_slope_buffers(&slopes),
+                     "static scratch address");
+    b.step_with_slopes({dt}, steps, slopes, teuk_b200::kStaticSlopeCapacity);
+    teuk_b200::check(cudaStreamSynchronize(b.stream), "step");
   });
 }
 

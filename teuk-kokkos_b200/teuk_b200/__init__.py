@@ -235,6 +235,7 @@ def _load() -> ctypes.CDLL:
         "teuk_b200_get_state": ([P, P, SZ, I], I),
         "teuk_b200_evaluate_rhs": ([P, P, P, SZ, D, I], I),
         "teuk_b200_step": ([P, D, D, I], I),
+        "teuk_b200_step_static_scratch": ([P, D, D, I], I),
         "teuk_b200_initialize_gaussian": ([P, ctypes.POINTER(_Gaussian)], I),
         "teuk_b200_sample_endpoint": ([P, ctypes.POINTER(WaveformRecord), SZ,
                                        ctypes.POINTER(SZ)], I),
@@ -388,6 +389,13 @@ class Pipeline:
 
     def step(self, time: float, dt: float, steps: int = 1):
         _check(_lib.teuk_b200_step(self._handle, time, dt, steps))
+
+    def step_static_scratch(self, time: float, dt: float, steps: int = 1):
+        """teuk_b200_step with the RK slopes in the library's static device
+        array: no device allocation (linear pipelines up to 524,288 band
+        values; calls must not overlap on one device)."""
+        _check(_lib.teuk_b200_step_static_scratch(self._handle, time, dt,
+                                                  steps))
 
     def initialize_gaussian(self, pulse: GaussianPulse):
         s, keep = pulse.to_struct()
