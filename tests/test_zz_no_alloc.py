@@ -59,7 +59,9 @@ def test_static_scratch_call_allocates_no_device_memory(require_gpu):
         free_after, _ = torch.cuda.mem_get_info()
     finally:
         gc.enable()
-    assert free_after == free_before
+    # an allocation would lower the free figure; the driver may return
+    # memory it cached for earlier work at any time, so only a drop fails
+    assert free_after >= free_before
 
 
 def test_static_scratch_rejects_band_state_beyond_capacity(require_gpu):
