@@ -58,6 +58,11 @@ def parse_args():
                    help="target length of the CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-serving", action="store_true")
+    p.add_argument("--serve-requests", type=int, default=48,
+                   help="requests of the continuous-batching measurement")
+    p.add_argument("--serve-steps", type=int, default=200,
+                   help="RK4 steps per serving request")
     return p.parse_args()
 
 
@@ -157,6 +162,90 @@ def recorded_traffic(algorithmic_bytes_per_launch: float):
         return per_unit * algorithmic_bytes_per_launch
     except Exception:
         return None
+
+
+# ---------------------------------------------------------------- serving
+def one_at_a_time_rate(tb, wl, kinds, steps: int):
+    """Plain FP64 path, one solve at a time: device grid-point updates/s of
+    a representative solve of each request kind (CUDA events)."""
+    import torch
+
+    rates = {}
+    stream = torch.cuda.Stream()
+    for kind, (config, pulse, dt) in kinds.items():
+        p = tb.Pipeline(config)
+        p.set_stream(stream.cuda_stream)
+        p.initialize_gaussian(pulse)
+        p.step(0.0, dt, 3)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        p.step(3 * dt, dt, steps)
+        b.record(stream)
+        b.synchronize()
+        rates[kind] = steps * wl.grid_points(config) / (a.elapsed_time(b) / 1e3)
+        p.close()
+    return rates
+
+
+def serving_run(tb, wl, capacity: float, requests: int, steps: int,
+                seed: int = 20260101):
+    """Poisson stream of mixed requests through the continuous-batching
+    server at ~80 % of the batched capacity; returns the 'serving' record."""
+    import torch
+
+    mix = wl.serving_mix(requests, seed)
+    work = [steps * wl.grid_points(c) for _, c, _, _ in mix]
+    rate = 0.8 * capacity / (sum(work) / len(work))
+    rng = np.random.Generator(np.random.PCG64(seed + 1))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=requests))
+    arrivals -= arrivals[0]
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(min(150e9, 0.8 * free))
+    server = tb.Server(hbm_budget_bytes=budget)
+    ids = []
+    t0 = time.perf_counter()
+    while True:
+        now = time.perf_counter() - t0
+        while len(ids) < requests and arrivals[len(ids)] <= now:
+            _, c, pulse, dt = mix[len(ids)]
+            ids.append(server.submit(c, pulse, dt, steps))
+        st = server.stats()
+        if st.active + st.queued == 0:
+            if len(ids) == requests:
+                break
+            time.sleep(max(0.0, arrivals[len(ids)] - now))
+            continue
+        server.advance(4)
+    makespan = time.perf_counter() - t0
+    latencies = np.array([server.result(i)[1] for i in ids])
+    st = server.stats()
+    kinds = {}
+    for kind, c, pulse, dt in mix:
+        kinds.setdefault(kind, (c, pulse, dt))
+    alone = one_at_a_time_rate(tb, wl, kinds, min(steps, 50))
+    alone_seconds = sum(w / alone[k] for w, (k, *_rest) in zip(work, mix))
+    server.close()
+    device_rate = st.grid_point_updates / st.device_seconds
+    return {
+        "requests": requests,
+        "mix": "40% schwarzschild nr=257 d8-4 ell<=8, 30% kerr_ringdown "
+               "nr=1025 d10-5 ell<=16, 30% uneven (a U[0,.95], nr in "
+               "{257,513,1025,2049}, ell U{8..20}, m=-2..2, d10-5)",
+        "steps_per_request": steps,
+        "arrivals": f"Poisson, {rate:.2f}/s (80% of batched capacity)",
+        "p50_time_to_waveform_s": float(np.percentile(latencies, 50)),
+        "p99_time_to_waveform_s": float(np.percentile(latencies, 99)),
+        "throughput": float(sum(work) / makespan),
+        "device_throughput": float(device_rate),
+        "one_at_a_time_device_throughput": float(sum(work) / alone_seconds),
+        "batched_vs_one_at_a_time": float(device_rate / (sum(work) / alone_seconds)),
+        "unit": UNIT,
+        "batched_steps": int(st.steps),
+        "makespan_s": makespan,
+        "rebuilds": int(st.rebuilds),
+        "rebuild_host_s": float(st.rebuild_seconds),
+    }
 
 
 # ---------------------------------------------------------------- CPU side
@@ -343,6 +432,11 @@ def b200_arm(args):
                "d2h_bytes_per_step": 16 * n_end,
                "ms_per_step": e_ms / args.steps}
 
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serving:
+        serving = serving_run(tb, wl, value, args.serve_requests,
+                              args.serve_steps)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         value_cpu, info = cpu_reference_run(config, pulse, dt, args.cpu_seconds)
@@ -367,6 +461,7 @@ def b200_arm(args):
                          "algorithmic_bytes_per_launch": algorithmic_per_launch},
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "serving": serving,
             "gpu_launches": launches,
             "clocks": clocks,
         }

@@ -38,9 +38,10 @@
  *                               slopes in a static device array
  *
  * Batched variants (teuk_b200_batch_*) pack many independent solves of
- * uneven shape into one set of stage launches; they have no single
- * counterpart in the reference, whose driver runs one pipeline per process
- * (include/teuk/solver_driver.hpp:86-353).
+ * uneven shape into one set of stage launches, and the server
+ * (teuk_b200_server_*) admits, advances and retires such solves
+ * continuously; neither has a counterpart in the reference, whose driver
+ * runs one pipeline per process (include/teuk/solver_driver.hpp:86-353).
  *
  * Conventions.  State arrays are complex128 stored as interleaved
  * (real, imag) doubles in the reference's (mode, field, radial, theta)
@@ -272,6 +273,62 @@ int teuk_b200_batch_synchronize(teuk_b200_batch* batch);
 /* Kernel launches issued per RK4 step (for launch accounting). */
 int teuk_b200_batch_launches_per_step(const teuk_b200_batch* batch,
                                       int* launches);
+
+/* ---- serving: continuous batching of solve requests --------------------
+ * No counterpart in the reference (one solve per process).  Requests are
+ * queued by teuk_b200_server_submit and admitted in arrival order while
+ * the device footprint of the admitted set stays within the budget; every
+ * admitted solve keeps its state on the device and advances inside the
+ * shared batched RK4 step; a solve that reaches its step count leaves the
+ * batch with its endpoint waveform records, and its memory and tile slots
+ * go to the next queued requests.  Linear (disabled-source) solves only. */
+typedef struct teuk_b200_server teuk_b200_server;
+
+typedef struct teuk_b200_server_options {
+  int abi_version;          /* TEUK_B200_ABI_VERSION */
+  size_t hbm_budget_bytes;  /* device bytes the admitted solves may hold */
+  int max_active;           /* cap on concurrent solves (0 = no cap) */
+  int graph;                /* replay each batched step from a CUDA graph */
+} teuk_b200_server_options;
+
+typedef struct teuk_b200_server_stats {
+  int queued;                 /* submitted, not admitted yet */
+  int active;                 /* in the batch */
+  int finished;               /* results ready */
+  long long steps;            /* batched steps run */
+  double grid_point_updates;  /* sum over solves of steps * modes * nr * ntheta */
+  double device_seconds;      /* device time of the batched steps */
+  size_t resident_bytes;      /* device bytes of the current batch */
+  int rebuilds;               /* batch layouts built on membership changes */
+  double rebuild_seconds;     /* host time spent building them (incl.
+                                 initial data of admitted solves) */
+} teuk_b200_server_stats;
+
+int teuk_b200_server_create(const teuk_b200_server_options* options,
+                            teuk_b200_server** out);
+int teuk_b200_server_destroy(teuk_b200_server* server);
+/* Queue one solve: Gaussian initial data `pulse`, `steps` RK4 steps of
+ * size dt from time 0.  Validation (the reference's constructor checks and
+ * the budget) happens here; *id identifies the request. */
+int teuk_b200_server_submit(teuk_b200_server* server,
+                            const teuk_b200_config* config,
+                            const teuk_b200_gaussian* pulse, double dt,
+                            int steps, uint64_t* id);
+/* Admit queued requests that fit, run up to `steps` batched RK4 steps
+ * (fewer when every admitted solve finishes), retire finished solves.
+ * *active receives the number of solves still in the batch. */
+int teuk_b200_server_advance(teuk_b200_server* server, int steps,
+                             int* active);
+/* Endpoint waveform records of a finished request (the records
+ * teuk_b200_sample_endpoint gives after the same steps) and its
+ * time-to-waveform in seconds from submit to retirement.  Returns
+ * TEUK_B200_ERR_INVALID_ARGUMENT with "request is not finished" while it
+ * is queued or running. */
+int teuk_b200_server_result(teuk_b200_server* server, uint64_t id,
+                            teuk_b200_waveform_record* out, size_t capacity,
+                            size_t* count, double* latency_seconds);
+int teuk_b200_server_stats_get(const teuk_b200_server* server,
+                               teuk_b200_server_stats* out);
 
 #ifdef __cplusplus
 }

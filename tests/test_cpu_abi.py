@@ -112,3 +112,17 @@ def test_cpp_facade_compiles_and_maps_exceptions(tmp_path):
     assert run.stdout.count("invalid_argument:") == 2
     expected = 0 if cuda_available() else 3
     assert run.returncode == expected, run.stdout + run.stderr
+
+
+def test_server_options_validated_before_device_work():
+    with pytest.raises(tb.InvalidArgument, match="budget must be positive"):
+        tb.Server(hbm_budget_bytes=0)
+    with pytest.raises(tb.InvalidArgument, match="max_active"):
+        tb.Server(hbm_budget_bytes=1 << 30, max_active=-1)
+
+
+@pytest.mark.skipif(cuda_available(), reason="host has a GPU")
+def test_server_has_no_cpu_fallback():
+    with pytest.raises(tb.TeukError) as info:
+        tb.Server(hbm_budget_bytes=1 << 30)
+    assert info.value.status == tb.ERR_CUDA

@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <deque>
 #include <cmath>
 #include <cstring>
 #include <exception>
@@ -16,6 +18,7 @@
 #include <numbers>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "engine.h"
@@ -128,6 +131,16 @@ struct DeviceArray {
       : ptr(other.ptr), count(other.count) {
     other.ptr = nullptr;
     other.count = 0;
+  }
+  DeviceArray& operator=(DeviceArray&& other) noexcept {
+    if (this != &other) {
+      release();
+      ptr = other.ptr;
+      count = other.count;
+      other.ptr = nullptr;
+      other.count = 0;
+    }
+    return *this;
   }
   void allocate(const size_t n) {
     release();
@@ -892,6 +905,282 @@ void initialize_nodal_gaussian(teuk_b200::NodalPipeline& p,
   p.reset_activation();
 }
 
+
+// Device bytes one linear solve holds inside a batch: four band buffers
+// (padded segments), its matrices and the nodal import scratch.
+size_t linear_footprint(const teuk_b200::InstancePlan& plan) {
+  size_t complex_count = 0;
+  size_t matrix = 0;
+  for (const auto& mp : plan.modes) {
+    if (!mp.parent) continue;
+    const size_t count = static_cast<size_t>(plan.config.nr) * 3 *
+                         static_cast<size_t>(mp.n_ell);
+    complex_count += (count + 15) / 16 * 16;
+    matrix += 2 * static_cast<size_t>(mp.n_ell * plan.config.ntheta);
+  }
+  return 4 * complex_count * sizeof(double2) + matrix * sizeof(double) +
+         plan.value_count() * sizeof(double2);
+}
+
+double wall_seconds() {
+  return std::chrono::duration<double>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+struct ServerRequest {
+  uint64_t id = 0;
+  teuk_b200::Config config;
+  std::vector<teuk_b200_gaussian_mode> modes;
+  teuk_b200_gaussian pulse{};
+  double dt = 0.0;
+  int steps = 0;
+  int done = 0;
+  int slot = -1;  // instance index in the current batch, -1 if not in it
+  size_t footprint = 0;
+  double points = 0.0;  // modes * nr * ntheta
+  double submit_time = 0.0;
+  double finish_time = -1.0;
+  std::vector<teuk_b200_waveform_record> records;
+};
+
+// Continuous batching over Batch: admitted solves share one batched RK4
+// step; a change of membership rebuilds the batch layout and moves the band
+// state of every continuing solve into it on the device.
+class Server {
+ public:
+  explicit Server(const teuk_b200_server_options& o) : options_(o) {
+    if (o.abi_version != TEUK_B200_ABI_VERSION) {
+      throw std::invalid_argument("teuk_b200_server_options.abi_version mismatch");
+    }
+    if (o.hbm_budget_bytes == 0) {
+      throw std::invalid_argument("server HBM budget must be positive");
+    }
+    if (o.max_active < 0) {
+      throw std::invalid_argument("server max_active must be nonnegative");
+    }
+    require_device();
+    teuk_b200::check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking),
+                     "cudaStreamCreate");
+  }
+  ~Server() {
+    batch_.reset();
+    for (cudaEvent_t e : events_) cudaEventDestroy(e);
+    if (stream_ != nullptr) cudaStreamDestroy(stream_);
+  }
+
+  uint64_t submit(const teuk_b200_config& raw, const teuk_b200_gaussian& pulse,
+                  const double dt, const int steps) {
+    auto r = std::make_shared<ServerRequest>();
+    r->config = teuk_b200::to_config(raw);
+    const teuk_b200::InstancePlan plan = teuk_b200::build_instance_plan(r->config);
+    if (r->config.source_mode != TEUK_B200_SOURCE_DISABLED) {
+      throw teuk_b200::Unsupported(
+          "the server batches linear (disabled-source) solves only");
+    }
+    if (!std::isfinite(dt) || !(dt > 0.0)) {
+      throw std::invalid_argument("pipeline step requires finite positive time data");
+    }
+    if (steps < 0) throw std::invalid_argument("step count must be nonnegative");
+    if (pulse.mode_count < 0 || (pulse.mode_count > 0 && pulse.modes == nullptr)) {
+      throw std::invalid_argument("Gaussian mode list pointer/count mismatch");
+    }
+    r->footprint = linear_footprint(plan);
+    if (r->footprint > options_.hbm_budget_bytes) {
+      throw std::invalid_argument("solve footprint exceeds the server HBM budget");
+    }
+    r->modes.assign(pulse.modes, pulse.modes + pulse.mode_count);
+    r->pulse = pulse;
+    r->dt = dt;
+    r->steps = steps;
+    r->points = static_cast<double>(r->config.modes.size()) * r->config.nr *
+                r->config.ntheta;
+    r->id = next_id_++;
+    r->submit_time = wall_seconds();
+    requests_[r->id] = r;
+    queue_.push_back(r);
+    return r->id;
+  }
+
+  int advance(const int steps) {
+    if (steps < 0) throw std::invalid_argument("step count must be nonnegative");
+    retire();
+    admit();
+    pending_ = 0;
+    for (int s = 0; s < steps && !active_.empty(); ++s) {
+      step_once();
+      retire();
+      admit();
+    }
+    collect_step_times();
+    return static_cast<int>(active_.size());
+  }
+
+  const ServerRequest& result(const uint64_t id) const {
+    const auto it = requests_.find(id);
+    if (it == requests_.end()) throw std::invalid_argument("unknown request id");
+    if (it->second->finish_time < 0.0) {
+      throw std::invalid_argument("request is not finished");
+    }
+    return *it->second;
+  }
+
+  teuk_b200_server_stats stats() const {
+    teuk_b200_server_stats st{};
+    st.queued = static_cast<int>(queue_.size());
+    st.active = static_cast<int>(active_.size());
+    st.finished = finished_;
+    st.steps = steps_run_;
+    st.grid_point_updates = grid_point_updates_;
+    st.device_seconds = device_seconds_;
+    st.resident_bytes = batch_ ? batch_->device_bytes() : 0;
+    st.rebuilds = rebuilds_;
+    st.rebuild_seconds = rebuild_seconds_;
+    return st;
+  }
+
+ private:
+  void admit() {
+    bool changed = membership_changed_;
+    while (!queue_.empty()) {
+      const auto& r = queue_.front();
+      if (options_.max_active > 0 &&
+          static_cast<int>(active_.size()) >= options_.max_active) {
+        break;
+      }
+      if (active_bytes_ + r->footprint > options_.hbm_budget_bytes) break;
+      active_bytes_ += r->footprint;
+      active_.push_back(r);
+      queue_.pop_front();
+      changed = true;
+    }
+    if (changed) rebuild();
+    membership_changed_ = false;
+  }
+
+  // New batch layout for the admitted set; continuing solves keep their
+  // band state (device-to-device), new ones get their Gaussian data.
+  void rebuild() {
+    if (active_.empty()) {
+      batch_.reset();
+      return;
+    }
+    collect_step_times();
+    const double t0 = wall_seconds();
+    std::vector<teuk_b200::Config> configs;
+    for (const auto& r : active_) configs.push_back(r->config);
+    auto next = std::make_unique<Batch>();
+    next->build(configs);
+    next->stream = stream_;
+    for (size_t i = 0; i < active_.size(); ++i) {
+      ServerRequest& r = *active_[i];
+      const int slot = static_cast<int>(i);
+      if (r.slot >= 0 && batch_) {
+        const auto& from = batch_->instance_segments[static_cast<size_t>(r.slot)];
+        const auto& to = next->instance_segments[i];
+        for (size_t k = 0; k < from.size(); ++k) {
+          const auto& a = batch_->h_seg[static_cast<size_t>(from[k])];
+          const auto& b = next->h_seg[static_cast<size_t>(to[k])];
+          const size_t n = static_cast<size_t>(r.config.nr) * 3 *
+                           static_cast<size_t>(a.n_ell);
+          teuk_b200::check(
+              cudaMemcpyAsync(next->y.ptr + b.offset, batch_->y.ptr + a.offset,
+                              n * sizeof(double2), cudaMemcpyDeviceToDevice,
+                              stream_),
+              "move band state");
+        }
+        next->frozen_dev[i] =
+            std::move(batch_->frozen_dev[static_cast<size_t>(r.slot)]);
+      } else {
+        teuk_b200_gaussian pulse = r.pulse;
+        pulse.modes = r.modes.data();
+        initialize_gaussian(*next, slot, &pulse);
+      }
+      r.slot = slot;
+    }
+    teuk_b200::check(cudaStreamSynchronize(stream_), "server rebuild");
+    batch_ = std::move(next);
+    ++rebuilds_;
+    rebuild_seconds_ += wall_seconds() - t0;
+  }
+
+  // One batched step, bracketed by a pair of events; the host does not
+  // wait for it (a retirement's endpoint read is the next synchronisation).
+  void step_once() {
+    std::vector<double> dts;
+    for (const auto& r : active_) dts.push_back(r->dt);
+    while (events_.size() < 2 * static_cast<size_t>(pending_ + 1)) {
+      cudaEvent_t e = nullptr;
+      teuk_b200::check(cudaEventCreate(&e), "cudaEventCreate");
+      events_.push_back(e);
+    }
+    teuk_b200::check(cudaEventRecord(events_[2 * pending_], stream_), "event");
+    batch_->step(dts, 1, options_.graph != 0);
+    teuk_b200::check(cudaEventRecord(events_[2 * pending_ + 1], stream_),
+                     "event");
+    ++pending_;
+    ++steps_run_;
+    for (const auto& r : active_) {
+      ++r->done;
+      grid_point_updates_ += r->points;
+    }
+  }
+
+  void collect_step_times() {
+    if (pending_ == 0) return;
+    teuk_b200::check(cudaStreamSynchronize(stream_), "server steps");
+    for (int i = 0; i < pending_; ++i) {
+      float ms = 0.0f;
+      teuk_b200::check(cudaEventElapsedTime(&ms, events_[2 * i],
+                                            events_[2 * i + 1]),
+                       "event time");
+      device_seconds_ += 1e-3 * ms;
+    }
+    pending_ = 0;
+  }
+
+  void retire() {
+    std::vector<std::shared_ptr<ServerRequest>> keep;
+    for (const auto& r : active_) {
+      if (r->done < r->steps) {
+        keep.push_back(r);
+        continue;
+      }
+      const teuk_b200::Config& c = r->config;
+      size_t count = 0;
+      r->records.resize(2 * c.modes.size() *
+                        static_cast<size_t>(c.ell_max_first + c.ell_max_second + 2));
+      batch_->sample_endpoint(r->slot, r->records.data(), r->records.size(),
+                              &count);
+      r->records.resize(count);
+      r->finish_time = wall_seconds();
+      r->slot = -1;
+      active_bytes_ -= r->footprint;
+      ++finished_;
+      membership_changed_ = true;
+    }
+    active_.swap(keep);
+  }
+
+  teuk_b200_server_options options_;
+  cudaStream_t stream_ = nullptr;
+  std::vector<cudaEvent_t> events_;  // start / stop pairs of pending steps
+  int pending_ = 0;
+  std::unique_ptr<Batch> batch_;
+  std::deque<std::shared_ptr<ServerRequest>> queue_;
+  std::vector<std::shared_ptr<ServerRequest>> active_;
+  std::unordered_map<uint64_t, std::shared_ptr<ServerRequest>> requests_;
+  uint64_t next_id_ = 1;
+  size_t active_bytes_ = 0;
+  bool membership_changed_ = false;
+  int finished_ = 0;
+  int rebuilds_ = 0;
+  double rebuild_seconds_ = 0.0;
+  long long steps_run_ = 0;
+  double grid_point_updates_ = 0.0;
+  double device_seconds_ = 0.0;
+};
+
 }  // namespace
 
 extern "C" {
@@ -1133,21 +1422,9 @@ int teuk_b200_footprint_bytes(const teuk_b200_config* config, size_t* bytes) {
     require(config != nullptr && bytes != nullptr, "null argument");
     const auto plan =
         teuk_b200::build_instance_plan(teuk_b200::to_config(*config));
-    if (plan.config.source_mode != TEUK_B200_SOURCE_DISABLED) {
-      *bytes = teuk_b200::nodal_footprint_bytes(plan);
-      return;
-    }
-    size_t complex_count = 0;
-    size_t matrix = 0;
-    for (const auto& mp : plan.modes) {
-      if (!mp.parent) continue;
-      size_t count = static_cast<size_t>(plan.config.nr) * 3 *
-                     static_cast<size_t>(mp.n_ell);
-      complex_count += (count + 15) / 16 * 16;
-      matrix += 2 * static_cast<size_t>(mp.n_ell * plan.config.ntheta);
-    }
-    *bytes = 4 * complex_count * sizeof(double2) + matrix * sizeof(double) +
-             plan.value_count() * sizeof(double2);
+    *bytes = plan.config.source_mode != TEUK_B200_SOURCE_DISABLED
+                 ? teuk_b200::nodal_footprint_bytes(plan)
+                 : linear_footprint(plan);
   });
 }
 
@@ -1260,6 +1537,71 @@ int teuk_b200_batch_launches_per_step(const teuk_b200_batch* b,
   return guarded([&] {
     require(b != nullptr && launches != nullptr, "null argument");
     *launches = 4 * static_cast<int>(b->batch->groups.size());
+  });
+}
+
+struct teuk_b200_server {
+  std::unique_ptr<Server> server;
+};
+
+int teuk_b200_server_create(const teuk_b200_server_options* options,
+                            teuk_b200_server** out) {
+  return guarded([&] {
+    require(options != nullptr && out != nullptr, "null argument");
+    auto s = std::make_unique<teuk_b200_server>();
+    s->server = std::make_unique<Server>(*options);
+    *out = s.release();
+  });
+}
+
+int teuk_b200_server_destroy(teuk_b200_server* server) {
+  delete server;
+  return TEUK_B200_OK;
+}
+
+int teuk_b200_server_submit(teuk_b200_server* server,
+                            const teuk_b200_config* config,
+                            const teuk_b200_gaussian* pulse, double dt,
+                            int steps, uint64_t* id) {
+  return guarded([&] {
+    require(server != nullptr && config != nullptr && pulse != nullptr &&
+                id != nullptr,
+            "null argument");
+    *id = server->server->submit(*config, *pulse, dt, steps);
+  });
+}
+
+int teuk_b200_server_advance(teuk_b200_server* server, int steps,
+                             int* active) {
+  return guarded([&] {
+    require(server != nullptr, "null server");
+    const int n = server->server->advance(steps);
+    if (active != nullptr) *active = n;
+  });
+}
+
+int teuk_b200_server_result(teuk_b200_server* server, uint64_t id,
+                            teuk_b200_waveform_record* out, size_t capacity,
+                            size_t* count, double* latency_seconds) {
+  return guarded([&] {
+    require(server != nullptr, "null server");
+    const ServerRequest& r = server->server->result(id);
+    if (count != nullptr) *count = r.records.size();
+    if (latency_seconds != nullptr) {
+      *latency_seconds = r.finish_time - r.submit_time;
+    }
+    if (out == nullptr) return;
+    require(capacity >= r.records.size(),
+            "waveform record capacity is too small");
+    std::copy(r.records.begin(), r.records.end(), out);
+  });
+}
+
+int teuk_b200_server_stats_get(const teuk_b200_server* server,
+                               teuk_b200_server_stats* out) {
+  return guarded([&] {
+    require(server != nullptr && out != nullptr, "null argument");
+    *out = server->server->stats();
   });
 }
 

@@ -500,6 +500,55 @@ __device__ __forceinline__ double2 window_dissipation(
   return acc;
 }
 
+// Hint the L2 to fetch [ptr, ptr + bytes) (bulk prefetch; no completion to
+// wait for, no effect on results).  Sizes are multiples of 16 bytes.
+__device__ __forceinline__ void l2_prefetch(const double2* ptr,
+                                            long long count) {
+  const char* c = reinterpret_cast<const char*>(ptr);
+  long long bytes = count * static_cast<long long>(sizeof(double2));
+  while (bytes > 0) {
+    const unsigned chunk =
+        bytes > 65536 ? 65536u : static_cast<unsigned>(bytes);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                 :
+                 : "l"(c), "r"(chunk)
+                 : "memory");
+    c += chunk;
+    bytes -= chunk;
+  }
+}
+
+// L2 prefetch of what tile t reads from HBM: its slab of RK stage inputs
+// (rows within H of the tile) and the own-row inputs of its RK update.
+__device__ void prefetch_tile(const StageLaunch& p, const int t, const int H,
+                              const bool slab, const bool update) {
+  const TileDesc tile = p.tiles[t];
+  const SegmentDesc seg = p.segments[tile.segment];
+  const int nr = p.instances[seg.instance].nr;
+  const long long rs = 3LL * seg.n_ell;
+  if (slab) {
+    const int s0 = max(0, tile.r0 - H), s1 = min(nr, tile.r1 + H);
+    const long long off = seg.offset + s0 * rs, n = (s1 - s0) * rs;
+    if (p.stage == kStage4) {
+      l2_prefetch(p.kA + off, n);
+    } else {
+      l2_prefetch(p.y + off, n);
+      if (p.stage == kStage2) l2_prefetch(p.kA + off, n);
+      if (p.stage == kStage3) l2_prefetch(p.kB + off, n);
+    }
+  }
+  if (update) {
+    const long long off = seg.offset + tile.r0 * rs;
+    const long long n = (tile.r1 - tile.r0) * rs;
+    if (p.stage == kStage2) l2_prefetch(p.kA + off, n);
+    if (p.stage == kStage3) {
+      l2_prefetch(p.y + off, n);
+      l2_prefetch(p.acc + off, n);
+    }
+    if (p.stage == kStage4) l2_prefetch(p.acc + off, n);
+  }
+}
+
 #ifndef TEUK_ROW_BLOCK
 #define TEUK_ROW_BLOCK 2
 #endif
@@ -538,6 +587,14 @@ __global__ void __launch_bounds__(kThreads, 2)
   double* sinv = Am + L.analysis();
   double* cosv = sinv + L.nt8;
   double* coef = cosv + L.nt8;  // t-rows x kCoefCount
+
+  // L2 prefetches: the own-row RK update inputs of this tile, and the slab
+  // and update inputs of the tile that takes this CTA's slot next
+  if (tid == 0 && p.prefetch_stride > 0) {
+    prefetch_tile(p, blockIdx.x, H, false, true);
+    const int next = blockIdx.x + p.prefetch_stride;
+    if (next < p.tile_count) prefetch_tile(p, next, H, true, true);
+  }
 
   // ---- phase 0: RK stage input over the slab, matrices, coefficients
   {
@@ -918,7 +975,27 @@ cudaError_t launch_typed(const StageLaunch& p, cudaStream_t stream) {
     if (err != cudaSuccess) return err;
     configured_bytes = static_cast<int>(bytes);
   }
-  kernel<<<p.tile_count, kThreads, bytes, stream>>>(p);
+  // resident CTAs for this shared-memory size, cached per size
+  static size_t resident_bytes = 0;
+  static int resident = 0;
+  if (bytes != resident_bytes) {
+    int device = 0, sms = 0, per_sm = 0;
+    cudaError_t err = cudaGetDevice(&device);
+    if (err == cudaSuccess) {
+      err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount,
+                                   device);
+    }
+    if (err == cudaSuccess) {
+      err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel,
+                                                          kThreads, bytes);
+    }
+    if (err != cudaSuccess) return err;
+    resident = sms * per_sm;
+    resident_bytes = bytes;
+  }
+  StageLaunch q = p;
+  q.prefetch_stride = resident;
+  kernel<<<p.tile_count, kThreads, bytes, stream>>>(q);
   return cudaGetLastError();
 }
 

@@ -38,6 +38,9 @@ struct StageLaunch {
   int coef_rows;       // rows of coefficient records
   int max_theta;
   int max_ell;
+  // CTAs resident at once (SMs x CTAs per SM), set by launch_stage: the
+  // tile blockIdx + prefetch_stride starts when this CTA's slot frees up
+  int prefetch_stride;
 };
 
 // Dynamic shared memory bytes for one launch description.

@@ -97,6 +97,29 @@ class Activation(ctypes.Structure):
     ]
 
 
+class _ServerOptions(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_int),
+        ("hbm_budget_bytes", ctypes.c_size_t),
+        ("max_active", ctypes.c_int),
+        ("graph", ctypes.c_int),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("queued", ctypes.c_int),
+        ("active", ctypes.c_int),
+        ("finished", ctypes.c_int),
+        ("steps", ctypes.c_longlong),
+        ("grid_point_updates", ctypes.c_double),
+        ("device_seconds", ctypes.c_double),
+        ("resident_bytes", ctypes.c_size_t),
+        ("rebuilds", ctypes.c_int),
+        ("rebuild_seconds", ctypes.c_double),
+    ]
+
+
 class _GaussianMode(ctypes.Structure):
     _fields_ = [
         ("ell", ctypes.c_int),
@@ -263,6 +286,17 @@ def _load() -> ctypes.CDLL:
         "teuk_b200_batch_set_stream": ([P, P], I),
         "teuk_b200_batch_synchronize": ([P], I),
         "teuk_b200_batch_launches_per_step": ([P, ctypes.POINTER(I)], I),
+        "teuk_b200_server_create": ([ctypes.POINTER(_ServerOptions),
+                                     ctypes.POINTER(P)], I),
+        "teuk_b200_server_destroy": ([P], I),
+        "teuk_b200_server_submit": ([P, ctypes.POINTER(_Config),
+                                     ctypes.POINTER(_Gaussian), D, I,
+                                     ctypes.POINTER(ctypes.c_uint64)], I),
+        "teuk_b200_server_advance": ([P, I, ctypes.POINTER(I)], I),
+        "teuk_b200_server_result": ([P, ctypes.c_uint64,
+                                     ctypes.POINTER(WaveformRecord), SZ,
+                                     ctypes.POINTER(SZ), DP], I),
+        "teuk_b200_server_stats_get": ([P, ctypes.POINTER(ServerStats)], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -421,6 +455,10 @@ class Pipeline:
     def reset_activation(self):
         _check(_lib.teuk_b200_reset_activation(self._handle))
 
+    def set_stream(self, stream_handle: int | None):
+        _check(_lib.teuk_b200_set_stream(self._handle,
+                                         ctypes.c_void_p(stream_handle or 0)))
+
     def synchronize(self):
         _check(_lib.teuk_b200_synchronize(self._handle))
 
@@ -515,3 +553,60 @@ class Batch:
         _check(_lib.teuk_b200_batch_launches_per_step(self._handle,
                                                       ctypes.byref(n)))
         return n.value
+
+
+class Server:
+    """Continuous batching: solves are admitted as memory allows, advance in
+    one shared batched step, and leave with their waveform records."""
+
+    def __init__(self, hbm_budget_bytes: int, max_active: int = 0,
+                 graph: bool = True):
+        opts = _ServerOptions(ABI_VERSION, int(hbm_budget_bytes),
+                              int(max_active), int(graph))
+        handle = ctypes.c_void_p()
+        _check(_lib.teuk_b200_server_create(ctypes.byref(opts),
+                                            ctypes.byref(handle)))
+        self._handle = handle
+
+    def close(self):
+        if getattr(self, "_handle", None):
+            _lib.teuk_b200_server_destroy(self._handle)
+            self._handle = None
+
+    __del__ = close
+
+    def submit(self, config: SolveConfig, pulse: GaussianPulse, dt: float,
+               steps: int) -> int:
+        s, keep = config.to_struct()
+        g, gkeep = pulse.to_struct()
+        rid = ctypes.c_uint64()
+        _check(_lib.teuk_b200_server_submit(self._handle, ctypes.byref(s),
+                                            ctypes.byref(g), dt, steps,
+                                            ctypes.byref(rid)))
+        return rid.value
+
+    def advance(self, steps: int = 1) -> int:
+        active = ctypes.c_int()
+        _check(_lib.teuk_b200_server_advance(self._handle, steps,
+                                             ctypes.byref(active)))
+        return active.value
+
+    def result(self, request_id: int):
+        """(waveform records, time-to-waveform seconds) of a finished
+        request; raises InvalidArgument while it is queued or running."""
+        count = ctypes.c_size_t()
+        latency = ctypes.c_double()
+        _check(_lib.teuk_b200_server_result(self._handle, request_id, None, 0,
+                                            ctypes.byref(count),
+                                            ctypes.byref(latency)))
+        buf = (WaveformRecord * max(count.value, 1))()
+        _check(_lib.teuk_b200_server_result(self._handle, request_id, buf,
+                                            count.value, ctypes.byref(count),
+                                            ctypes.byref(latency)))
+        return _records(buf, count.value), latency.value
+
+    def stats(self) -> ServerStats:
+        st = ServerStats()
+        _check(_lib.teuk_b200_server_stats_get(self._handle, ctypes.byref(st)))
+        return st
+

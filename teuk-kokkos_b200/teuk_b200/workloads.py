@@ -102,6 +102,49 @@ def schwarzschild_quadrupole(seed: int = 20260101):
                                  modes=[(2, 2, amp)]), dt
 
 
+def uneven_instance(rng: np.random.Generator, cfl: float = 0.25):
+    """One solve of the batched uneven-instance mix: spin U[0, 0.95],
+    nr from {257, 513, 1025, 2049}, D10-5, ell_max U{8..20}, m = -2..2
+    (ntheta by the exact-product rule), a Gaussian in ell = 2, m = +-2 with
+    centre U[6M, 14M], width U[0.5M, 1.5M] and amplitude 1e-3."""
+    spin = float(rng.uniform(0.0, 0.95))
+    nr = int(rng.choice([257, 513, 1025, 2049]))
+    ell = int(rng.integers(8, 21))
+    base = SolveConfig(mass=1.0, spin=spin, compactification_length=1.0,
+                       radial_points=nr, theta_nodes=(3 * ell + 2) // 2,
+                       ell_max_first=ell, ell_max_second=ell,
+                       modes=(-2, -1, 0, 1, 2), reduction_damping=0.1,
+                       dissipation=0.0, discretization=D105)
+    dt = cfl_time_step(base, cfl)
+    sigma = min(0.005, 0.9 * dissipation_bound(D105, dt / base.spacing))
+    config = replace(base, dissipation=sigma)
+    center, width = compactified(config, float(rng.uniform(6.0, 14.0)),
+                                 float(rng.uniform(0.5, 1.5)))
+    modes = [(2, m, 1e-3 * complex(rng.standard_normal(), rng.standard_normal()))
+             for m in (-2, 2)]
+    return config, GaussianPulse(center=center, width=width, modes=modes), dt
+
+
+def serving_mix(count: int, seed: int = 20260101):
+    """Request stream for the continuous-batching measurement: 40 %
+    Schwarzschild quadrupoles (nr 257), 30 % Kerr ringdowns (nr 1025),
+    30 % uneven instances; each entry (kind, config, pulse, dt)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for i in range(count):
+        u = rng.uniform()
+        if u < 0.4:
+            config, pulse, dt = schwarzschild_quadrupole(seed + i)
+            out.append(("schwarzschild", config, pulse, dt))
+        elif u < 0.7:
+            config, pulse, dt = kerr_ringdown(seed + i)
+            out.append(("kerr_ringdown", config, pulse, dt))
+        else:
+            config, pulse, dt = uneven_instance(rng)
+            out.append(("uneven", config, pulse, dt))
+    return out
+
+
 def band_noise(config: SolveConfig, seed: int, scale: float = 1e-6):
     """Seeded complex N(0,1) * scale nodal noise on the first-order psi field
     of every parent mode; set_state projects it onto each fixed-m band."""
