@@ -33,6 +33,10 @@
  *                               (include/teuk/spatial_pipeline.hpp:386-420)
  *   teuk_b200_last_error        the std::invalid_argument / runtime_error
  *                               message the reference would throw
+ *   teuk_b200_checkpoint_write / teuk_b200_checkpoint_load
+ *                               write_pipeline_checkpoint /
+ *                               load_pipeline_checkpoint_verified
+ *                               (include/teuk/pipeline_checkpoint.hpp:782-936)
  *   teuk_b200_step_static_scratch
  *                               no counterpart: teuk_b200_step with its RK
  *                               slopes in a static device array
@@ -235,6 +239,23 @@ int teuk_b200_reset_activation(teuk_b200_pipeline* pipeline);
  * pipeline's own stream). */
 int teuk_b200_set_stream(teuk_b200_pipeline* pipeline, void* cuda_stream);
 int teuk_b200_synchronize(teuk_b200_pipeline* pipeline);
+/* Pipeline checkpoint format v5 of the reference: `directory` receives
+ * metadata.txt (key=value provenance, geometry, activation, progress and
+ * the FNV-1a 64 checksum) and state.bin (the 13-field state as interleaved
+ * little-endian binary64).  `time_step` is the run's step, recorded as
+ * provenance.  write_pipeline_checkpoint
+ * (include/teuk/pipeline_checkpoint.hpp:782-857). */
+int teuk_b200_checkpoint_write(teuk_b200_pipeline* pipeline,
+                               const char* directory, double time_step,
+                               double time, uint64_t step);
+/* load_pipeline_checkpoint_verified (pipeline_checkpoint.hpp:869-936):
+ * format, registry, numerical configuration (incl. time_step), geometry,
+ * size, checksum and band-limit checks all pass before the pipeline's
+ * state and activation latch change; *time and *step receive the recorded
+ * progress. */
+int teuk_b200_checkpoint_load(teuk_b200_pipeline* pipeline,
+                              const char* directory, double time_step,
+                              double* time, uint64_t* step);
 /* Device bytes held by one pipeline built from `config` (admission). */
 int teuk_b200_footprint_bytes(const teuk_b200_config* config,
                               size_t* bytes);

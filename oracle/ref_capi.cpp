@@ -18,6 +18,7 @@
 
 #include "teuk/diagnostics.hpp"
 #include "teuk/pipeline_bands.hpp"
+#include "teuk/pipeline_checkpoint.hpp"
 #include "teuk/pipeline_initial_data.hpp"
 #include "teuk/spatial_pipeline.hpp"
 #include "teuk/waveform_output.hpp"
@@ -101,6 +102,7 @@ struct teuk_ref_pipeline {
         sampler(registry, {c.ell_max_first, c.ell_max_second}, c.theta_nodes,
                 c.compactification_length, horizon),
         ell_max_first(c.ell_max_first),
+        config(c),
         background{c.mass, c.spin, c.compactification_length},
         scratch("ref_scratch_state", registry.size(),
                 teuk::point_pipeline_field_count,
@@ -117,6 +119,7 @@ struct teuk_ref_pipeline {
   teuk::SpatialPipeline pipeline;
   teuk::EndpointWaveformSampler sampler;
   int ell_max_first;
+  teuk_b200_config config;  // scalar fields only (mode pointers not kept)
   teuk::KerrParameters background;
   teuk::FieldView scratch;
   teuk::FieldView scratch_out;
@@ -332,6 +335,46 @@ int teuk_ref_sbp_matrix(int disc, int n, double* derivative, double* norm) {
     for (std::size_t row = 0; row < count; ++row) {
       norm[row] = teuk::radial_norm_weight(d, count, row);
     }
+  });
+}
+
+// write_pipeline_checkpoint / load_pipeline_checkpoint_verified
+// (include/teuk/pipeline_checkpoint.hpp:782-936) on the reference pipeline.
+static teuk::PipelineCheckpointConfiguration checkpoint_configuration(
+    const teuk_ref_pipeline& p, const double time_step) {
+  teuk::PipelineCheckpointConfiguration c;
+  c.background = p.background;
+  c.ell_max_first = p.config.ell_max_first;
+  c.ell_max_second = p.config.ell_max_second;
+  c.theta_nodes = p.config.theta_nodes;
+  c.reduction_damping = p.config.reduction_damping;
+  c.dissipation = p.config.dissipation;
+  c.reduction = p.config.reduction == TEUK_B200_STAGE_CONSTRAINED
+                    ? teuk::ReductionEvolution::StageConstrained
+                    : teuk::ReductionEvolution::FreeDamped;
+  c.time_step = time_step;
+  c.source_policy = policy(p.config);
+  c.radial_discretization = discretization(p.config.discretization);
+  return c;
+}
+
+int teuk_ref_checkpoint_write(teuk_ref_pipeline* p, const char* directory,
+                              double time_step, double time, uint64_t step) {
+  return guarded([&] {
+    (void)teuk::write_pipeline_checkpoint(
+        p->execution, directory, p->pipeline, p->registry,
+        checkpoint_configuration(*p, time_step), {time, step});
+  });
+}
+
+int teuk_ref_checkpoint_load(teuk_ref_pipeline* p, const char* directory,
+                             double time_step, double* time, uint64_t* step) {
+  return guarded([&] {
+    const auto metadata = teuk::load_pipeline_checkpoint(
+        p->execution, directory, p->pipeline, p->registry,
+        checkpoint_configuration(*p, time_step));
+    if (time != nullptr) *time = metadata.progress.time;
+    if (step != nullptr) *step = metadata.progress.step;
   });
 }
 

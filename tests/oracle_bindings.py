@@ -59,6 +59,11 @@ def load_ref(threads: bool = False) -> ctypes.CDLL:
         "teuk_ref_transform_matrices": ([I, I, I, I, DP, DP,
                                          ctypes.POINTER(I)], I),
         "teuk_ref_sbp_matrix": ([I, I, DP, DP], I),
+        "teuk_ref_checkpoint_write": ([P, ctypes.c_char_p, D, D,
+                                       ctypes.c_uint64], I),
+        "teuk_ref_checkpoint_load": ([P, ctypes.c_char_p, D,
+                                      ctypes.POINTER(ctypes.c_double),
+                                      ctypes.POINTER(ctypes.c_uint64)], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -142,6 +147,19 @@ class RefPipeline:
         self._check(self.lib.teuk_ref_sample_endpoint(self._handle, buf, cap,
                                                       ctypes.byref(count)))
         return tb._records(buf, count.value)
+
+    def checkpoint_write(self, directory, time_step: float, time: float,
+                         step: int):
+        self._check(self.lib.teuk_ref_checkpoint_write(
+            self._handle, str(directory).encode(), time_step, time, step))
+
+    def checkpoint_load(self, directory, time_step: float):
+        t = ctypes.c_double()
+        n = ctypes.c_uint64()
+        self._check(self.lib.teuk_ref_checkpoint_load(
+            self._handle, str(directory).encode(), time_step, ctypes.byref(t),
+            ctypes.byref(n)))
+        return t.value, n.value
 
     def activation(self) -> tb.Activation:
         a = tb.Activation()

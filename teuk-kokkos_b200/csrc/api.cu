@@ -23,6 +23,7 @@
 
 #include "engine.h"
 #include "kernels.h"
+#include "checkpoint.h"
 #include "second_order.h"
 #include "static_scratch.h"
 #include "teuk_b200.h"
@@ -1414,6 +1415,56 @@ int teuk_b200_synchronize(teuk_b200_pipeline* p) {
     teuk_b200::check(cudaStreamSynchronize(p->nodal ? p->nodal->stream()
                                                      : p->batch->stream),
                      "synchronize");
+  });
+}
+
+int teuk_b200_checkpoint_write(teuk_b200_pipeline* p, const char* directory,
+                               double time_step, double time, uint64_t step) {
+  return guarded([&] {
+    require(p != nullptr && directory != nullptr, "null argument");
+    const teuk_b200::InstancePlan& plan =
+        p->nodal ? p->nodal->plan() : p->batch->plans[0];
+    std::vector<double> state(2 * plan.value_count());
+    teuk_b200::CheckpointActivation a;
+    if (p->nodal) {
+      p->nodal->get_state(state.data(), TEUK_B200_HOST);
+      const auto s = p->nodal->activation();
+      a = {s.active, s.activation_time, s.consecutive_passes,
+           s.last_eligibility_time};
+    } else {
+      p->batch->get_state(0, state.data(), plan.value_count(), TEUK_B200_HOST);
+      a = {plan.active != 0, plan.activation_time, plan.consecutive_passes,
+           plan.last_eligibility_time};
+    }
+    teuk_b200::write_checkpoint(directory, plan, a, time_step, time, step,
+                                state);
+  });
+}
+
+int teuk_b200_checkpoint_load(teuk_b200_pipeline* p, const char* directory,
+                              double time_step, double* time, uint64_t* step) {
+  return guarded([&] {
+    require(p != nullptr && directory != nullptr, "null argument");
+    const teuk_b200::InstancePlan& plan =
+        p->nodal ? p->nodal->plan() : p->batch->plans[0];
+    const teuk_b200::CheckpointContents c =
+        teuk_b200::read_checkpoint(directory, plan, time_step);
+    const teuk_b200_activation a{c.activation.active ? 1 : 0,
+                                 c.activation.activation_time,
+                                 c.activation.consecutive_passes,
+                                 c.activation.last_eligibility_time};
+    if (p->nodal) {
+      p->nodal->set_state(c.state.data(), TEUK_B200_HOST);
+      p->nodal->restore_activation({a.active != 0, a.activation_time,
+                                    a.consecutive_passes,
+                                    a.last_eligibility_time});
+    } else {
+      p->batch->set_state(0, c.state.data(), plan.value_count(),
+                          TEUK_B200_HOST);
+      restore_activation(p->batch->plans[0], a);
+    }
+    if (time != nullptr) *time = c.time;
+    if (step != nullptr) *step = c.step;
   });
 }
 

@@ -267,6 +267,10 @@ def _load() -> ctypes.CDLL:
         "teuk_b200_reset_activation": ([P], I),
         "teuk_b200_set_stream": ([P, P], I),
         "teuk_b200_synchronize": ([P], I),
+        "teuk_b200_checkpoint_write": ([P, ctypes.c_char_p, D, D,
+                                        ctypes.c_uint64], I),
+        "teuk_b200_checkpoint_load": ([P, ctypes.c_char_p, D, DP,
+                                       ctypes.POINTER(ctypes.c_uint64)], I),
         "teuk_b200_footprint_bytes": ([ctypes.POINTER(_Config),
                                        ctypes.POINTER(SZ)], I),
         "teuk_b200_batch_create": ([ctypes.POINTER(_Config), I,
@@ -448,6 +452,21 @@ class Pipeline:
         a = Activation()
         _check(_lib.teuk_b200_get_activation(self._handle, ctypes.byref(a)))
         return a
+
+    def checkpoint_write(self, directory, time_step: float, time: float,
+                         step: int):
+        """Write the reference's checkpoint format v5 into `directory`."""
+        _check(_lib.teuk_b200_checkpoint_write(
+            self._handle, str(directory).encode(), time_step, time, step))
+
+    def checkpoint_load(self, directory, time_step: float):
+        """Verified load of a v5 checkpoint; returns (time, step)."""
+        t = ctypes.c_double()
+        n = ctypes.c_uint64()
+        _check(_lib.teuk_b200_checkpoint_load(
+            self._handle, str(directory).encode(), time_step, ctypes.byref(t),
+            ctypes.byref(n)))
+        return t.value, n.value
 
     def restore_activation(self, a: Activation):
         _check(_lib.teuk_b200_restore_activation(self._handle, ctypes.byref(a)))
