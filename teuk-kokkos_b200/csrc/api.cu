@@ -125,21 +125,25 @@ template <class T>
 struct DeviceArray {
   T* ptr = nullptr;
   size_t count = 0;
+  bool owned = true;  // false: memory lent by a longer-lived owner
   DeviceArray() = default;
   DeviceArray(const DeviceArray&) = delete;
   DeviceArray& operator=(const DeviceArray&) = delete;
   DeviceArray(DeviceArray&& other) noexcept
-      : ptr(other.ptr), count(other.count) {
+      : ptr(other.ptr), count(other.count), owned(other.owned) {
     other.ptr = nullptr;
     other.count = 0;
+    other.owned = true;
   }
   DeviceArray& operator=(DeviceArray&& other) noexcept {
     if (this != &other) {
       release();
       ptr = other.ptr;
       count = other.count;
+      owned = other.owned;
       other.ptr = nullptr;
       other.count = 0;
+      other.owned = true;
     }
     return *this;
   }
@@ -150,12 +154,31 @@ struct DeviceArray {
           "cudaMalloc");
     count = n;
   }
+  void borrow(T* p, const size_t n) {
+    release();
+    ptr = p;
+    count = n;
+    owned = false;
+  }
   void release() {
-    if (ptr != nullptr) cudaFree(ptr);
+    if (ptr != nullptr && owned) cudaFree(ptr);
     ptr = nullptr;
     count = 0;
+    owned = true;
   }
   ~DeviceArray() { release(); }
+};
+
+// Band buffers that outlive one batch layout: two state buffers (the live
+// one and the next layout's) and the three RK slope buffers, grown on
+// demand and lent to each Batch a server builds.
+struct StateArena {
+  DeviceArray<double2> y[2];
+  DeviceArray<double2> kA, kB, acc;
+  int current = 0;  // y[current] holds the live batch's state
+  static void grow(DeviceArray<double2>& a, const size_t n) {
+    if (a.count < n) a.allocate(n + n / 4);
+  }
 };
 
 constexpr int kTargetTileRows = 48;
@@ -190,7 +213,8 @@ struct Batch {
   DeviceArray<int> d_seg_mode;
   DeviceArray<TileDesc> d_tiles;
   DeviceArray<double> d_mat, d_trig;
-  DeviceArray<double2> d_nodal;     // one instance's nodal state
+  DeviceArray<double2> d_nodal;     // one instance's nodal state (lazy)
+  size_t nodal_max = 0;
   DeviceArray<double2> d_endpoint;  // gathered endpoint coefficients
   DeviceArray<int> d_parent_mask;    // per instance, per registry mode
   DeviceArray<int> d_flag;
@@ -214,12 +238,31 @@ struct Batch {
     if (configs.empty()) {
       throw std::invalid_argument("a batch needs at least one solve");
     }
+    std::vector<InstancePlan> planned;
     for (const Config& c : configs) {
       // The reference's construction-time validation runs first, so invalid
       // inputs report the same error whatever their source policy.
-      plans.push_back(build_instance_plan(c));
+      planned.push_back(build_instance_plan(c));
     }
-    for (const Config& c : configs) {
+    build_planned(std::move(planned));
+  }
+
+  double2* nodal_scratch() {
+    if (d_nodal.ptr == nullptr) d_nodal.allocate(nodal_max);
+    return d_nodal.ptr;
+  }
+
+  // Layout and device buffers for already validated plans.  With an arena
+  // the band buffers are borrowed from it (the state buffer that is not
+  // live) instead of allocated.
+  void build_planned(std::vector<InstancePlan> planned,
+                     StateArena* arena = nullptr) {
+    if (planned.empty()) {
+      throw std::invalid_argument("a batch needs at least one solve");
+    }
+    plans = std::move(planned);
+    for (const InstancePlan& plan : plans) {
+      const Config& c = plan.config;
       if (c.source_mode != 0) {
         throw Unsupported(
             "second-order source policies run through teuk_b200_create "
@@ -337,10 +380,22 @@ struct Batch {
     }
 
     // Device allocations.
-    y.allocate(total_complex);
-    kA.allocate(total_complex);
-    kB.allocate(total_complex);
-    acc.allocate(total_complex);
+    if (arena != nullptr) {
+      DeviceArray<double2>& next = arena->y[1 - arena->current];
+      StateArena::grow(next, total_complex);
+      StateArena::grow(arena->kA, total_complex);
+      StateArena::grow(arena->kB, total_complex);
+      StateArena::grow(arena->acc, total_complex);
+      y.borrow(next.ptr, total_complex);
+      kA.borrow(arena->kA.ptr, total_complex);
+      kB.borrow(arena->kB.ptr, total_complex);
+      acc.borrow(arena->acc.ptr, total_complex);
+    } else {
+      y.allocate(total_complex);
+      kA.allocate(total_complex);
+      kB.allocate(total_complex);
+      acc.allocate(total_complex);
+    }
     check(cudaMemset(y.ptr, 0, total_complex * sizeof(double2)), "memset y");
     d_inst.allocate(h_inst.size());
     d_seg.allocate(h_seg.size());
@@ -348,11 +403,10 @@ struct Batch {
     d_tiles.allocate(h_tiles.size());
     d_mat.allocate(std::max<size_t>(h_mat.size(), 1));
     d_trig.allocate(h_trig.size());
-    size_t nodal_max = 0;
+    nodal_max = 0;
     for (const InstancePlan& plan : plans) {
       nodal_max = std::max(nodal_max, plan.value_count());
     }
-    d_nodal.allocate(nodal_max);
     d_endpoint.allocate(std::max<size_t>(h_seg.size(), 1) * 2 *
                         static_cast<size_t>(max_ell));
     std::vector<int> mask;
@@ -442,10 +496,10 @@ struct Batch {
     const size_t bytes = count * sizeof(double2);
     const double2* source = nullptr;
     if (memory == TEUK_B200_HOST) {
-      check(cudaMemcpyAsync(d_nodal.ptr, state, bytes, cudaMemcpyHostToDevice,
+      check(cudaMemcpyAsync(nodal_scratch(), state, bytes, cudaMemcpyHostToDevice,
                             stream),
             "set_state upload");
-      source = d_nodal.ptr;
+      source = nodal_scratch();
     } else if (memory == TEUK_B200_DEVICE) {
       source = reinterpret_cast<const double2*>(state);
     } else {
@@ -489,15 +543,15 @@ struct Batch {
     const size_t bytes = plan.value_count() * sizeof(double2);
     const auto& frozen = frozen_dev[static_cast<size_t>(instance)];
     if (zero_frozen || frozen.ptr == nullptr) {
-      check(cudaMemsetAsync(d_nodal.ptr, 0, bytes, stream), "zero nodal");
+      check(cudaMemsetAsync(nodal_scratch(), 0, bytes, stream), "zero nodal");
     } else {
-      check(cudaMemcpyAsync(d_nodal.ptr, frozen.ptr, bytes,
+      check(cudaMemcpyAsync(nodal_scratch(), frozen.ptr, bytes,
                             cudaMemcpyDeviceToDevice, stream),
             "frozen restore");
     }
     ConvertLaunch c = convert(instance);
     c.modal = modal;
-    c.nodal_out = d_nodal.ptr;
+    c.nodal_out = nodal_scratch();
     check(launch_modal_to_nodal(c, stream), "modal_to_nodal");
   }
 
@@ -511,7 +565,7 @@ struct Batch {
     if (out == nullptr) throw std::invalid_argument("null state pointer");
     assemble_nodal(instance, y.ptr, false);
     const size_t bytes = count * sizeof(double2);
-    check(cudaMemcpyAsync(out, d_nodal.ptr, bytes,
+    check(cudaMemcpyAsync(out, nodal_scratch(), bytes,
                           memory == TEUK_B200_HOST ? cudaMemcpyDeviceToHost
                                                    : cudaMemcpyDeviceToDevice,
                           stream),
@@ -540,10 +594,10 @@ struct Batch {
     const size_t bytes = count * sizeof(double2);
     const double2* source = reinterpret_cast<const double2*>(stage);
     if (memory == TEUK_B200_HOST) {
-      check(cudaMemcpyAsync(d_nodal.ptr, stage, bytes, cudaMemcpyHostToDevice,
+      check(cudaMemcpyAsync(nodal_scratch(), stage, bytes, cudaMemcpyHostToDevice,
                             stream),
             "evaluate_rhs upload");
-      source = d_nodal.ptr;
+      source = nodal_scratch();
     }
     ConvertLaunch c = convert(instance);
     c.nodal_in = source;
@@ -551,7 +605,7 @@ struct Batch {
     check(launch_nodal_to_modal(c, stream), "nodal_to_modal");
     launch_stage_kind(kRhsOnly, kB.ptr);
     assemble_nodal(instance, kA.ptr, true);
-    check(cudaMemcpyAsync(out, d_nodal.ptr, bytes,
+    check(cudaMemcpyAsync(out, nodal_scratch(), bytes,
                           memory == TEUK_B200_HOST ? cudaMemcpyDeviceToHost
                                                    : cudaMemcpyDeviceToDevice,
                           stream),
@@ -610,6 +664,97 @@ struct Batch {
     for (int s = 0; s < steps; ++s) {
       check(cudaGraphLaunch(graph_exec, stream), "graph launch");
     }
+  }
+
+  // Gaussian initial data of one solve computed on the device straight into
+  // its band segments (initialize_compactified_gaussian_pulse,
+  // include/teuk/pipeline_initial_data.hpp:211-339); its frozen fields are
+  // zero.
+  void gaussian_device(const int instance, const double center,
+                       const double width, const bool compact,
+                       const std::vector<int>& ell, const std::vector<int>& m,
+                       const std::vector<double>& re,
+                       const std::vector<double>& im) {
+    check_instance(instance);
+    const InstancePlan& plan = plans[static_cast<size_t>(instance)];
+    const Config& c = plan.config;
+    validate_gaussian(plan, center, width, ell, m);
+    const auto& segs = instance_segments[static_cast<size_t>(instance)];
+    if (segs.empty()) return;
+    const int nr = c.nr;
+    std::vector<double> line(2 * static_cast<size_t>(nr), 0.0);
+    std::vector<double> dline(2 * static_cast<size_t>(nr), 0.0);
+    for (int r = 0; r < nr; ++r) {
+      line[2 * static_cast<size_t>(r)] = gaussian_profile(
+          plan.spacing * static_cast<double>(r), center, width, compact);
+    }
+    sbp_derivative_line(c.disc, line.data(), nr, 1.0 / plan.spacing,
+                        dline.data());
+    std::vector<double> profile(2 * static_cast<size_t>(nr));
+    for (int r = 0; r < nr; ++r) {
+      profile[static_cast<size_t>(r)] = line[2 * static_cast<size_t>(r)];
+      profile[static_cast<size_t>(nr + r)] = dline[2 * static_cast<size_t>(r)];
+    }
+    std::vector<double2> seeds(segs.size() * static_cast<size_t>(max_ell),
+                               make_double2(0.0, 0.0));
+    for (size_t k = 0; k < segs.size(); ++k) {
+      const SegmentDesc& sd = h_seg[static_cast<size_t>(segs[k])];
+      for (size_t i = 0; i < ell.size(); ++i) {
+        if (m[i] != sd.m) continue;
+        double2& v = seeds[k * static_cast<size_t>(max_ell) +
+                           static_cast<size_t>(ell[i] - sd.ell_min)];
+        v.x += re[i];
+        v.y += im[i];
+      }
+    }
+    DeviceArray<double2> d_seeds;
+    DeviceArray<double> d_profile;
+    DeviceArray<unsigned long long> d_worst;
+    d_seeds.allocate(seeds.size());
+    d_profile.allocate(profile.size());
+    d_worst.allocate(1);
+    check(cudaMemcpyAsync(d_seeds.ptr, seeds.data(), seeds.size() * sizeof(double2),
+                          cudaMemcpyHostToDevice, stream),
+          "upload seeds");
+    check(cudaMemcpyAsync(d_profile.ptr, profile.data(),
+                          profile.size() * sizeof(double), cudaMemcpyHostToDevice,
+                          stream),
+          "upload profile");
+    check(cudaMemsetAsync(d_worst.ptr, 0, sizeof(unsigned long long), stream),
+          "zero residual");
+    check(cudaMemsetAsync(d_flag.ptr, 0, sizeof(int), stream), "zero flag");
+    GaussianLaunch g{};
+    g.y = y.ptr;
+    g.segments = d_seg.ptr + segs.front();
+    g.segment_count = static_cast<int>(segs.size());
+    g.instance = h_inst[static_cast<size_t>(instance)];
+    g.matrices = d_mat.ptr;
+    g.trig = d_trig.ptr;
+    g.seeds = d_seeds.ptr;
+    g.profile = d_profile.ptr;
+    g.max_ell = max_ell;
+    g.worst_residual = d_worst.ptr;
+    g.singular = d_flag.ptr;
+    check(launch_gaussian_band(g, stream), "Gaussian initial data");
+    unsigned long long bits = 0;
+    int singular = 0;
+    check(cudaMemcpyAsync(&bits, d_worst.ptr, sizeof(bits), cudaMemcpyDeviceToHost,
+                          stream),
+          "read residual");
+    check(cudaMemcpyAsync(&singular, d_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost,
+                          stream),
+          "read flag");
+    check(cudaStreamSynchronize(stream), "Gaussian initial data");
+    if (singular != 0) {
+      throw std::runtime_error("singular Galerkin initialization matrix");
+    }
+    double worst = 0.0;
+    std::memcpy(&worst, &bits, sizeof(worst));
+    if (!std::isfinite(worst) || worst > 2.0e-12) {
+      throw std::runtime_error(
+          "Galerkin initial-time-derivative solve failed its residual check");
+    }
+    frozen_dev[static_cast<size_t>(instance)].release();
   }
 
   // RK4 steps whose three slope buffers (k1 / stage-4 input, k2, weighted
@@ -875,13 +1020,9 @@ void initialize_gaussian(Batch& b, const int instance,
     re.push_back(pulse->modes[i].amplitude_real);
     im.push_back(pulse->modes[i].amplitude_imag);
   }
-  auto& plan = b.plans[static_cast<size_t>(instance)];
-  std::vector<double> nodal;
-  teuk_b200::gaussian_initial_state(plan, pulse->center, pulse->width,
-                                    pulse->compact_support != 0, ell, m, re,
-                                    im, nodal);
-  b.set_state(instance, nodal.data(), plan.value_count(), TEUK_B200_HOST);
-  reset_activation(plan);
+  b.gaussian_device(instance, pulse->center, pulse->width,
+                    pulse->compact_support != 0, ell, m, re, im);
+  reset_activation(b.plans[static_cast<size_t>(instance)]);
 }
 
 void initialize_nodal_gaussian(teuk_b200::NodalPipeline& p,
@@ -932,6 +1073,7 @@ double wall_seconds() {
 struct ServerRequest {
   uint64_t id = 0;
   teuk_b200::Config config;
+  teuk_b200::InstancePlan plan;  // validated at submit, reused by rebuilds
   std::vector<teuk_b200_gaussian_mode> modes;
   teuk_b200_gaussian pulse{};
   double dt = 0.0;
@@ -966,6 +1108,7 @@ class Server {
   }
   ~Server() {
     batch_.reset();
+    if (stream_ != nullptr) cudaStreamSynchronize(stream_);
     for (cudaEvent_t e : events_) cudaEventDestroy(e);
     if (stream_ != nullptr) cudaStreamDestroy(stream_);
   }
@@ -974,7 +1117,8 @@ class Server {
                   const double dt, const int steps) {
     auto r = std::make_shared<ServerRequest>();
     r->config = teuk_b200::to_config(raw);
-    const teuk_b200::InstancePlan plan = teuk_b200::build_instance_plan(r->config);
+    r->plan = teuk_b200::build_instance_plan(r->config);
+    const teuk_b200::InstancePlan& plan = r->plan;
     if (r->config.source_mode != TEUK_B200_SOURCE_DISABLED) {
       throw teuk_b200::Unsupported(
           "the server batches linear (disabled-source) solves only");
@@ -1068,10 +1212,10 @@ class Server {
     }
     collect_step_times();
     const double t0 = wall_seconds();
-    std::vector<teuk_b200::Config> configs;
-    for (const auto& r : active_) configs.push_back(r->config);
+    std::vector<teuk_b200::InstancePlan> plans;
+    for (const auto& r : active_) plans.push_back(r->plan);
     auto next = std::make_unique<Batch>();
-    next->build(configs);
+    next->build_planned(std::move(plans), &arena_);
     next->stream = stream_;
     for (size_t i = 0; i < active_.size(); ++i) {
       ServerRequest& r = *active_[i];
@@ -1101,6 +1245,7 @@ class Server {
     }
     teuk_b200::check(cudaStreamSynchronize(stream_), "server rebuild");
     batch_ = std::move(next);
+    arena_.current = 1 - arena_.current;
     ++rebuilds_;
     rebuild_seconds_ += wall_seconds() - t0;
   }
@@ -1166,6 +1311,7 @@ class Server {
   teuk_b200_server_options options_;
   cudaStream_t stream_ = nullptr;
   std::vector<cudaEvent_t> events_;  // start / stop pairs of pending steps
+  teuk_b200::StateArena arena_;      // band buffers reused across layouts
   int pending_ = 0;
   std::unique_ptr<Batch> batch_;
   std::deque<std::shared_ptr<ServerRequest>> queue_;

@@ -173,6 +173,15 @@ struct RowCoefficients {
   double c_re, c_im;  // psi coefficient
 };
 
+// Checks of initialize_compactified_gaussian_pulse
+// (include/teuk/pipeline_initial_data.hpp:211-250) with its messages.
+void validate_gaussian(const InstancePlan& plan, double center, double width,
+                       const std::vector<int>& ell,
+                       const std::vector<int>& m_values);
+// Radial profile of the pulse at R (Gaussian, or the compact bump).
+double gaussian_profile(double R, double center, double width,
+                        bool compact_support);
+
 // Gaussian initial data of one instance, nodal (m,13,r,theta) host array in
 // the reference's order; returns the Galerkin residual.
 double gaussian_initial_state(const InstancePlan& plan, double center,

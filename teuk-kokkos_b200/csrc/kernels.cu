@@ -1171,6 +1171,226 @@ cudaError_t launch_frozen_scan(const double2* nodal, const int* parent_mask,
   return cudaGetLastError();
 }
 
+namespace {
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) {
+    v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  }
+  return v;
+}
+
+// doubles of one warp's scratch: the Galerkin matrix and its copy, the
+// right-hand side and its copy, the solution, the seed's nodal values, the
+// 1/C_T factors and the nodal right-hand side
+__host__ __device__ inline int gaussian_warp_doubles(const int ne, const int nt) {
+  return 2 * ne * ne + 6 * ne + 5 * nt;
+}
+
+// initialize_compactified_gaussian_pulse in band space, one warp per
+// (segment, r) row: the Galerkin system of
+// include/teuk/pipeline_initial_data.hpp:142-207 built on the
+// Gauss-Legendre nodes and solved by Gaussian elimination with partial
+// pivoting (first maximal pivot, 128 eps singularity floor) and back
+// substitution, then the relative residual check.
+__global__ void gaussian_band_kernel(const GaussianLaunch p) {
+  extern __shared__ double gsm[];
+  const int warps = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const InstanceDesc& in = p.instance;
+  const int nr = in.nr, nt = in.ntheta;
+  double* base = gsm + warp * gaussian_warp_doubles(p.max_ell, nt);
+  const double* sinv = p.trig + in.trig_offset;
+  const double* cosv = sinv + nt;
+  const double a2 = in.spin * in.spin;
+  const long long rows = static_cast<long long>(p.segment_count) * nr;
+  for (long long row = static_cast<long long>(blockIdx.x) * warps + warp;
+       row < rows; row += static_cast<long long>(gridDim.x) * warps) {
+    const int s = static_cast<int>(row / nr);
+    const int r = static_cast<int>(row - static_cast<long long>(s) * nr);
+    const SegmentDesc seg = p.segments[s];
+    const int ne = seg.n_ell;
+    double* M = base;
+    double* M0 = M + ne * ne;
+    double* rhs = M0 + ne * ne;
+    double* rhs0 = rhs + 2 * ne;
+    double* x = rhs0 + 2 * ne;
+    double* ang = x + 2 * ne;
+    double* inv = ang + 2 * nt;
+    double* nod = inv + nt;
+    const double* St = p.matrices + seg.mat_offset;  // St[l][j]
+    const double* At = St + ne * nt;                 // At[j][l]
+    const double2* seed = p.seeds + static_cast<long long>(s) * p.max_ell;
+    const double prof = p.profile[r], dprof = p.profile[nr + r];
+    double cf[kCoefCount];
+    row_coefficients(in, seg.m, r, cf);
+    for (int j = lane; j < nt; j += 32) {
+      double re = 0.0, im = 0.0;
+      for (int l = 0; l < ne; ++l) {
+        const double sv = St[l * nt + j];
+        re += sv * seed[l].x;
+        im += sv * seed[l].y;
+      }
+      ang[2 * j] = re;
+      ang[2 * j + 1] = im;
+      const double it = 1.0 / (cf[0] - a2 * sinv[j] * sinv[j]);
+      inv[j] = it;
+      const double gre = cf[3];
+      const double gim = cf[4] + 2.0 * (kSpinWeight * in.spin * cosv[j]);
+      const double qre = dprof * re, qim = dprof * im;
+      const double pre = prof * re, pim = prof * im;
+      const double k2 = -2.0 * cf[1];
+      nod[2 * j] = it * (k2 * qre + (gre * pre - gim * pim));
+      nod[2 * j + 1] = it * (k2 * qim + (gre * pim + gim * pre));
+    }
+    __syncwarp();
+    for (int l = lane; l < ne; l += 32) {
+      double re = 0.0, im = 0.0;
+      for (int j = 0; j < nt; ++j) {
+        const double a = At[j * ne + l];
+        re += a * nod[2 * j];
+        im += a * nod[2 * j + 1];
+      }
+      rhs[2 * l] = rhs0[2 * l] = re;
+      rhs[2 * l + 1] = rhs0[2 * l + 1] = im;
+    }
+    double scale = 0.0;
+    for (int idx = lane; idx < ne * ne; idx += 32) {
+      const int i = idx / ne, c = idx - (idx / ne) * ne;
+      double v = 0.0;
+      for (int j = 0; j < nt; ++j) v += At[j * ne + i] * inv[j] * St[c * nt + j];
+      M[idx] = M0[idx] = v;
+      scale = fmax(scale, fabs(v));
+    }
+    scale = warp_max(scale);
+    __syncwarp();
+    const double floor = 128.0 * 2.220446049250313e-16 * scale;
+    bool ok = true;
+    for (int col = 0; col < ne; ++col) {
+      double best = -1.0;
+      int piv = ne;
+      for (int i = col + lane; i < ne; i += 32) {
+        const double v = fabs(M[i * ne + col]);
+        if (v > best) {
+          best = v;
+          piv = i;
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int op = __shfl_xor_sync(0xffffffffu, piv, o);
+        if (ob > best || (ob == best && op < piv)) {
+          best = ob;
+          piv = op;
+        }
+      }
+      if (!isfinite(best) || best <= floor) {
+        if (lane == 0) atomicExch(p.singular, 1);
+        ok = false;
+        break;
+      }
+      if (piv != col) {
+        for (int j = col + lane; j < ne; j += 32) {
+          const double t = M[col * ne + j];
+          M[col * ne + j] = M[piv * ne + j];
+          M[piv * ne + j] = t;
+        }
+        if (lane == 0) {
+          const double tr = rhs[2 * col], ti = rhs[2 * col + 1];
+          rhs[2 * col] = rhs[2 * piv];
+          rhs[2 * col + 1] = rhs[2 * piv + 1];
+          rhs[2 * piv] = tr;
+          rhs[2 * piv + 1] = ti;
+        }
+      }
+      __syncwarp();
+      const double diag = M[col * ne + col];
+      for (int i = col + 1 + lane; i < ne; i += 32) {
+        const double f = M[i * ne + col] / diag;
+        M[i * ne + col] = 0.0;
+        for (int j = col + 1; j < ne; ++j) M[i * ne + j] -= f * M[col * ne + j];
+        rhs[2 * i] -= f * rhs[2 * col];
+        rhs[2 * i + 1] -= f * rhs[2 * col + 1];
+      }
+      __syncwarp();
+    }
+    if (!ok) continue;  // uniform across the warp
+    if (lane == 0) {
+      for (int i = ne - 1; i >= 0; --i) {
+        double re = rhs[2 * i], im = rhs[2 * i + 1];
+        for (int c = i + 1; c < ne; ++c) {
+          re -= M[i * ne + c] * x[2 * c];
+          im -= M[i * ne + c] * x[2 * c + 1];
+        }
+        x[2 * i] = re / M[i * ne + i];
+        x[2 * i + 1] = im / M[i * ne + i];
+      }
+    }
+    __syncwarp();
+    double res2 = 0.0, rhs2 = 0.0;
+    for (int i = lane; i < ne; i += 32) {
+      double re = -rhs0[2 * i], im = -rhs0[2 * i + 1];
+      for (int c = 0; c < ne; ++c) {
+        re += M0[i * ne + c] * x[2 * c];
+        im += M0[i * ne + c] * x[2 * c + 1];
+      }
+      const double h = hypot(re, im), g = hypot(rhs0[2 * i], rhs0[2 * i + 1]);
+      res2 += h * h;
+      rhs2 += g * g;
+    }
+    res2 = warp_sum(res2);
+    rhs2 = warp_sum(rhs2);
+    if (lane == 0) {
+      const double rel = sqrt(res2) / fmax(sqrt(rhs2), 2.2250738585072014e-308);
+      atomicMax(p.worst_residual,
+                static_cast<unsigned long long>(__double_as_longlong(rel)));
+    }
+    double2* yrow = p.y + seg.offset + static_cast<long long>(r) * 3 * ne;
+    for (int l = lane; l < ne; l += 32) {
+      yrow[l] = make_double2(x[2 * l], x[2 * l + 1]);
+      yrow[ne + l] = make_double2(dprof * seed[l].x, dprof * seed[l].y);
+      yrow[2 * ne + l] = make_double2(prof * seed[l].x, prof * seed[l].y);
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace
+
+size_t gaussian_smem_bytes(const int max_ell, const int ntheta,
+                           int* warps_per_block) {
+  const size_t per_warp =
+      sizeof(double) * static_cast<size_t>(gaussian_warp_doubles(max_ell, ntheta));
+  int warps = static_cast<int>((96 * 1024) / per_warp);
+  warps = warps < 1 ? 1 : (warps > 8 ? 8 : warps);
+  if (warps_per_block != nullptr) *warps_per_block = warps;
+  return per_warp * static_cast<size_t>(warps);
+}
+
+cudaError_t launch_gaussian_band(const GaussianLaunch& p, cudaStream_t stream) {
+  int warps = 1;
+  const size_t bytes = gaussian_smem_bytes(p.max_ell, p.instance.ntheta, &warps);
+  static size_t configured = 0;
+  if (bytes > configured) {
+    const cudaError_t err = cudaFuncSetAttribute(
+        gaussian_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        static_cast<int>(bytes));
+    if (err != cudaSuccess) return err;
+    configured = bytes;
+  }
+  const long long rows = static_cast<long long>(p.segment_count) * p.instance.nr;
+  if (rows == 0) return cudaSuccess;
+  long long blocks = (rows + warps - 1) / warps;
+  if (blocks > 65535) blocks = 65535;
+  gaussian_band_kernel<<<static_cast<unsigned>(blocks), 32 * warps, bytes,
+                         stream>>>(p);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_endpoint_gather(const double2* y,
                                    const SegmentDesc* segments,
                                    const InstanceDesc* instances,

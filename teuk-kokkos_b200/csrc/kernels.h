@@ -82,4 +82,26 @@ cudaError_t launch_endpoint_gather(const double2* y,
                                    int segment_count, int max_ell,
                                    double2* out, cudaStream_t stream);
 
+// Gaussian initial data of one solve written straight into band storage
+// (include/teuk/pipeline_initial_data.hpp:142-339 in band space): psi =
+// profile(R) seed, Q = (D profile)(R) seed, and P from the per-row Galerkin
+// system A diag(1/C_T) S p = A [C_T^{-1} (-2K Q + G psi)], solved by one warp
+// per (segment, radial row) with partial pivoting.
+struct GaussianLaunch {
+  double2* y;
+  const SegmentDesc* segments;  // the solve's segments (parents)
+  int segment_count;
+  InstanceDesc instance;
+  const double* matrices;
+  const double* trig;      // sin(theta) then cos(theta) at instance.trig_offset
+  const double2* seeds;    // segment-major, max_ell complex seeds each
+  const double* profile;   // profile(R_r) [nr], then (D profile)(R_r) [nr]
+  int max_ell;
+  unsigned long long* worst_residual;  // bits of the largest relative residual
+  int* singular;                       // set when a pivot falls below the floor
+};
+size_t gaussian_smem_bytes(int max_ell, int ntheta, int* warps_per_block);
+cudaError_t launch_gaussian_band(const GaussianLaunch& launch,
+                                 cudaStream_t stream);
+
 }  // namespace teuk_b200

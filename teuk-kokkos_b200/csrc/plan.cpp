@@ -574,19 +574,12 @@ double relative_residual(const std::vector<Cx>& matrix,
 // fields: psi = profile(R) * S_m seed, Q = D psi with the production radial
 // operator, P from the projected C_T^{-1} Galerkin system (:142-207), then
 // projection of every field onto its band.  Higher fields start at zero.
-double gaussian_initial_state(const InstancePlan& plan, const double center,
-                              const double width, const bool compact_support,
-                              const std::vector<int>& ell,
-                              const std::vector<int>& m_values,
-                              const std::vector<double>& amp_re,
-                              const std::vector<double>& amp_im,
-                              std::vector<double>& nodal) {
+void validate_gaussian(const InstancePlan& plan, const double center,
+                       const double width, const std::vector<int>& ell,
+                       const std::vector<int>& m_values) {
   const Config& c = plan.config;
-  const int nr = c.nr;
-  const int nt = c.ntheta;
-  const std::size_t nmodes = c.modes.size();
   const int ell_max = c.ell_max_first;
-  if (ell_max < 2 || nt < ell_max + 1) {
+  if (ell_max < 2 || c.ntheta < ell_max + 1) {
     throw std::invalid_argument(
         "initial-data angular band does not fit the pipeline grid");
   }
@@ -611,6 +604,28 @@ double gaussian_initial_state(const InstancePlan& plan, const double center,
       }
     }
   }
+}
+
+double gaussian_profile(const double R, const double center,
+                        const double width, const bool compact_support) {
+  const double x = (R - center) / width;
+  if (!compact_support) return std::exp(-x * x);
+  if (std::abs(R - center) >= width) return 0.0;
+  return std::exp(1.0 - 1.0 / (1.0 - x * x));
+}
+
+double gaussian_initial_state(const InstancePlan& plan, const double center,
+                              const double width, const bool compact_support,
+                              const std::vector<int>& ell,
+                              const std::vector<int>& m_values,
+                              const std::vector<double>& amp_re,
+                              const std::vector<double>& amp_im,
+                              std::vector<double>& nodal) {
+  const Config& c = plan.config;
+  const int nr = c.nr;
+  const int nt = c.ntheta;
+  const std::size_t nmodes = c.modes.size();
+  validate_gaussian(plan, center, width, ell, m_values);
   const auto at = [&](const std::size_t mode, const int field, const int r,
                       const int j) -> std::size_t {
     return 2 * (((mode * kFieldCount + static_cast<std::size_t>(field)) *
@@ -621,10 +636,7 @@ double gaussian_initial_state(const InstancePlan& plan, const double center,
   };
   nodal.assign(2 * plan.value_count(), 0.0);
   const auto profile = [&](const double R) {
-    const double x = (R - center) / width;
-    if (!compact_support) return std::exp(-x * x);
-    if (std::abs(R - center) >= width) return 0.0;
-    return std::exp(1.0 - 1.0 / (1.0 - x * x));
+    return gaussian_profile(R, center, width, compact_support);
   };
   // psi
   for (std::size_t mode = 0; mode < nmodes; ++mode) {
