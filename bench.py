@@ -339,20 +339,15 @@ def build_batch(tb, wl, config, pulse, batch_size, seed0, pinned):
 
 def b200_arm(args):
     import torch
-    import torch.distributed as dist
 
     import teuk_b200 as tb
+    from teuk_b200 import distributed as td
     from teuk_b200 import workloads as wl
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    info = td.rank_info()
+    world, rank, local = info.world_size, info.rank, info.local_rank
     torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    td.init("nccl", device=torch.device("cuda", local))
 
     meta, config, pulse, dt = workload_config(args.batch)
     shape = config.shape()
@@ -363,9 +358,7 @@ def b200_arm(args):
     batch.set_stream(stream.cuda_stream)
     dts = [dt] * B
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
+    barrier = td.barrier
 
     # warm-up (graph capture happens here)
     batch.step(dts, steps=max(args.warmup, 0), graph=True)
@@ -385,12 +378,10 @@ def b200_arm(args):
     barrier()
     clocks = sampler.stop()
     ms = start.elapsed_time(end)
-    elapsed = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(elapsed, op=dist.ReduceOp.MAX)
-    ms_max = float(elapsed.item())
     gp = wl.grid_points(config)
-    value = world * B * gp * args.steps / (ms_max / 1e3)
+    # every rank advanced its own B solves: whole-job units / slowest rank
+    value, slowest = td.whole_job_rate(B * gp * args.steps, ms / 1e3, "cuda")
+    ms_max = slowest * 1e3
     launches_per_step = batch.launches_per_step()
 
     # roofline of the stage kernel (four launches per RK4 step)
@@ -421,13 +412,11 @@ def b200_arm(args):
         e_end.record(stream)
         e_end.synchronize()
         barrier()
-        e_ms = torch.tensor([e_start.elapsed_time(e_end)], dtype=torch.float64,
-                            device="cuda")
-        if world > 1:
-            dist.all_reduce(e_ms, op=dist.ReduceOp.MAX)
-        e_ms = float(e_ms.item())
+        e_value, e_slowest = td.whole_job_rate(
+            B * gp * args.steps, e_start.elapsed_time(e_end) / 1e3, "cuda")
+        e_ms = e_slowest * 1e3
         state_bytes = wl.state_bytes(config) * B
-        e2e = {"value": world * B * gp * args.steps / (e_ms / 1e3), "unit": UNIT,
+        e2e = {"value": e_value, "unit": UNIT,
                "h2d_bytes_per_step": (state_bytes + 8 * B) / args.steps,
                "d2h_bytes_per_step": 16 * n_end,
                "ms_per_step": e_ms / args.steps}
@@ -467,8 +456,7 @@ def b200_arm(args):
         }
         print(json.dumps(line), flush=True)
     batch.close()
-    if world > 1:
-        dist.destroy_process_group()
+    td.finalize()
 
 
 def main():
