@@ -37,6 +37,10 @@
  *                               write_pipeline_checkpoint /
  *                               load_pipeline_checkpoint_verified
  *                               (include/teuk/pipeline_checkpoint.hpp:782-936)
+ *   teuk_b200_parse_run_config / teuk_b200_resolved_config
+ *                               parse_run_configuration_text /
+ *                               resolved_configuration_text
+ *                               (include/teuk/config.hpp:683-831)
  *   teuk_b200_step_static_scratch
  *                               no counterpart: teuk_b200_step with its RK
  *                               slopes in a static device array
@@ -294,6 +298,56 @@ int teuk_b200_batch_synchronize(teuk_b200_batch* batch);
 /* Kernel launches issued per RK4 step (for launch accounting). */
 int teuk_b200_batch_launches_per_step(const teuk_b200_batch* batch,
                                       int* launches);
+
+/* ---- runtime configuration (.cfg) --------------------------------------
+ * The teuk_solver schema (include/teuk/config.hpp): `key = value` lines,
+ * '#' comments, `key=value` command-line overrides, unknown keys rejected,
+ * the reference's defaults, validation order and messages.  The plus2
+ * companion keys are accepted and validated as schema only. */
+#define TEUK_B200_MAX_MODES 64
+#define TEUK_B200_MAX_SEEDS 64
+#define TEUK_B200_PATH_CAPACITY 1024
+
+typedef struct teuk_b200_run_config {
+  int abi_version;                /* TEUK_B200_ABI_VERSION */
+  double mass, spin, compactification_length;
+  int radial_points, theta_nodes, ell_max_first, ell_max_second;
+  int mode_count, modes[TEUK_B200_MAX_MODES];       /* stored registry */
+  int parent_count, parents[TEUK_B200_MAX_MODES];   /* first_order_modes */
+  int target_count, targets[TEUK_B200_MAX_MODES];   /* second_order_modes */
+  double reduction_damping, dissipation;
+  int reduction, discretization;
+  int source_mode;  /* disabled unless second_order.enabled */
+  double source_start_time, normalized_constraint_tolerance;
+  int required_consecutive_passes;
+  double final_time;
+  int steps;
+  double cfl;
+  double time_step;               /* final_time / steps */
+  int initial_data_type;          /* 0 gaussian, 1 checkpoint */
+  double center, width;           /* compactified radii (fraction * R_H) */
+  int compact_support;
+  int seed_count;                 /* after the sharp-partner expansion */
+  teuk_b200_gaussian_mode seeds[TEUK_B200_MAX_SEEDS];
+  char checkpoint_directory[TEUK_B200_PATH_CAPACITY];
+  char output_directory[TEUK_B200_PATH_CAPACITY];
+  int diagnostic_every, checkpoint_every;
+} teuk_b200_run_config;
+
+/* parse_run_configuration_text: `text` is the .cfg content, `overrides`
+ * are `key=value` strings applied on top. */
+int teuk_b200_parse_run_config(const char* text, const char* const* overrides,
+                               int override_count, teuk_b200_run_config* out);
+/* The pipeline configuration of a parsed run (make_run_mode_registry,
+ * make_source_policy); its mode pointers refer to `run`'s arrays. */
+int teuk_b200_run_pipeline_config(const teuk_b200_run_config* run,
+                                  teuk_b200_config* out);
+/* resolved_configuration_text of the parsed run (the body of
+ * resolved_config.cfg); *length receives the byte count (excluding the
+ * terminating zero written when it fits). */
+int teuk_b200_resolved_config(const char* text, const char* const* overrides,
+                              int override_count, char* out, size_t capacity,
+                              size_t* length);
 
 /* ---- serving: continuous batching of solve requests --------------------
  * No counterpart in the reference (one solve per process).  Requests are

@@ -9,6 +9,7 @@
 #include <Kokkos_Core.hpp>
 
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <exception>
 #include <memory>
@@ -16,7 +17,9 @@
 #include <string>
 #include <vector>
 
+#include "teuk/config.hpp"
 #include "teuk/diagnostics.hpp"
+#include "teuk/initial_data_factory.hpp"
 #include "teuk/pipeline_bands.hpp"
 #include "teuk/pipeline_checkpoint.hpp"
 #include "teuk/pipeline_initial_data.hpp"
@@ -375,6 +378,92 @@ int teuk_ref_checkpoint_load(teuk_ref_pipeline* p, const char* directory,
         checkpoint_configuration(*p, time_step));
     if (time != nullptr) *time = metadata.progress.time;
     if (step != nullptr) *step = metadata.progress.step;
+  });
+}
+
+// parse_run_configuration_text / resolved_configuration_text
+// (include/teuk/config.hpp:683-831) and the registry / policy / Gaussian
+// mapping of initial_data_factory.hpp:16-79, for parity tests of the
+// engine's own parser.
+static std::vector<std::string> ref_overrides(const char* const* overrides,
+                                              const int count) {
+  std::vector<std::string> out;
+  for (int i = 0; i < count; ++i) out.emplace_back(overrides[i]);
+  return out;
+}
+
+int teuk_ref_resolved_config(const char* text, const char* const* overrides,
+                             int override_count, char* out, size_t capacity,
+                             size_t* length) {
+  return guarded([&] {
+    const std::string resolved = teuk::resolved_configuration_text(
+        teuk::parse_run_configuration_text(
+            text, ref_overrides(overrides, override_count)));
+    *length = resolved.size();
+    if (out != nullptr && capacity > resolved.size()) {
+      std::memcpy(out, resolved.c_str(), resolved.size() + 1);
+    }
+  });
+}
+
+int teuk_ref_parse_run_config(const char* text, const char* const* overrides,
+                              int override_count, teuk_b200_run_config* out) {
+  return guarded([&] {
+    const teuk::RunParameters run = teuk::parse_run_configuration_text(
+        text, ref_overrides(overrides, override_count));
+    const teuk::ModeRegistry registry = teuk::make_run_mode_registry(run);
+    const teuk::SecondOrderSourcePolicy policy = teuk::make_source_policy(run);
+    teuk_b200_run_config r{};
+    r.abi_version = TEUK_B200_ABI_VERSION;
+    r.mass = run.background.mass;
+    r.spin = run.background.spin;
+    r.compactification_length = run.background.compactification_length;
+    r.radial_points = run.grid.radial_points;
+    r.theta_nodes = run.grid.theta_points;
+    r.ell_max_first = run.grid.ell_max_first;
+    r.ell_max_second = run.grid.ell_max_second;
+    r.mode_count = static_cast<int>(registry.modes().size());
+    std::copy(registry.modes().begin(), registry.modes().end(), r.modes);
+    r.parent_count = static_cast<int>(registry.parents().size());
+    std::copy(registry.parents().begin(), registry.parents().end(), r.parents);
+    r.target_count = static_cast<int>(registry.targets().size());
+    std::copy(registry.targets().begin(), registry.targets().end(), r.targets);
+    r.reduction_damping = run.method.reduction_damping;
+    r.dissipation = run.method.dissipation;
+    r.reduction = run.method.reduction == teuk::ReductionEvolution::StageConstrained;
+    r.discretization = static_cast<int>(run.method.radial_discretization);
+    r.source_mode = static_cast<int>(policy.mode);
+    r.source_start_time = policy.source_start_time;
+    r.normalized_constraint_tolerance = policy.normalized_constraint_tolerance;
+    r.required_consecutive_passes = policy.required_consecutive_passes;
+    r.final_time = run.time.final_time;
+    r.steps = run.time.steps;
+    r.cfl = run.time.cfl;
+    r.time_step = run.time.final_time / static_cast<double>(run.time.steps);
+    r.initial_data_type =
+        run.initial_data.type == teuk::InitialDataType::Checkpoint ? 1 : 0;
+    const double horizon =
+        run.background.compactification_length *
+        run.background.compactification_length /
+        teuk::outer_horizon_radius(run.background.mass, run.background.spin);
+    r.center = run.initial_data.center_fraction * horizon;
+    r.width = run.initial_data.width_fraction * horizon;
+    r.compact_support = run.initial_data.compact_support ? 1 : 0;
+    if (run.initial_data.type == teuk::InitialDataType::Gaussian) {
+      const auto seeds = teuk::expanded_gaussian_modes(run.initial_data);
+      r.seed_count = static_cast<int>(seeds.size());
+      for (std::size_t i = 0; i < seeds.size(); ++i) {
+        r.seeds[i] = {seeds[i].ell, seeds[i].m, seeds[i].amplitude.real(),
+                      seeds[i].amplitude.imag()};
+      }
+    }
+    std::snprintf(r.checkpoint_directory, sizeof(r.checkpoint_directory), "%s",
+                  run.initial_data.checkpoint_directory.c_str());
+    std::snprintf(r.output_directory, sizeof(r.output_directory), "%s",
+                  run.output.directory.c_str());
+    r.diagnostic_every = run.output.diagnostic_interval;
+    r.checkpoint_every = run.output.checkpoint_interval;
+    *out = r;
   });
 }
 

@@ -311,3 +311,44 @@ def oracle_gauss_legendre(n: int):
     assert lib.oracle_gauss_legendre(n, x.ctypes.data_as(dp),
                                      w.ctypes.data_as(dp)) == 0
     return x, w
+
+
+def _ref_config_calls():
+    lib = load_ref()
+    if not hasattr(lib, "_config_ready"):
+        CP = ctypes.POINTER(ctypes.c_char_p)
+        lib.teuk_ref_resolved_config.argtypes = [
+            ctypes.c_char_p, CP, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t,
+            ctypes.POINTER(ctypes.c_size_t)]
+        lib.teuk_ref_resolved_config.restype = ctypes.c_int
+        lib.teuk_ref_parse_run_config.argtypes = [
+            ctypes.c_char_p, CP, ctypes.c_int, ctypes.POINTER(tb.RunConfig)]
+        lib.teuk_ref_parse_run_config.restype = ctypes.c_int
+        lib._config_ready = True
+    return lib
+
+
+def ref_resolved_config(text: str, overrides=()):
+    """(status, resolved text or error message) from the reference parser."""
+    lib = _ref_config_calls()
+    arr, n = tb._override_array(overrides)
+    length = ctypes.c_size_t()
+    status = lib.teuk_ref_resolved_config(text.encode(), arr, n, None, 0,
+                                          ctypes.byref(length))
+    if status != 0:
+        return status, lib.teuk_ref_last_error().decode()
+    buf = ctypes.create_string_buffer(length.value + 1)
+    lib.teuk_ref_resolved_config(text.encode(), arr, n, buf, length.value + 1,
+                                 ctypes.byref(length))
+    return 0, buf.value.decode()
+
+
+def ref_parse_run_config(text: str, overrides=()):
+    lib = _ref_config_calls()
+    arr, n = tb._override_array(overrides)
+    out = tb.RunConfig()
+    status = lib.teuk_ref_parse_run_config(text.encode(), arr, n,
+                                           ctypes.byref(out))
+    if status != 0:
+        raise RefError(lib.teuk_ref_last_error().decode())
+    return out

@@ -21,10 +21,11 @@ REPO = PACKAGE.parent
 CSRC = PACKAGE / "csrc"
 LIB_DIR = PACKAGE / "lib"
 LIBRARY = LIB_DIR / "libteuk_b200.so"
-SOURCES = ["plan.cpp", "checkpoint.cpp", "kernels.cu", "second_order.cu",
+SOURCES = ["plan.cpp", "checkpoint.cpp", "run_config.cpp", "kernels.cu",
+           "second_order.cu",
            "static_scratch.cu", "api.cu"]
 HEADERS = ["engine.h", "kernels.h", "second_order.h", "static_scratch.h",
-           "checkpoint.h", "sbp_tables.h"]
+           "checkpoint.h", "run_config.h", "sbp_tables.h"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

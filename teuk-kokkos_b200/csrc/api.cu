@@ -24,6 +24,7 @@
 #include "engine.h"
 #include "kernels.h"
 #include "checkpoint.h"
+#include "run_config.h"
 #include "second_order.h"
 #include "static_scratch.h"
 #include "teuk_b200.h"
@@ -1611,6 +1612,136 @@ int teuk_b200_checkpoint_load(teuk_b200_pipeline* p, const char* directory,
     }
     if (time != nullptr) *time = c.time;
     if (step != nullptr) *step = c.step;
+  });
+}
+
+namespace {
+
+std::vector<std::string> override_list(const char* const* overrides,
+                                       const int count) {
+  require(count >= 0 && (count == 0 || overrides != nullptr),
+          "override list pointer/count mismatch");
+  std::vector<std::string> out;
+  for (int i = 0; i < count; ++i) {
+    require(overrides[i] != nullptr, "null override");
+    out.emplace_back(overrides[i]);
+  }
+  return out;
+}
+
+void copy_path(char* dst, const std::string& src) {
+  if (src.size() >= TEUK_B200_PATH_CAPACITY) {
+    throw std::invalid_argument("configuration path exceeds the C ABI capacity");
+  }
+  std::memcpy(dst, src.c_str(), src.size() + 1);
+}
+
+}  // namespace
+
+int teuk_b200_parse_run_config(const char* text, const char* const* overrides,
+                               int override_count, teuk_b200_run_config* out) {
+  return guarded([&] {
+    require(text != nullptr && out != nullptr, "null argument");
+    const teuk_b200::RunParameters run = teuk_b200::parse_run_configuration(
+        text, override_list(overrides, override_count));
+    const teuk_b200::Config c = teuk_b200::pipeline_config(run);
+    // seeds only describe Gaussian initial data
+    const auto seeds = run.initial_type == 0
+                           ? teuk_b200::expanded_seeds(run)
+                           : std::vector<teuk_b200::RunSeed>{};
+    if (c.modes.size() > TEUK_B200_MAX_MODES ||
+        seeds.size() > TEUK_B200_MAX_SEEDS) {
+      throw std::invalid_argument("configuration exceeds the C ABI capacity");
+    }
+    teuk_b200_run_config r{};
+    r.abi_version = TEUK_B200_ABI_VERSION;
+    r.mass = c.mass;
+    r.spin = c.spin;
+    r.compactification_length = c.length;
+    r.radial_points = c.nr;
+    r.theta_nodes = c.ntheta;
+    r.ell_max_first = c.ell_max_first;
+    r.ell_max_second = c.ell_max_second;
+    r.mode_count = static_cast<int>(c.modes.size());
+    std::copy(c.modes.begin(), c.modes.end(), r.modes);
+    r.parent_count = static_cast<int>(c.parents.size());
+    std::copy(c.parents.begin(), c.parents.end(), r.parents);
+    r.target_count = static_cast<int>(c.targets.size());
+    std::copy(c.targets.begin(), c.targets.end(), r.targets);
+    r.reduction_damping = c.damping;
+    r.dissipation = c.dissipation;
+    r.reduction = c.reduction;
+    r.discretization = c.disc;
+    r.source_mode = c.source_mode;
+    r.source_start_time = c.source_start_time;
+    r.normalized_constraint_tolerance = c.constraint_tolerance;
+    r.required_consecutive_passes = c.required_passes;
+    r.final_time = run.final_time;
+    r.steps = run.steps;
+    r.cfl = run.cfl;
+    r.time_step = teuk_b200::run_time_step(run);
+    r.initial_data_type = run.initial_type;
+    const double horizon =
+        c.length * c.length / teuk_b200::outer_horizon_radius(c.mass, c.spin);
+    r.center = run.center_fraction * horizon;
+    r.width = run.width_fraction * horizon;
+    r.compact_support = run.compact_support ? 1 : 0;
+    r.seed_count = static_cast<int>(seeds.size());
+    for (size_t i = 0; i < seeds.size(); ++i) {
+      r.seeds[i] = {seeds[i].ell, seeds[i].m, seeds[i].amplitude.real(),
+                    seeds[i].amplitude.imag()};
+    }
+    copy_path(r.checkpoint_directory, run.checkpoint_directory);
+    copy_path(r.output_directory, run.output_directory);
+    r.diagnostic_every = run.diagnostic_every;
+    r.checkpoint_every = run.checkpoint_every;
+    *out = r;
+  });
+}
+
+int teuk_b200_run_pipeline_config(const teuk_b200_run_config* run,
+                                  teuk_b200_config* out) {
+  return guarded([&] {
+    require(run != nullptr && out != nullptr, "null argument");
+    teuk_b200_config c{};
+    c.abi_version = TEUK_B200_ABI_VERSION;
+    c.mass = run->mass;
+    c.spin = run->spin;
+    c.compactification_length = run->compactification_length;
+    c.radial_points = run->radial_points;
+    c.theta_nodes = run->theta_nodes;
+    c.ell_max_first = run->ell_max_first;
+    c.ell_max_second = run->ell_max_second;
+    c.mode_count = run->mode_count;
+    c.modes = run->modes;
+    c.parent_count = run->parent_count;
+    c.parents = run->parents;
+    c.target_count = run->target_count;
+    c.targets = run->targets;
+    c.reduction_damping = run->reduction_damping;
+    c.dissipation = run->dissipation;
+    c.reduction = run->reduction;
+    c.discretization = run->discretization;
+    c.source_mode = run->source_mode;
+    c.source_start_time = run->source_start_time;
+    c.normalized_constraint_tolerance = run->normalized_constraint_tolerance;
+    c.required_consecutive_passes = run->required_consecutive_passes;
+    *out = c;
+  });
+}
+
+int teuk_b200_resolved_config(const char* text, const char* const* overrides,
+                              int override_count, char* out, size_t capacity,
+                              size_t* length) {
+  return guarded([&] {
+    require(text != nullptr, "null argument");
+    const std::string resolved = teuk_b200::resolved_configuration_text(
+        teuk_b200::parse_run_configuration(
+            text, override_list(overrides, override_count)));
+    if (length != nullptr) *length = resolved.size();
+    if (out == nullptr) return;
+    require(capacity > resolved.size(), "resolved configuration capacity is too small");
+    std::memcpy(out, resolved.c_str(), resolved.size() + 1);
   });
 }
 

@@ -1160,6 +1160,7 @@ NodalPipeline::NodalPipeline(const InstancePlan& plan)
 }
 
 NodalPipeline::~NodalPipeline() {
+  for (StepGraph& g : graphs_) release_graph(g);
   buf_.reset();
   if (own_stream_ != nullptr) cudaStreamDestroy(own_stream_);
 }
@@ -1498,6 +1499,37 @@ void NodalPipeline::consider_activation(const double accepted_time) {
 // (include/teuk/spatial_pipeline.hpp:1291-1310, device_rk4.hpp:84-128)
 void NodalPipeline::advance_fixed(const double, const double dt) {
   if (!(dt > 0.0)) return;
+  // One RK4 step is replayed from a CUDA graph per (latch state, dt,
+  // stream): the latch is host state read while the step is recorded, and
+  // it only changes between steps.
+  StepGraph& g = graphs_[activation_.active ? 1 : 0];
+  if (g.exec == nullptr || g.dt != dt || g.stream != stream_) {
+    release_graph(g);
+    check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal),
+          "begin step capture");
+    try {
+      record_step(dt);
+    } catch (...) {
+      cudaGraph_t discard = nullptr;
+      cudaStreamEndCapture(stream_, &discard);
+      if (discard != nullptr) cudaGraphDestroy(discard);
+      throw;
+    }
+    check(cudaStreamEndCapture(stream_, &g.graph), "end step capture");
+    check(cudaGraphInstantiate(&g.exec, g.graph, 0), "instantiate step");
+    g.dt = dt;
+    g.stream = stream_;
+  }
+  check(cudaGraphLaunch(g.exec, stream_), "step graph launch");
+}
+
+void NodalPipeline::release_graph(StepGraph& g) {
+  if (g.exec != nullptr) cudaGraphExecDestroy(g.exec);
+  if (g.graph != nullptr) cudaGraphDestroy(g.graph);
+  g = StepGraph{};
+}
+
+void NodalPipeline::record_step(const double dt) {
   Buffers& b = *buf_;
   const long long n = static_cast<long long>(value_count());
   const int grid = grid_for(n);

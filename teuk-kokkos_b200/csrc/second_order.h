@@ -93,6 +93,14 @@ class NodalPipeline {
   void evaluate(const double2* stage, double2* out);
   void consider_activation(double accepted_time);
   void advance_fixed(double time, double dt);
+  struct StepGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    double dt = 0.0;
+    cudaStream_t stream = nullptr;
+  };
+  void record_step(double dt);
+  static void release_graph(StepGraph& g);
   ConstraintNorms sample_constraints();
   void sync_check(const char* what);
 
@@ -105,6 +113,7 @@ class NodalPipeline {
   std::vector<double> matrices_;
   SourceActivation activation_;
   ConstraintNorms norms_;
+  StepGraph graphs_[2];  // latch off / on
   cudaStream_t own_stream_ = nullptr;
   cudaStream_t stream_ = nullptr;
   std::unique_ptr<Buffers> buf_;

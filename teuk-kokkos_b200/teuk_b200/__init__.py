@@ -139,6 +139,80 @@ class _Gaussian(ctypes.Structure):
     ]
 
 
+MAX_MODES = 64
+MAX_SEEDS = 64
+PATH_CAPACITY = 1024
+
+
+class RunConfig(ctypes.Structure):
+    """teuk_b200_run_config: a parsed and validated .cfg run."""
+    _fields_ = [
+        ("abi_version", ctypes.c_int),
+        ("mass", ctypes.c_double),
+        ("spin", ctypes.c_double),
+        ("compactification_length", ctypes.c_double),
+        ("radial_points", ctypes.c_int),
+        ("theta_nodes", ctypes.c_int),
+        ("ell_max_first", ctypes.c_int),
+        ("ell_max_second", ctypes.c_int),
+        ("mode_count", ctypes.c_int),
+        ("modes", ctypes.c_int * MAX_MODES),
+        ("parent_count", ctypes.c_int),
+        ("parents", ctypes.c_int * MAX_MODES),
+        ("target_count", ctypes.c_int),
+        ("targets", ctypes.c_int * MAX_MODES),
+        ("reduction_damping", ctypes.c_double),
+        ("dissipation", ctypes.c_double),
+        ("reduction", ctypes.c_int),
+        ("discretization", ctypes.c_int),
+        ("source_mode", ctypes.c_int),
+        ("source_start_time", ctypes.c_double),
+        ("normalized_constraint_tolerance", ctypes.c_double),
+        ("required_consecutive_passes", ctypes.c_int),
+        ("final_time", ctypes.c_double),
+        ("steps", ctypes.c_int),
+        ("cfl", ctypes.c_double),
+        ("time_step", ctypes.c_double),
+        ("initial_data_type", ctypes.c_int),
+        ("center", ctypes.c_double),
+        ("width", ctypes.c_double),
+        ("compact_support", ctypes.c_int),
+        ("seed_count", ctypes.c_int),
+        ("seeds", _GaussianMode * MAX_SEEDS),
+        ("checkpoint_directory", ctypes.c_char * PATH_CAPACITY),
+        ("output_directory", ctypes.c_char * PATH_CAPACITY),
+        ("diagnostic_every", ctypes.c_int),
+        ("checkpoint_every", ctypes.c_int),
+    ]
+
+    def solve_config(self) -> "SolveConfig":
+        return SolveConfig(
+            mass=self.mass, spin=self.spin,
+            compactification_length=self.compactification_length,
+            radial_points=self.radial_points, theta_nodes=self.theta_nodes,
+            ell_max_first=self.ell_max_first, ell_max_second=self.ell_max_second,
+            modes=tuple(self.modes[:self.mode_count]),
+            parents=tuple(self.parents[:self.parent_count]),
+            targets=tuple(self.targets[:self.target_count]),
+            reduction_damping=self.reduction_damping,
+            dissipation=self.dissipation, reduction=self.reduction,
+            discretization=self.discretization, source_mode=self.source_mode,
+            source_start_time=self.source_start_time,
+            normalized_constraint_tolerance=self.normalized_constraint_tolerance,
+            required_consecutive_passes=self.required_consecutive_passes)
+
+    def pulse(self) -> "GaussianPulse":
+        modes = [(s.ell, s.m, complex(s.amplitude_real, s.amplitude_imag))
+                 for s in self.seeds[:self.seed_count]]
+        return GaussianPulse(center=self.center, width=self.width, modes=modes,
+                             compact_support=bool(self.compact_support))
+
+
+def _override_array(overrides):
+    items = [o.encode() for o in overrides]
+    return (ctypes.c_char_p * max(len(items), 1))(*items), len(items)
+
+
 class WaveformRecord(ctypes.Structure):
     _fields_ = [
         ("boundary", ctypes.c_int),
@@ -290,6 +364,13 @@ def _load() -> ctypes.CDLL:
         "teuk_b200_batch_set_stream": ([P, P], I),
         "teuk_b200_batch_synchronize": ([P], I),
         "teuk_b200_batch_launches_per_step": ([P, ctypes.POINTER(I)], I),
+        "teuk_b200_parse_run_config": ([ctypes.c_char_p,
+                                        ctypes.POINTER(ctypes.c_char_p), I,
+                                        ctypes.POINTER(RunConfig)], I),
+        "teuk_b200_resolved_config": ([ctypes.c_char_p,
+                                       ctypes.POINTER(ctypes.c_char_p), I,
+                                       ctypes.c_char_p, SZ,
+                                       ctypes.POINTER(SZ)], I),
         "teuk_b200_server_create": ([ctypes.POINTER(_ServerOptions),
                                      ctypes.POINTER(P)], I),
         "teuk_b200_server_destroy": ([P], I),
@@ -362,6 +443,28 @@ def _records(buffer, count):
             "endpoint": complex(r.endpoint_real, r.endpoint_imag),
         })
     return out
+
+
+def parse_run_config(text: str, overrides=()) -> RunConfig:
+    """Parse and validate a teuk_solver .cfg text (+ key=value overrides)."""
+    arr, n = _override_array(overrides)
+    out = RunConfig()
+    _check(_lib.teuk_b200_parse_run_config(text.encode(), arr, n,
+                                           ctypes.byref(out)))
+    return out
+
+
+def resolved_config(text: str, overrides=()) -> str:
+    """resolved_config.cfg body of a .cfg text."""
+    arr, n = _override_array(overrides)
+    length = ctypes.c_size_t()
+    _check(_lib.teuk_b200_resolved_config(text.encode(), arr, n, None, 0,
+                                          ctypes.byref(length)))
+    buf = ctypes.create_string_buffer(length.value + 1)
+    _check(_lib.teuk_b200_resolved_config(text.encode(), arr, n, buf,
+                                          length.value + 1,
+                                          ctypes.byref(length)))
+    return buf.value.decode()
 
 
 def footprint_bytes(config: SolveConfig) -> int:
