@@ -59,6 +59,7 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-serving", action="store_true")
+    p.add_argument("--no-second-order", action="store_true")
     p.add_argument("--serve-requests", type=int, default=48,
                    help="requests of the continuous-batching measurement")
     p.add_argument("--serve-steps", type=int, default=200,
@@ -248,6 +249,50 @@ def serving_run(tb, wl, capacity: float, requests: int, steps: int,
     }
 
 
+# ---------------------------------------------------------------- second order
+def second_order_run(tb, wl, steps: int, cpu_steps: int):
+    """The quadratic-source configuration (full 13-field stage graph with
+    the source active) on the GPU, beside the reference build on the host
+    cores for a few steps of the same solve."""
+    import torch
+
+    config, pulse, dt = wl.second_order_self_coupling()
+    p = tb.Pipeline(config)
+    stream = torch.cuda.Stream()
+    p.set_stream(stream.cuda_stream)
+    p.initialize_gaussian(pulse)
+    p.step(0.0, dt, 2)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    p.step(2 * dt, dt, steps)
+    b.record(stream)
+    b.synchronize()
+    gp = wl.grid_points(config)
+    gpu_rate = steps * gp / (a.elapsed_time(b) / 1e3)
+    p.close()
+    sys.path.insert(0, str(REPO / "tests"))
+    import oracle_bindings as ob
+
+    ref_rate, cores = None, os.cpu_count()
+    if ob.ref_available(threads=True):
+        ref = ob.RefPipeline(config, threads=True)
+        ref.initialize_gaussian(pulse)
+        t0 = time.perf_counter()
+        ref.step(0.0, dt, cpu_steps)
+        ref_rate = cpu_steps * gp / (time.perf_counter() - t0)
+        ref.close()
+    return {
+        "workload": "a=0.9 nr=1025 d10-5 parents m=+-2 ell<=10, targets "
+                    "m={-4,0,4} ell<=20, ntheta=48, source unrestricted "
+                    "(active), Gaussian parents amp 1e-2",
+        "value": gpu_rate, "unit": UNIT, "steps": steps,
+        "reference_cpu": ref_rate, "reference_cores": cores,
+        "reference_steps": cpu_steps,
+        "dtype": "f64", "storage": "nodal (m, 13 fields, r, theta)",
+    }
+
+
 # ---------------------------------------------------------------- CPU side
 def cpu_reference_run(config, pulse, dt, seconds: float, warmup: int = 1,
                       steps: int | None = None):
@@ -421,6 +466,10 @@ def b200_arm(args):
                "d2h_bytes_per_step": 16 * n_end,
                "ms_per_step": e_ms / args.steps}
 
+    second_order = None
+    if rank == 0 and world == 1 and not args.no_second_order:
+        second_order = second_order_run(tb, wl, 20, 2)
+
     serving = None
     if rank == 0 and world == 1 and not args.no_serving:
         serving = serving_run(tb, wl, value, args.serve_requests,
@@ -451,6 +500,7 @@ def b200_arm(args):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "serving": serving,
+            "second_order": second_order,
             "gpu_launches": launches,
             "clocks": clocks,
         }

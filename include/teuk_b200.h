@@ -37,6 +37,9 @@
  *                               write_pipeline_checkpoint /
  *                               load_pipeline_checkpoint_verified
  *                               (include/teuk/pipeline_checkpoint.hpp:782-936)
+ *   teuk_b200_diagnostics_sample
+ *                               PipelineDiagnostics::sample_pipeline
+ *                               (include/teuk/pipeline_diagnostics.hpp:143-345)
  *   teuk_b200_parse_run_config / teuk_b200_resolved_config
  *                               parse_run_configuration_text /
  *                               resolved_configuration_text
@@ -260,6 +263,43 @@ int teuk_b200_checkpoint_write(teuk_b200_pipeline* pipeline,
 int teuk_b200_checkpoint_load(teuk_b200_pipeline* pipeline,
                               const char* directory, double time_step,
                               double* time, uint64_t* step);
+/* PipelineDiagnostics::sample_pipeline (include/teuk/pipeline_diagnostics.hpp
+ * :143-345): RMS and maximum of every stored field and of its last stored
+ * right-hand side, of the two reduction constraints Q - D psi, of the
+ * source and the forcing, plus the latch and source-constraint summary.
+ * All reductions run on the device; a nonfinite value fails the call with
+ * the reference's message. */
+typedef struct teuk_b200_norm {
+  double rms;
+  double maximum;
+} teuk_b200_norm;
+
+typedef struct teuk_b200_diagnostics {
+  teuk_b200_norm state[TEUK_B200_FIELD_COUNT];
+  teuk_b200_norm rhs[TEUK_B200_FIELD_COUNT];
+  teuk_b200_norm first_reduction_constraint;
+  teuk_b200_norm second_reduction_constraint;
+  teuk_b200_norm source_over_r3;
+  teuk_b200_norm forcing;
+  double independent_reconstruction_constraint_maximum;
+  /* SourceConstraintNorms of the last latch check: psi3 Bianchi, psi2
+   * Bianchi, h_ll reality */
+  double constraint_absolute_maximum[3];
+  double constraint_normalized_maximum[3];
+  double constraint_weighted_rms[3];
+  double constraint_normalized_weighted[3];
+  double constraint_controlling_normalized;
+  int constraints_finite;
+  teuk_b200_activation activation;
+  int second_order_source_active;
+  size_t point_count;
+  int scri_finite;
+  int horizon_finite;
+  int all_finite;
+} teuk_b200_diagnostics;
+
+int teuk_b200_diagnostics_sample(teuk_b200_pipeline* pipeline,
+                                 teuk_b200_diagnostics* out);
 /* Device bytes held by one pipeline built from `config` (admission). */
 int teuk_b200_footprint_bytes(const teuk_b200_config* config,
                               size_t* bytes);

@@ -21,6 +21,7 @@
 #include "teuk/diagnostics.hpp"
 #include "teuk/initial_data_factory.hpp"
 #include "teuk/pipeline_bands.hpp"
+#include "teuk/pipeline_diagnostics.hpp"
 #include "teuk/pipeline_checkpoint.hpp"
 #include "teuk/pipeline_initial_data.hpp"
 #include "teuk/spatial_pipeline.hpp"
@@ -463,6 +464,56 @@ int teuk_ref_parse_run_config(const char* text, const char* const* overrides,
                   run.output.directory.c_str());
     r.diagnostic_every = run.output.diagnostic_interval;
     r.checkpoint_every = run.output.checkpoint_interval;
+    *out = r;
+  });
+}
+
+// PipelineDiagnostics::sample_pipeline (include/teuk/pipeline_diagnostics.hpp)
+int teuk_ref_diagnostics(teuk_ref_pipeline* p, teuk_b200_diagnostics* out) {
+  return guarded([&] {
+    const auto& c = p->config;
+    teuk::PipelineDiagnostics diagnostics(
+        p->registry.size(),
+        teuk::UniformRadialGrid(static_cast<std::size_t>(c.radial_points), 0.0,
+                                p->horizon),
+        static_cast<std::size_t>(c.theta_nodes), "ref_diagnostics",
+        discretization(c.discretization));
+    const auto report = diagnostics.sample_pipeline(p->execution, p->pipeline);
+    teuk_b200_diagnostics r{};
+    for (std::size_t f = 0; f < teuk::point_pipeline_field_count; ++f) {
+      r.state[f] = {report.fields[f].state.rms, report.fields[f].state.maximum};
+      r.rhs[f] = {report.fields[f].rhs.rms, report.fields[f].rhs.maximum};
+    }
+    r.first_reduction_constraint = {report.first_reduction_constraint.rms,
+                                    report.first_reduction_constraint.maximum};
+    r.second_reduction_constraint = {report.second_reduction_constraint.rms,
+                                     report.second_reduction_constraint.maximum};
+    r.source_over_r3 = {report.source_over_r3.rms, report.source_over_r3.maximum};
+    r.forcing = {report.forcing.rms, report.forcing.maximum};
+    r.independent_reconstruction_constraint_maximum =
+        report.independent_reconstruction_constraint_maximum;
+    const teuk::SourceConstraintFamilyNorms* fam[3] = {
+        &report.normalized_source_constraints.psi3_bianchi,
+        &report.normalized_source_constraints.psi2_bianchi,
+        &report.normalized_source_constraints.hll_reality};
+    for (int k = 0; k < 3; ++k) {
+      r.constraint_absolute_maximum[k] = fam[k]->absolute_maximum;
+      r.constraint_normalized_maximum[k] = fam[k]->normalized_maximum;
+      r.constraint_weighted_rms[k] = fam[k]->weighted_rms;
+      r.constraint_normalized_weighted[k] = fam[k]->normalized_weighted;
+    }
+    r.constraint_controlling_normalized =
+        report.normalized_source_constraints.controlling_normalized;
+    r.constraints_finite = report.normalized_source_constraints.all_finite;
+    r.activation = {report.source_activation.active ? 1 : 0,
+                    report.source_activation.activation_time,
+                    report.source_activation.consecutive_passes,
+                    report.source_activation.last_eligibility_time};
+    r.second_order_source_active = report.second_order_source_active ? 1 : 0;
+    r.point_count = report.point_count;
+    r.scri_finite = report.scri_finite;
+    r.horizon_finite = report.horizon_finite;
+    r.all_finite = report.all_finite;
     *out = r;
   });
 }

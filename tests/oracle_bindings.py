@@ -161,6 +161,17 @@ class RefPipeline:
             ctypes.byref(n)))
         return t.value, n.value
 
+    def diagnostics(self) -> tb.Diagnostics:
+        lib = self.lib
+        if not hasattr(lib, "_diag_ready"):
+            lib.teuk_ref_diagnostics.argtypes = [ctypes.c_void_p,
+                                                 ctypes.POINTER(tb.Diagnostics)]
+            lib.teuk_ref_diagnostics.restype = ctypes.c_int
+            lib._diag_ready = True
+        d = tb.Diagnostics()
+        self._check(lib.teuk_ref_diagnostics(self._handle, ctypes.byref(d)))
+        return d
+
     def activation(self) -> tb.Activation:
         a = tb.Activation()
         self._check(self.lib.teuk_ref_get_activation(self._handle,

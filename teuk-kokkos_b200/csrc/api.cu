@@ -1745,6 +1745,124 @@ int teuk_b200_resolved_config(const char* text, const char* const* overrides,
   });
 }
 
+int teuk_b200_diagnostics_sample(teuk_b200_pipeline* p,
+                                 teuk_b200_diagnostics* out) {
+  return guarded([&] {
+    require(p != nullptr && out != nullptr, "null argument");
+    using teuk_b200::DeviceArray;
+    const teuk_b200::InstancePlan& plan =
+        p->nodal ? p->nodal->plan() : p->batch->plans[0];
+    const teuk_b200::Config& c = plan.config;
+    cudaStream_t stream = p->nodal ? p->nodal->stream() : p->batch->stream;
+    teuk_b200::DiagnosticsLaunch d{};
+    if (p->nodal) {
+      d.state = p->nodal->state_device();
+      d.rhs = p->nodal->storage_rhs_device();
+      d.source = p->nodal->source_device();
+      d.forcing = p->nodal->forcing_device();
+    } else {
+      // nodal view of the band state; the linear pipeline never writes its
+      // storage RHS, source or forcing, which therefore read as zero
+      p->batch->assemble_nodal(0, p->batch->y.ptr, false);
+      d.state = p->batch->nodal_scratch();
+    }
+    teuk_b200::check(teuk_b200::upload_nodal_sbp_constants(),
+                     "upload SBP constants");
+    DeviceArray<double> sums;
+    DeviceArray<unsigned long long> maxima;
+    DeviceArray<int> finite;
+    sums.allocate(30);
+    maxima.allocate(30);
+    finite.allocate(8);
+    const int ones[8] = {1, 1, 1, 1, 1, 1, 1, 1};
+    teuk_b200::check(cudaMemsetAsync(sums.ptr, 0, 30 * sizeof(double), stream),
+                     "zero sums");
+    teuk_b200::check(
+        cudaMemsetAsync(maxima.ptr, 0, 30 * sizeof(unsigned long long), stream),
+        "zero maxima");
+    teuk_b200::check(cudaMemcpyAsync(finite.ptr, ones, sizeof(ones),
+                                     cudaMemcpyHostToDevice, stream),
+                     "finite flags");
+    d.modes = static_cast<int>(c.modes.size());
+    d.nr = c.nr;
+    d.nt = c.ntheta;
+    d.disc = c.disc;
+    d.inv_spacing = 1.0 / plan.spacing;
+    d.sums = sums.ptr;
+    d.maxima = maxima.ptr;
+    d.finite = finite.ptr;
+    teuk_b200::check(teuk_b200::launch_diagnostics(d, stream), "diagnostics");
+    double h_sums[30];
+    unsigned long long h_max[30];
+    int h_finite[8];
+    teuk_b200::check(cudaMemcpyAsync(h_sums, sums.ptr, sizeof(h_sums),
+                                     cudaMemcpyDeviceToHost, stream),
+                     "read sums");
+    teuk_b200::check(cudaMemcpyAsync(h_max, maxima.ptr, sizeof(h_max),
+                                     cudaMemcpyDeviceToHost, stream),
+                     "read maxima");
+    teuk_b200::check(cudaMemcpyAsync(h_finite, finite.ptr, sizeof(h_finite),
+                                     cudaMemcpyDeviceToHost, stream),
+                     "read flags");
+    teuk_b200::check(cudaStreamSynchronize(stream), "diagnostics");
+    teuk_b200_diagnostics r{};
+    const size_t points = c.modes.size() * static_cast<size_t>(c.nr) *
+                          static_cast<size_t>(c.ntheta);
+    const double inv = 1.0 / static_cast<double>(points);
+    const auto norm = [&](const int slot) {
+      double m = 0.0;
+      std::memcpy(&m, &h_max[slot], sizeof(m));
+      return teuk_b200_norm{std::sqrt(h_sums[slot] * inv), std::sqrt(m)};
+    };
+    for (int f = 0; f < teuk_b200::kFieldCount; ++f) {
+      r.state[f] = norm(f);
+      r.rhs[f] = norm(teuk_b200::kFieldCount + f);
+    }
+    r.first_reduction_constraint = norm(26);
+    r.second_reduction_constraint = norm(27);
+    r.source_over_r3 = norm(28);
+    r.forcing = norm(29);
+    r.point_count = points;
+    r.scri_finite = h_finite[6];
+    r.horizon_finite = h_finite[7];
+    r.all_finite = 1;
+    for (const int f : h_finite) r.all_finite &= f != 0 ? 1 : 0;
+    if (r.all_finite == 0) {
+      // PipelineDiagnostics::nonfinite_message
+      std::string message = "pipeline diagnostics found nonfinite values in";
+      const char* names[8] = {" state", " rhs", " first-constraint",
+                              " second-constraint", " source", " forcing",
+                              " scri-endpoint", " horizon-endpoint"};
+      for (int f = 0; f < 8; ++f) {
+        if (h_finite[f] == 0) message += names[f];
+      }
+      throw std::runtime_error(message);
+    }
+    if (p->nodal) {
+      const teuk_b200::ConstraintNorms& n = p->nodal->constraint_norms();
+      for (int k = 0; k < 3; ++k) {
+        r.constraint_absolute_maximum[k] = n.absolute_maximum[k];
+        r.constraint_normalized_maximum[k] = n.normalized_maximum[k];
+        r.constraint_weighted_rms[k] = n.weighted_rms[k];
+        r.constraint_normalized_weighted[k] = n.normalized_weighted[k];
+      }
+      r.constraint_controlling_normalized = n.controlling_normalized;
+      r.constraints_finite = n.all_finite ? 1 : 0;
+      r.independent_reconstruction_constraint_maximum =
+          p->nodal->independent_constraint_maximum();
+      const auto a = p->nodal->activation();
+      r.activation = {a.active ? 1 : 0, a.activation_time, a.consecutive_passes,
+                      a.last_eligibility_time};
+    } else {
+      r.constraints_finite = 1;
+      r.activation = {plan.active, plan.activation_time, plan.consecutive_passes,
+                      plan.last_eligibility_time};
+    }
+    r.second_order_source_active = r.activation.active;
+    *out = r;
+  });
+}
+
 int teuk_b200_footprint_bytes(const teuk_b200_config* config, size_t* bytes) {
   return guarded([&] {
     require(config != nullptr && bytes != nullptr, "null argument");

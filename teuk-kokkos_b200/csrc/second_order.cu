@@ -911,6 +911,111 @@ __global__ void norms_normalized_kernel(const Geo g, const Arr residuals,
   }
 }
 
+__device__ __forceinline__ double dwarp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double dwarp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ bool finite2(const C2 v) {
+  return isfinite(v.re) && isfinite(v.im);
+}
+
+// One warp-reduced sum / max per slot and iteration; the first lane adds
+// them to the device accumulators.
+__device__ void reduce_slot(const DiagnosticsLaunch& p, const int slot,
+                            const double value, const int lane) {
+  const double s = dwarp_sum(value);
+  const double m = dwarp_max(value);
+  if (lane == 0) {
+    atomicAdd(&p.sums[slot], s);
+    atomicMax(&p.maxima[slot],
+              static_cast<unsigned long long>(__double_as_longlong(m)));
+  }
+}
+
+__global__ void diagnostics_kernel(const DiagnosticsLaunch p) {
+  // flags: 0 state, 1 rhs, 2 first constraint, 3 second constraint,
+  // 4 source, 5 forcing, 6 scri, 7 horizon
+  const int lane = threadIdx.x & 31;
+  const long long total = static_cast<long long>(p.modes) * p.nr * p.nt;
+  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+  const long long rounds = (total + stride - 1) / stride;
+  for (long long k = 0; k < rounds; ++k) {
+    const long long i = k * stride + blockIdx.x * static_cast<long long>(blockDim.x) +
+                        threadIdx.x;
+    const bool in = i < total;
+    int t = 0, r = 0, mode = 0;
+    if (in) {
+      t = static_cast<int>(i % p.nt);
+      r = static_cast<int>((i / p.nt) % p.nr);
+      mode = static_cast<int>(i / (static_cast<long long>(p.nt) * p.nr));
+    }
+    const bool scri = in && r == 0, horizon = in && r + 1 == p.nr;
+    const auto bad = [&](const int flag) {
+      atomicExch(&p.finite[flag], 0);
+      if (scri) atomicExch(&p.finite[6], 0);
+      if (horizon) atomicExch(&p.finite[7], 0);
+    };
+    const auto at = [&](const double2* a, const int f) {
+      return a + ((static_cast<long long>(mode) * kFieldCount + f) * p.nr + r) * p.nt + t;
+    };
+    for (int f = 0; f < kFieldCount; ++f) {
+      double sv = 0.0, rv = 0.0;
+      if (in) {
+        const C2 v = ld(*at(p.state, f));
+        if (finite2(v)) {
+          sv = v.re * v.re + v.im * v.im;
+        } else {
+          bad(0);
+        }
+        if (p.rhs != nullptr) {
+          const C2 w = ld(*at(p.rhs, f));
+          if (finite2(w)) {
+            rv = w.re * w.re + w.im * w.im;
+          } else {
+            bad(1);
+          }
+        }
+      }
+      reduce_slot(p, f, sv, lane);
+      reduce_slot(p, kFieldCount + f, rv, lane);
+    }
+    for (int c = 0; c < 2; ++c) {
+      double v2 = 0.0;
+      if (in) {
+        const int q = c == 0 ? kFirstQ : kSecondQ;
+        const int psi = c == 0 ? kFirstPsi : kSecondPsi;
+        const C2 d = deriv(p.disc, at(p.state, psi) - static_cast<long long>(r) * p.nt,
+                           p.nt, p.nr, r, p.inv_spacing);
+        const C2 v = ld(*at(p.state, q)) - d;
+        if (finite2(v)) {
+          v2 = v.re * v.re + v.im * v.im;
+        } else {
+          atomicExch(&p.finite[2 + c], 0);
+        }
+      }
+      reduce_slot(p, 2 * kFieldCount + c, v2, lane);
+    }
+    for (int c = 0; c < 2; ++c) {
+      const double2* a = c == 0 ? p.source : p.forcing;
+      double v2 = 0.0;
+      if (in && a != nullptr) {
+        const C2 v = ld(a[i]);
+        if (finite2(v)) {
+          v2 = v.re * v.re + v.im * v.im;
+        } else {
+          bad(4 + c);
+        }
+      }
+      reduce_slot(p, 2 * kFieldCount + 2 + c, v2, lane);
+    }
+  }
+}
+
 int grid_for(const long long n) {
   const long long b = (n + kBlock - 1) / kBlock;
   return static_cast<int>(b < 8192 ? (b > 0 ? b : 1) : 8192);
@@ -1483,6 +1588,9 @@ void NodalPipeline::consider_activation(const double accepted_time) {
   }
   evaluate(buf_->state, buf_->rhs_out);
   norms_ = sample_constraints();
+  independent_max_ = std::max({norms_.absolute_maximum[0],
+                               norms_.absolute_maximum[1],
+                               norms_.absolute_maximum[2]});
   const bool passed = norms_.all_finite &&
                       norms_.controlling_normalized <= c.constraint_tolerance;
   activation_.last_eligibility_time = accepted_time;
@@ -1571,6 +1679,7 @@ void NodalPipeline::reset_activation() {
   const Config& c = plan_.config;
   activation_ = {};
   norms_ = {};
+  independent_max_ = 0.0;
   if (c.source_mode == TEUK_B200_SOURCE_UNRESTRICTED &&
       c.source_start_time == 0.0) {
     activation_.active = true;
@@ -1609,8 +1718,10 @@ void NodalPipeline::evaluate_rhs(const double* stage, double* out,
   const cudaMemcpyKind in_kind =
       memory == TEUK_B200_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   check(cudaMemcpyAsync(buf_->rhs_in, stage, bytes, in_kind, stream_), "rhs in");
-  evaluate(buf_->rhs_in, buf_->rhs_out);
-  check(cudaMemcpyAsync(out, buf_->rhs_out, bytes,
+  // the storage RHS (rhs_out) is left to the latch check, as the reference
+  // leaves storage().rhs() alone when a caller evaluates its own views
+  evaluate(buf_->rhs_in, buf_->k[3]);
+  check(cudaMemcpyAsync(out, buf_->k[3], bytes,
                         memory == TEUK_B200_HOST ? cudaMemcpyDeviceToHost
                                                  : cudaMemcpyDeviceToDevice,
                         stream_),
@@ -1652,6 +1763,17 @@ std::size_t nodal_footprint_bytes(const InstancePlan& plan) {
       4 * std::max<std::size_t>(pairs, 1) * plane;
   return complex_count * sizeof(double2);
 }
+
+cudaError_t launch_diagnostics(const DiagnosticsLaunch& p, cudaStream_t stream) {
+  const long long total = static_cast<long long>(p.modes) * p.nr * p.nt;
+  diagnostics_kernel<<<grid_for(total), kBlock, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+const double2* NodalPipeline::state_device() const { return buf_->state; }
+const double2* NodalPipeline::storage_rhs_device() const { return buf_->rhs_out; }
+const double2* NodalPipeline::source_device() const { return buf_->source; }
+const double2* NodalPipeline::forcing_device() const { return buf_->forcing; }
 
 cudaError_t upload_nodal_sbp_constants() {
   const SbpConstants constants = build_sbp_constants();

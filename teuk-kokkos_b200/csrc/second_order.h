@@ -62,6 +62,23 @@ struct DeviceError : std::runtime_error {
 // Device bytes a NodalPipeline allocates for `plan`.
 std::size_t nodal_footprint_bytes(const InstancePlan& plan);
 
+// Reductions of PipelineDiagnostics::sample
+// (include/teuk/pipeline_diagnostics.hpp:143-291) over nodal
+// (mode, 13, r, theta) arrays; a null rhs / source / forcing reads as zero.
+struct DiagnosticsLaunch {
+  const double2* state;
+  const double2* rhs;
+  const double2* source;   // (mode, r, theta)
+  const double2* forcing;  // (mode, r, theta)
+  int modes, nr, nt, disc;
+  double inv_spacing;
+  double* sums;                // 30: 13 state, 13 rhs, 4 scalars
+  unsigned long long* maxima;  // 30, as bits of nonnegative doubles
+  int* finite;                 // 8 flags, 1 = finite
+};
+cudaError_t launch_diagnostics(const DiagnosticsLaunch& launch,
+                               cudaStream_t stream);
+
 class NodalPipeline {
  public:
   struct Buffers;
@@ -87,6 +104,13 @@ class NodalPipeline {
   // Endpoint psi of the first-order (field 2) or second-order (field 12)
   // state: (mode, theta) nodal values at radial index `radial`.
   void endpoint_slice(int field, int radial, std::vector<double2>& out);
+  // Storage views of the reference pipeline: state, storage rhs (written by
+  // the latch check), source_over_r3, forcing.
+  const double2* state_device() const;
+  const double2* storage_rhs_device() const;
+  const double2* source_device() const;
+  const double2* forcing_device() const;
+  double independent_constraint_maximum() const { return independent_max_; }
 
  private:
   void build_coordinators();
@@ -112,6 +136,7 @@ class NodalPipeline {
   std::vector<int> coordinator_diag_[10][3];
   std::vector<double> matrices_;
   SourceActivation activation_;
+  double independent_max_ = 0.0;  // sqrt(source_constraint_max_squared)
   ConstraintNorms norms_;
   StepGraph graphs_[2];  // latch off / on
   cudaStream_t own_stream_ = nullptr;

@@ -213,6 +213,45 @@ def _override_array(overrides):
     return (ctypes.c_char_p * max(len(items), 1))(*items), len(items)
 
 
+class Norm(ctypes.Structure):
+    _fields_ = [("rms", ctypes.c_double), ("maximum", ctypes.c_double)]
+
+
+class Diagnostics(ctypes.Structure):
+    """teuk_b200_diagnostics (PipelineDiagnosticsReport)."""
+    _fields_ = [
+        ("state", Norm * FIELD_COUNT),
+        ("rhs", Norm * FIELD_COUNT),
+        ("first_reduction_constraint", Norm),
+        ("second_reduction_constraint", Norm),
+        ("source_over_r3", Norm),
+        ("forcing", Norm),
+        ("independent_reconstruction_constraint_maximum", ctypes.c_double),
+        ("constraint_absolute_maximum", ctypes.c_double * 3),
+        ("constraint_normalized_maximum", ctypes.c_double * 3),
+        ("constraint_weighted_rms", ctypes.c_double * 3),
+        ("constraint_normalized_weighted", ctypes.c_double * 3),
+        ("constraint_controlling_normalized", ctypes.c_double),
+        ("constraints_finite", ctypes.c_int),
+        ("activation", Activation),
+        ("second_order_source_active", ctypes.c_int),
+        ("point_count", ctypes.c_size_t),
+        ("scri_finite", ctypes.c_int),
+        ("horizon_finite", ctypes.c_int),
+        ("all_finite", ctypes.c_int),
+    ]
+
+    def norms(self):
+        """Flat list of every (rms, maximum) pair in report order."""
+        out = [(n.rms, n.maximum) for n in self.state]
+        out += [(n.rms, n.maximum) for n in self.rhs]
+        for name in ("first_reduction_constraint", "second_reduction_constraint",
+                     "source_over_r3", "forcing"):
+            n = getattr(self, name)
+            out.append((n.rms, n.maximum))
+        return out
+
+
 class WaveformRecord(ctypes.Structure):
     _fields_ = [
         ("boundary", ctypes.c_int),
@@ -341,6 +380,7 @@ def _load() -> ctypes.CDLL:
         "teuk_b200_reset_activation": ([P], I),
         "teuk_b200_set_stream": ([P, P], I),
         "teuk_b200_synchronize": ([P], I),
+        "teuk_b200_diagnostics_sample": ([P, ctypes.POINTER(Diagnostics)], I),
         "teuk_b200_checkpoint_write": ([P, ctypes.c_char_p, D, D,
                                         ctypes.c_uint64], I),
         "teuk_b200_checkpoint_load": ([P, ctypes.c_char_p, D, DP,
@@ -555,6 +595,12 @@ class Pipeline:
         a = Activation()
         _check(_lib.teuk_b200_get_activation(self._handle, ctypes.byref(a)))
         return a
+
+    def diagnostics(self) -> Diagnostics:
+        """Device-side PipelineDiagnostics sample of the current state."""
+        d = Diagnostics()
+        _check(_lib.teuk_b200_diagnostics_sample(self._handle, ctypes.byref(d)))
+        return d
 
     def checkpoint_write(self, directory, time_step: float, time: float,
                          step: int):

@@ -102,6 +102,33 @@ def schwarzschild_quadrupole(seed: int = 20260101):
                                  modes=[(2, 2, amp)]), dt
 
 
+def second_order_self_coupling(seed: int = 20260101, radial_points: int = 1025,
+                               cfl: float = 0.25, source_start_time: float = 0.0):
+    """Quadratic-source run: a = 0.9, M = 1, D10-5, parents m = +-2 with
+    ell <= 10, targets m in {-4, 0, 4} with ell <= 20, ntheta 48, source
+    Unrestricted from `source_start_time`; seeded Gaussian parents in
+    ell = 2 (centre 10M, width 1M, amplitude 1e-2).  Returns
+    (config, pulse, dt)."""
+    from . import SOURCE_UNRESTRICTED
+
+    base = SolveConfig(mass=1.0, spin=0.9, compactification_length=1.0,
+                       radial_points=radial_points, theta_nodes=48,
+                       ell_max_first=10, ell_max_second=20,
+                       modes=(-4, -2, 0, 2, 4), parents=(-2, 2),
+                       targets=(-4, 0, 4), reduction_damping=0.1,
+                       dissipation=0.0, discretization=D105,
+                       source_mode=SOURCE_UNRESTRICTED,
+                       source_start_time=source_start_time)
+    dt = cfl_time_step(base, cfl)
+    sigma = min(0.005, 0.9 * dissipation_bound(D105, dt / base.spacing))
+    config = replace(base, dissipation=sigma)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    center, width = compactified(config, 10.0, 1.0)
+    modes = [(2, m, 1e-2 * complex(rng.standard_normal(), rng.standard_normal()))
+             for m in (-2, 2)]
+    return config, GaussianPulse(center=center, width=width, modes=modes), dt
+
+
 def uneven_instance(rng: np.random.Generator, cfl: float = 0.25):
     """One solve of the batched uneven-instance mix: spin U[0, 0.95],
     nr from {257, 513, 1025, 2049}, D10-5, ell_max U{8..20}, m = -2..2
