@@ -338,6 +338,12 @@ int teuk_b200_batch_synchronize(teuk_b200_batch* batch);
 /* Kernel launches issued per RK4 step (for launch accounting). */
 int teuk_b200_batch_launches_per_step(const teuk_b200_batch* batch,
                                       int* launches);
+/* Launch groups (one per discretization and reduction) whose stages run the
+ * streaming kernel (persistent CTAs over radial strips; n_ell <= 16 and at
+ * most 32 Gauss-Legendre nodes) and those that run the tile kernel.  No
+ * counterpart in the reference: kernel selection of this engine. */
+int teuk_b200_batch_stage_kernels(const teuk_b200_batch* batch,
+                                  int* streaming_groups, int* tile_groups);
 
 /* ---- runtime configuration (.cfg) --------------------------------------
  * The teuk_solver schema (include/teuk/config.hpp): `key = value` lines,

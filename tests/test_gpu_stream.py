@@ -1,0 +1,112 @@
+"""Streaming stage kernel on shapes that split every segment into several
+radial strips, against the reference build and against the tile kernel.
+
+The engine runs launch groups with n_ell <= 16 and at most 32 Gauss-Legendre
+nodes through the streaming kernel (persistent CTAs, bulk-copy ring);
+TEUK_B200_STAGE_KERNEL=tile makes a pipeline built while it is set use the
+tile kernel instead.  Segments of one launch differ in n_ell (m = -4..4), so
+the ring also changes its row stride between strips.
+Tolerance: 1e-10 relative to the field's max norm against the reference;
+the two engine kernels agree to 1e-12 (they differ in summation order only).
+"""
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+import teuk_b200 as tb
+from cases import CASES, pulse_for, relative_error, step_size
+from oracle_bindings import RefPipeline
+from test_gpu_parity import _generic_band_state
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+LONG = {
+    # D10-5 free-damped Kerr, 300 radial points: strips of 64-75 rows
+    "kerr_d105_long": replace(CASES["kerr_d105"], radial_points=300),
+    # D8-4 stage-constrained Kerr with odd m (n_ell 3..5)
+    "kerr_d84_sc_long": replace(CASES["kerr_d42_sc"], discretization=tb.D84,
+                                radial_points=260, dissipation=0.005),
+    # Schwarzschild D4-2 (pointwise psi_t)
+    "schw_d42_long": replace(CASES["schw_d84"], discretization=tb.D42,
+                             radial_points=203, dissipation=0.01),
+}
+
+
+def _pair(name, seed=11):
+    config = LONG[name]
+    gpu = tb.Pipeline(config)
+    ref = RefPipeline(config)
+    pulse = pulse_for(config, seed)
+    gpu.initialize_gaussian(pulse)
+    ref.initialize_gaussian(pulse)
+    return config, gpu, ref
+
+
+@pytest.mark.parametrize("name", sorted(LONG))
+def test_long_rhs_matches_reference(require_gpu, name):
+    config, gpu, ref = _pair(name)
+    state = _generic_band_state(ref, 23)
+    g = gpu.evaluate_rhs(state)
+    r = ref.evaluate_rhs(state)
+    for f in range(3):
+        assert relative_error(g[:, f], r[:, f]) < TOL, f"field {f}"
+    assert np.all(g[:, 3:] == 0)
+
+
+@pytest.mark.parametrize("name", sorted(LONG))
+def test_long_rk4_matches_reference(require_gpu, name):
+    config, gpu, ref = _pair(name)
+    dt = step_size(config, 0.1)
+    gpu.step(0.0, dt, 6)
+    ref.step(0.0, dt, 6)
+    g, r = gpu.get_state(), ref.get_state()
+    for f in range(3):
+        assert relative_error(g[:, f], r[:, f]) < TOL, f"field {f}"
+    assert np.array_equal(g[:, 3:], r[:, 3:])
+
+
+@pytest.mark.parametrize("name", sorted(LONG) + ["kerr_d105", "kerr_d42_sc"])
+def test_stream_kernel_equals_tile_kernel(require_gpu, monkeypatch, name):
+    config = LONG.get(name, CASES.get(name))
+    pulse = pulse_for(config, 5)
+    stream = tb.Batch([config])
+    monkeypatch.setenv("TEUK_B200_STAGE_KERNEL", "tile")
+    tile = tb.Batch([config])
+    monkeypatch.delenv("TEUK_B200_STAGE_KERNEL")
+    assert stream.stage_kernels() == (1, 0)
+    assert tile.stage_kernels() == (0, 1)
+    for p in (stream, tile):
+        p.initialize_gaussian(0, pulse)
+    dt = step_size(config, 0.1)
+    stream.step([dt], 12)
+    tile.step([dt], 12)
+    a, b = stream.get_state(0), tile.get_state(0)
+    for f in range(3):
+        assert relative_error(a[:, f], b[:, f]) < 1e-12, f"field {f}"
+
+
+def test_mixed_batch_matches_solo(require_gpu):
+    """Solves of different radial sizes, spins and n_ell share launches; each
+    result equals the same solve run alone (the streaming kernel's rows do
+    not depend on how segments are split into strips)."""
+    base = LONG["kerr_d105_long"]
+    configs = [base,
+               replace(base, radial_points=129, spin=0.3),
+               replace(base, radial_points=777, spin=0.9, ell_max_first=12,
+                       ell_max_second=12),
+               replace(base, radial_points=64, spin=0.0)]
+    pulses = [pulse_for(c, 31 + i) for i, c in enumerate(configs)]
+    dts = [step_size(c, 0.1) for c in configs]
+    batch = tb.Batch(configs)
+    assert batch.stage_kernels() == (1, 0)
+    for i, p in enumerate(pulses):
+        batch.initialize_gaussian(i, p)
+    batch.step(dts, 5)
+    for i, c in enumerate(configs):
+        solo = tb.Pipeline(c)
+        solo.initialize_gaussian(pulses[i])
+        solo.step(0.0, dts[i], 5)
+        assert np.array_equal(batch.get_state(i), solo.get_state()), i

@@ -24,7 +24,7 @@ LIBRARY = LIB_DIR / "libteuk_b200.so"
 SOURCES = ["plan.cpp", "checkpoint.cpp", "run_config.cpp", "kernels.cu",
            "second_order.cu",
            "static_scratch.cu", "api.cu"]
-HEADERS = ["engine.h", "kernels.h", "second_order.h", "static_scratch.h",
+HEADERS = ["engine.h", "kernels.h", "second_order.h", "stream_kernel.cuh", "static_scratch.h",
            "checkpoint.h", "run_config.h", "sbp_tables.h"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -9,6 +9,7 @@
 #include <chrono>
 #include <deque>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <exception>
 #include <limits>
@@ -205,6 +206,8 @@ struct Batch {
   std::vector<double> h_trig;
   std::vector<StageLaunch> groups;  // one per (disc, reduction)
   std::vector<int> group_first_tile;
+  std::vector<TileDesc> h_strips;       // streaming-kernel strips
+  std::vector<int> group_first_strip;   // -1: group runs the tile kernel
   size_t total_complex = 0;
   int max_ell = 1;
 
@@ -213,6 +216,10 @@ struct Batch {
   DeviceArray<SegmentDesc> d_seg;
   DeviceArray<int> d_seg_mode;
   DeviceArray<TileDesc> d_tiles;
+  DeviceArray<TileDesc> d_strips;
+  DeviceArray<int> d_error;  // streaming-kernel wait timeouts
+  DeviceArray<double> d_coef;  // Teukolsky row coefficients per solve row
+  int coef_rows = 0;
   DeviceArray<double> d_mat, d_trig;
   DeviceArray<double2> d_nodal;     // one instance's nodal state (lazy)
   size_t nodal_max = 0;
@@ -294,6 +301,8 @@ struct Batch {
       d.trig_offset = static_cast<int>(h_trig.size());
       d.reduction = c.reduction;
       d.disc = c.disc;
+      d.coef_row0 = coef_rows;
+      coef_rows += c.nr;
       h_trig.insert(h_trig.end(), plan.sinv.begin(), plan.sinv.end());
       h_trig.insert(h_trig.end(), plan.cosv.begin(), plan.cosv.end());
       h_inst.push_back(d);
@@ -374,6 +383,7 @@ struct Batch {
             throw std::invalid_argument(
                 "solve shape exceeds the stage kernel's shared-memory tile");
           }
+          group_first_strip.push_back(plan_strips(g, disc, red));
           groups.push_back(g);
           group_first_tile.push_back(first_tile);
         }
@@ -402,6 +412,10 @@ struct Batch {
     d_seg.allocate(h_seg.size());
     d_seg_mode.allocate(seg_mode.size());
     d_tiles.allocate(h_tiles.size());
+    d_strips.allocate(std::max<size_t>(h_strips.size(), 1));
+    d_error.allocate(1);
+    check(cudaMemset(d_error.ptr, 0, sizeof(int)), "memset error word");
+    d_coef.allocate(static_cast<size_t>(std::max(coef_rows, 1)) * kCoefRecord);
     d_mat.allocate(std::max<size_t>(h_mat.size(), 1));
     d_trig.allocate(h_trig.size());
     nodal_max = 0;
@@ -425,6 +439,11 @@ struct Batch {
           "cudaStreamCreate");
     stream = own_stream;
     upload_descriptors();
+    for (size_t i = 0; i < h_inst.size(); ++i) {
+      check(launch_coefficient_table(d_inst.ptr + i, h_inst[i].nr,
+                                     h_inst[i].coef_row0, d_coef.ptr, stream),
+            "coefficient table");
+    }
     check(cudaMemcpy(d_seg.ptr, h_seg.data(), h_seg.size() * sizeof(SegmentDesc),
                      cudaMemcpyHostToDevice),
           "upload segments");
@@ -434,6 +453,12 @@ struct Batch {
     check(cudaMemcpy(d_tiles.ptr, h_tiles.data(),
                      h_tiles.size() * sizeof(TileDesc), cudaMemcpyHostToDevice),
           "upload tiles");
+    if (!h_strips.empty()) {
+      check(cudaMemcpy(d_strips.ptr, h_strips.data(),
+                       h_strips.size() * sizeof(TileDesc),
+                       cudaMemcpyHostToDevice),
+            "upload strips");
+    }
     if (!h_mat.empty()) {
       check(cudaMemcpy(d_mat.ptr, h_mat.data(), h_mat.size() * sizeof(double),
                        cudaMemcpyHostToDevice),
@@ -445,6 +470,14 @@ struct Batch {
     for (size_t gi = 0; gi < groups.size(); ++gi) {
       StageLaunch& g = groups[gi];
       g.tiles = d_tiles.ptr + group_first_tile[gi];
+      g.error = d_error.ptr;
+      g.coef_table = d_coef.ptr;
+      if (group_first_strip[gi] >= 0) {
+        g.strips = d_strips.ptr + group_first_strip[gi];
+      } else {
+        g.strips = nullptr;
+        g.strip_count = 0;
+      }
       g.instances = d_inst.ptr;
       g.segments = d_seg.ptr;
       g.matrices = d_mat.ptr;
@@ -453,6 +486,62 @@ struct Batch {
       g.kA = kA.ptr;
       g.kB = kB.ptr;
       g.acc = acc.ptr;
+    }
+  }
+
+  // Radial strips of a launch group for the streaming kernel, sorted by
+  // n_ell (largest first) so that a CTA's consecutive strips mostly share
+  // one ring row stride.  Returns the group's first strip index, or -1 when
+  // the group's shape needs the tile kernel.
+  int plan_strips(StageLaunch& g, const int disc, const int red) {
+    g.strips = nullptr;
+    g.strip_count = 0;
+    if (g.max_ell > kStreamMaxEll || g.max_theta > kStreamMaxNodes) return -1;
+    const char* forced = std::getenv("TEUK_B200_STAGE_KERNEL");
+    if (forced != nullptr && std::string(forced) == "tile") return -1;
+    int device = 0, sms = 0;
+    check(cudaGetDevice(&device), "cudaGetDevice");
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device),
+          "SM count");
+    std::vector<int> segs;
+    long long rows = 0;
+    for (size_t s = 0; s < h_seg.size(); ++s) {
+      const InstanceDesc& in = h_inst[static_cast<size_t>(h_seg[s].instance)];
+      if (in.disc != disc || in.reduction != red) continue;
+      segs.push_back(static_cast<int>(s));
+      rows += in.nr;
+    }
+    const long long want = static_cast<long long>(std::max(sms, 1)) * kStripsPerCta;
+    const int target = static_cast<int>(std::min<long long>(
+        1024, std::max<long long>(kStripMinRows, rows / want)));
+    std::stable_sort(segs.begin(), segs.end(), [&](const int a, const int b) {
+      return h_seg[static_cast<size_t>(a)].n_ell > h_seg[static_cast<size_t>(b)].n_ell;
+    });
+    const int first = static_cast<int>(h_strips.size());
+    for (const int s : segs) {
+      const int nr = h_inst[static_cast<size_t>(h_seg[static_cast<size_t>(s)].instance)].nr;
+      int n = std::max(1, nr / target);
+      n = std::max(1, std::min(n, nr / kStripMinRows));
+      for (int t = 0; t < n; ++t) {
+        const int r0 = static_cast<int>(static_cast<long long>(nr) * t / n);
+        const int r1 = static_cast<int>(static_cast<long long>(nr) * (t + 1) / n);
+        h_strips.push_back({s, r0, r1, 0});
+      }
+    }
+    g.strip_count = static_cast<int>(h_strips.size()) - first;
+    return g.strip_count > 0 ? first : -1;
+  }
+
+  // Raises the error a streaming-kernel wait recorded (after a stream sync).
+  void check_kernel_error() {
+    if (d_error.ptr == nullptr) return;
+    int code = 0;
+    check(cudaMemcpy(&code, d_error.ptr, sizeof(int), cudaMemcpyDeviceToHost),
+          "read kernel error word");
+    if (code != 0) {
+      cudaMemset(d_error.ptr, 0, sizeof(int));
+      throw CudaError("stage kernel pipeline wait timed out (code " +
+                      std::to_string(code) + ")");
     }
   }
 
@@ -572,6 +661,7 @@ struct Batch {
                           stream),
           "get_state copy");
     check(cudaStreamSynchronize(stream), "get_state");
+    check_kernel_error();
   }
 
   void launch_stage_kind(const int kind, double2* input) {
@@ -612,6 +702,7 @@ struct Batch {
                           stream),
           "evaluate_rhs copy");
     check(cudaStreamSynchronize(stream), "evaluate_rhs");
+    check_kernel_error();
   }
 
   void set_dt(const std::vector<double>& dt) {
@@ -801,6 +892,7 @@ struct Batch {
           "endpoint copy");
     if (memory == TEUK_B200_HOST) {
       check(cudaStreamSynchronize(stream), "endpoint sync");
+      check_kernel_error();
     }
   }
 
@@ -881,6 +973,7 @@ struct Batch {
     return 4 * total_complex * sizeof(double2) + d_nodal.count * sizeof(double2) +
            h_mat.size() * sizeof(double) + h_trig.size() * sizeof(double) +
            h_tiles.size() * sizeof(TileDesc) + h_seg.size() * sizeof(SegmentDesc) +
+           h_strips.size() * sizeof(TileDesc) + d_coef.count * sizeof(double) +
            d_endpoint.count * sizeof(double2);
   }
 };
@@ -1050,7 +1143,8 @@ void initialize_nodal_gaussian(teuk_b200::NodalPipeline& p,
 
 
 // Device bytes one linear solve holds inside a batch: four band buffers
-// (padded segments), its matrices and the nodal import scratch.
+// (padded segments), its matrices, its row coefficients and the nodal
+// import scratch.
 size_t linear_footprint(const teuk_b200::InstancePlan& plan) {
   size_t complex_count = 0;
   size_t matrix = 0;
@@ -1062,6 +1156,8 @@ size_t linear_footprint(const teuk_b200::InstancePlan& plan) {
     matrix += 2 * static_cast<size_t>(mp.n_ell * plan.config.ntheta);
   }
   return 4 * complex_count * sizeof(double2) + matrix * sizeof(double) +
+         static_cast<size_t>(plan.config.nr) * teuk_b200::kCoefRecord *
+             sizeof(double) +
          plan.value_count() * sizeof(double2);
 }
 
@@ -1276,6 +1372,7 @@ class Server {
   void collect_step_times() {
     if (pending_ == 0) return;
     teuk_b200::check(cudaStreamSynchronize(stream_), "server steps");
+    if (batch_) batch_->check_kernel_error();
     for (int i = 0; i < pending_; ++i) {
       float ms = 0.0f;
       teuk_b200::check(cudaEventElapsedTime(&ms, events_[2 * i],
@@ -1437,6 +1534,7 @@ int teuk_b200_step(teuk_b200_pipeline* p, double time, double dt, int steps) {
     }
     p->batch->step({dt}, steps, false);
     teuk_b200::check(cudaStreamSynchronize(p->batch->stream), "step");
+    p->batch->check_kernel_error();
   });
 }
 
@@ -1467,6 +1565,7 @@ int teuk_b200_step_static_scratch(teuk_b200_pipeline* p, double time,
                      "static scratch address");
     b.step_with_slopes({dt}, steps, slopes, teuk_b200::kStaticSlopeCapacity);
     teuk_b200::check(cudaStreamSynchronize(b.stream), "step");
+    b.check_kernel_error();
   });
 }
 
@@ -1562,6 +1661,7 @@ int teuk_b200_synchronize(teuk_b200_pipeline* p) {
     teuk_b200::check(cudaStreamSynchronize(p->nodal ? p->nodal->stream()
                                                      : p->batch->stream),
                      "synchronize");
+    if (!p->nodal) p->batch->check_kernel_error();
   });
 }
 
@@ -1975,6 +2075,7 @@ int teuk_b200_batch_synchronize(teuk_b200_batch* b) {
   return guarded([&] {
     require(b != nullptr, "null batch");
     teuk_b200::check(cudaStreamSynchronize(b->batch->stream), "synchronize");
+    b->batch->check_kernel_error();
   });
 }
 
@@ -1983,6 +2084,21 @@ int teuk_b200_batch_launches_per_step(const teuk_b200_batch* b,
   return guarded([&] {
     require(b != nullptr && launches != nullptr, "null argument");
     *launches = 4 * static_cast<int>(b->batch->groups.size());
+  });
+}
+
+int teuk_b200_batch_stage_kernels(const teuk_b200_batch* b,
+                                  int* streaming_groups, int* tile_groups) {
+  return guarded([&] {
+    require(b != nullptr && streaming_groups != nullptr &&
+                tile_groups != nullptr,
+            "null argument");
+    int streaming = 0;
+    for (const teuk_b200::StageLaunch& g : b->batch->groups) {
+      if (g.strips != nullptr && g.strip_count > 0) ++streaming;
+    }
+    *streaming_groups = streaming;
+    *tile_groups = static_cast<int>(b->batch->groups.size()) - streaming;
   });
 }
 

@@ -58,7 +58,7 @@ struct InstanceDesc {
   int trig_offset;  // doubles into the trig pool: sin^2(theta)[nt], cos[nt]
   int reduction;    // 0 free damped, 1 stage constrained
   int disc;
-  int pad;
+  int coef_row0;    // first row of this solve in the coefficient table
 };
 
 struct SegmentDesc {

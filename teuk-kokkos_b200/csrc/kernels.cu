@@ -961,8 +961,40 @@ __global__ void __launch_bounds__(kThreads, 2)
   }
 }
 
+#include "stream_kernel.cuh"
+
+template <int DISC, int SC>
+cudaError_t launch_stream_typed(const StageLaunch& p, cudaStream_t stream) {
+  const size_t bytes = StreamLayout(SC).total;
+  auto kernel = stream_stage_kernel<DISC, SC>;
+  static int configured_bytes = 0;
+  static int sms = 0;
+  if (configured_bytes != static_cast<int>(bytes)) {
+    cudaError_t err = cudaFuncSetAttribute(
+        kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        static_cast<int>(bytes));
+    if (err != cudaSuccess) return err;
+    configured_bytes = static_cast<int>(bytes);
+  }
+  if (sms == 0) {
+    int device = 0;
+    cudaError_t err = cudaGetDevice(&device);
+    if (err == cudaSuccess) {
+      err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount,
+                                   device);
+    }
+    if (err != cudaSuccess) return err;
+  }
+  const int grid = p.strip_count < sms ? p.strip_count : sms;
+  kernel<<<grid, kStreamThreads, bytes, stream>>>(p);
+  return cudaGetLastError();
+}
+
 template <int DISC, int SC>
 cudaError_t launch_typed(const StageLaunch& p, cudaStream_t stream) {
+  if (p.strips != nullptr && p.strip_count > 0) {
+    return launch_stream_typed<DISC, SC>(p, stream);
+  }
   const size_t bytes = stage_smem_bytes(p);
   auto kernel = stage_kernel<DISC, SC>;
   // The opt-in limit is raised once per instantiation to the largest size
@@ -1111,6 +1143,19 @@ size_t stage_smem_bytes(const StageLaunch& p) {
       2 * static_cast<size_t>(L.nt8) +
       static_cast<size_t>(p.coef_rows) * kCoefCount;
   return complex_count * sizeof(double2) + double_count * sizeof(double);
+}
+
+cudaError_t launch_coefficient_table(const InstanceDesc* instance_device,
+                                     const int nr, const int row0,
+                                     double* table, cudaStream_t stream) {
+  if (nr <= 0) return cudaSuccess;
+  coefficient_table_kernel<<<(nr + 127) / 128, 128, 0, stream>>>(
+      instance_device, nr, table + static_cast<long long>(row0) * kCoefCount);
+  return cudaGetLastError();
+}
+
+size_t stream_smem_bytes(const int reduction) {
+  return StreamLayout(reduction == 1 ? 1 : 0).total;
 }
 
 cudaError_t upload_sbp_constants(const SbpConstants& constants) {

@@ -41,7 +41,34 @@ struct StageLaunch {
   // CTAs resident at once (SMs x CTAs per SM), set by launch_stage: the
   // tile blockIdx + prefetch_stride starts when this CTA's slot frees up
   int prefetch_stride;
+  // Radial strips for the streaming kernel (null: tile kernel only).  A
+  // strip is a TileDesc whose rows are at least kStripMinRows long.
+  const TileDesc* strips;
+  int strip_count;
+  // device word set to a non-zero code when a streaming-kernel wait timed
+  // out (read by the host after the step)
+  int* error;
+  // Teukolsky row coefficients of every solve, kCoefRecord doubles per
+  // radial row (coefficient_table_kernel); the m-dependent imaginary parts
+  // (entries 4, 6, 8) are stored for m = 1 and scaled by m where used.
+  const double* coef_table;
 };
+
+inline constexpr int kCoefRecord = 10;
+// Fills the coefficient table rows of one solve: table[(row0 + r) * 10 + k].
+cudaError_t launch_coefficient_table(const InstanceDesc* instance_device,
+                                     int nr, int row0, double* table,
+                                     cudaStream_t stream);
+
+// Streaming kernel eligibility of a launch group: n_ell <= 16 and at most 32
+// Gauss-Legendre nodes per row.
+inline constexpr int kStreamMaxEll = 16;
+inline constexpr int kStreamMaxNodes = 32;
+inline constexpr int kStripMinRows = 64;
+// Radial strips per CTA the host aims for when it splits segments.
+inline constexpr int kStripsPerCta = 8;
+// Dynamic shared memory of the streaming kernel.
+size_t stream_smem_bytes(int reduction);
 
 // Dynamic shared memory bytes for one launch description.
 size_t stage_smem_bytes(const StageLaunch& launch);

@@ -1,0 +1,965 @@
+// Streaming RK stage kernel: persistent CTAs walk radial strips of band
+// segments through a shared-memory ring filled by bulk asynchronous copies.
+// Included by kernels.cu inside its anonymous namespace (it shares the SBP
+// constant tables, the complex helpers and the FP64 MMA wrapper).
+//
+// Per CTA (one per SM, 512 threads):
+//   warps 0-7     transform warps: stage combine u = y + c k in place,
+//                 effective Q (stage-constrained reduction) and
+//                 psi_t = A diag(.) S (.) on the FP64 tensor path, two warps
+//                 per 4-row block (each takes half of the node tiles of the
+//                 synthesis and one ell tile of the analysis);
+//   warps 8-15    stencil warps: SBP derivatives, dissipation, RHS assembly
+//                 and the RK update of every output row, two rows and one
+//                 ell column per thread, split into a psi role and a P/Q
+//                 role that exchange partial sums through shared memory.
+//                 Their first thread is also the loader: it issues the
+//                 cp.async.bulk copies of each 16-row chunk of the stage
+//                 inputs and of the Teukolsky row coefficients into a
+//                 4-stage ring (completion through mbarrier transaction
+//                 counts) as soon as no later work of the strip reads the
+//                 rows a stage holds.
+// The roles run concurrently on different chunks: the copies of the next
+// chunks, the transforms of the current one and the stencils of the rows it
+// completes overlap.  Every halo row is loaded and transformed once per
+// strip.  Four warps per SM sub-partition, 128 registers per thread.
+//
+// Every wait on an mbarrier gives up after kStreamWaitNs: the waiting role
+// raises the CTA's abort flag and records an error code that the host reads
+// after the step, and the other role leaves at its next wait.
+
+constexpr int kStreamNep = 16;                              // ell lanes per row
+constexpr int kStreamMaxTheta = 32;                         // nodes per row
+constexpr int kStreamChunk = 16;                            // rows per copy
+constexpr int kStreamStages = 4;                            // ring stages
+constexpr int kStreamRing = kStreamChunk * kStreamStages;  // ring rows
+constexpr int kStreamTWarps = 8;
+constexpr int kStreamSWarps = 8;
+constexpr int kStreamThreads = 32 * (kStreamTWarps + kStreamSWarps);
+constexpr int kStreamTThreads = 32 * kStreamTWarps;
+constexpr int kStreamSThreads = 32 * kStreamSWarps;
+constexpr int kStreamRB = 2;     // rows per stencil thread
+constexpr int kStreamBlocks = 4;  // 4-row transform blocks per 16 rows
+constexpr unsigned long long kStreamWaitNs = 2000000000ull;
+static_assert(kStreamNep == kStreamMaxEll, "ell lanes");
+static_assert(kStreamMaxTheta == kStreamMaxNodes, "node tiles");
+static_assert(kStripMinRows >= 2 * 17, "strip edges clear of closures");
+static_assert(kCoefRecord == kCoefCount, "coefficient record");
+static_assert(kStreamSThreads == 2 * kStreamNep * kStreamChunk / kStreamRB,
+              "one stencil thread per (role, row pair, ell)");
+static_assert(kStreamTWarps == 2 * kStreamBlocks, "two warps per block");
+constexpr int kStreamXs = 20;  // padded staging strides (bank-conflict free)
+constexpr int kStreamTs = 36;
+
+__device__ __forceinline__ unsigned smem_u32(const void* ptr) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(ptr));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar,
+                                          const unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;"
+               :
+               : "r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];"
+               :
+               : "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar,
+                                                      const unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+               :
+               : "r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar,
+                                              const unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// global -> shared bulk copy completing on `bar` (no multicast)
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src,
+                                              const unsigned bytes,
+                                              unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1], %2, [%3];"
+      :
+      : "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_mbarrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void named_sync(const int id, const int threads) {
+  asm volatile("bar.sync %0, %1;" : : "r"(id), "r"(threads) : "memory");
+}
+// Barrier over `threads` threads of the CTA that also ANDs `pred` across
+// them: every participant gets the same answer.
+__device__ __forceinline__ bool named_sync_and(const int id, const int threads,
+                                               const bool pred) {
+  unsigned all;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(all)
+      : "r"(pred ? 1u : 0u), "r"(id), "r"(threads)
+      : "memory");
+  return all != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait for the phase of `bar` with the given parity.  False when
+// the CTA is aborting (this wait timed out, or another one did).
+__device__ bool stream_wait(unsigned long long* bar, const unsigned parity,
+                            volatile int* abort_flag, int* error,
+                            const int code) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (true) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (*abort_flag != 0) return false;
+    if (global_ns() - t0 > kStreamWaitNs) {
+      *abort_flag = 1;
+      if (error != nullptr) atomicExch(error, code);
+      return false;
+    }
+  }
+}
+
+// Row range bookkeeping of one strip (rows of one segment).
+struct StripGeom {
+  long long seg_offset;  // complex offset of row 0 of the segment
+  int segment, instance, m, ne, rs, nr, coef_row0;
+  int r0, r1;  // output rows
+  int s0, s1;  // input rows (with halo)
+  int t0, t1;  // psi_t / effective-Q rows
+  int chunks;
+  int shift;  // ring row of absolute row q: (q + shift) & (kStreamRing - 1)
+};
+
+// Loader state, kept in shared memory (only its one thread touches it).
+struct StreamLoaderState {
+  StripGeom sg;  // geometry of `strip`
+  int strip;     // strip of the next chunk to load (>= strip_count: done)
+  int c;         // its chunk index within the strip
+  int g;         // its global chunk index
+  int prev_rs;   // row stride of the strip of chunk g - 1
+};
+
+// Shared-memory carve-up (bytes), identical on host and device.
+struct StreamLayout {
+  static constexpr int kRowMax = 3 * kStreamNep;  // complex per ring row
+  size_t bars, loader, uring, xring, aring, pring, qring, coef, xw, tw, xch,
+      total;
+  __host__ __device__ explicit StreamLayout(const int sc) {
+    size_t o = 0;
+    bars = o;
+    o += 128;  // 2 x stages mbarriers + abort flag
+    loader = o;
+    o += (sizeof(StreamLoaderState) + 127) / 128 * 128;
+    const size_t ring = static_cast<size_t>(kStreamRing) * kRowMax * 16;
+    uring = o;
+    o += ring;
+    xring = o;
+    o += ring;
+    aring = o;
+    o += ring;
+    pring = o;
+    o += static_cast<size_t>(kStreamRing) * kStreamNep * 16;
+    qring = o;
+    if (sc) o += static_cast<size_t>(kStreamRing) * kStreamNep * 16;
+    coef = o;
+    o += static_cast<size_t>(kStreamRing) * kCoefCount * 8;
+    xw = o;
+    o += static_cast<size_t>(kStreamBlocks) * 16 * kStreamXs * 8;
+    tw = o;
+    o += static_cast<size_t>(kStreamBlocks) * 8 * kStreamTs * 8;
+    xch = o;
+    o += static_cast<size_t>(kStreamSThreads / 2) * 2 * kStreamRB * 16;
+    total = o;
+  }
+};
+
+template <int H, int HD>
+__device__ __forceinline__ StripGeom strip_geom(const StageLaunch& p,
+                                                const int strip,
+                                                const int first_chunk) {
+  const TileDesc t = p.strips[strip];
+  const SegmentDesc seg = p.segments[t.segment];
+  const InstanceDesc& in = p.instances[seg.instance];
+  StripGeom g;
+  g.seg_offset = seg.offset;
+  g.segment = t.segment;
+  g.instance = seg.instance;
+  g.m = seg.m;
+  g.ne = seg.n_ell;
+  g.rs = 3 * seg.n_ell;
+  g.nr = in.nr;
+  g.coef_row0 = in.coef_row0;
+  g.r0 = t.r0;
+  g.r1 = t.r1;
+  g.s0 = max(0, t.r0 - H);
+  g.s1 = min(g.nr, t.r1 + H);
+  g.t0 = max(0, t.r0 - HD);
+  g.t1 = min(g.nr, t.r1 + HD);
+  g.chunks = (g.s1 - g.s0 + kStreamChunk - 1) / kStreamChunk;
+  g.shift = first_chunk * kStreamChunk - g.s0;
+  return g;
+}
+
+__device__ __forceinline__ int ring_row(const int q, const int shift) {
+  return (q + shift) & (kStreamRing - 1);
+}
+
+// First row that is not yet computable for a stencil of half width `half`
+// (closure: rows below `closure_rows` read the first `need` rows, rows in
+// the last `closure_rows` read the last ones) when rows [.., avail) exist.
+__device__ __forceinline__ int computable_end(const int avail, const int nr,
+                                              const int half, const int need,
+                                              const int closure_rows) {
+  if (avail >= nr) return nr;
+  if (avail < need) return 0;
+  return min(avail - half, nr - closure_rows);
+}
+
+// SBP first derivative / dissipation with an accessor for absolute rows
+// (closure rows included); mirrors sbp_derivative / sbp_dissipation.
+template <int DISC, class Row>
+__device__ __forceinline__ double2 ring_derivative(const Row& at, const int r,
+                                                   const int nr) {
+  using T = DiscTraits<DISC>;
+  double2 acc = make_double2(0.0, 0.0);
+  if (r < T::BR) {
+#pragma unroll
+    for (int c = 0; c < T::W; ++c) acc = cfma(c_sbp.left[DISC][r][c], at(c), acc);
+  } else if (r + T::BR >= nr) {
+    const int rr = nr - 1 - r;
+#pragma unroll
+    for (int c = 0; c < T::W; ++c) {
+      acc = cfma(-c_sbp.left[DISC][rr][c], at(nr - 1 - c), acc);
+    }
+  } else {
+#pragma unroll
+    for (int k = T::HALF; k >= 1; --k) {
+      acc = cfma(c_sbp.interior[DISC][k], csub(at(r + k), at(r - k)), acc);
+    }
+  }
+  return acc;
+}
+
+template <int DISC, class Row>
+__device__ __forceinline__ double2 ring_dissipation(const Row& at, const int r,
+                                                    const int nr) {
+  using T = DiscTraits<DISC>;
+  double2 acc = make_double2(0.0, 0.0);
+  if (r < T::SPECIAL) {
+    for (int j = 0; j <= r + T::P; ++j) {
+      acc = cfma(c_sbp.diss_left[DISC][r][j], at(j), acc);
+    }
+  } else if (r >= nr - T::SPECIAL) {
+    const int rr = nr - 1 - r;
+    for (int j = 0; j <= rr + T::P; ++j) {
+      acc = cfma(c_sbp.diss_left[DISC][rr][j], at(nr - 1 - j), acc);
+    }
+  } else {
+    acc = cscale(c_sbp.diss_interior[DISC][0], at(r));
+#pragma unroll
+    for (int k = 1; k <= T::P; ++k) {
+      acc = cfma(c_sbp.diss_interior[DISC][k], cadd(at(r + k), at(r - k)), acc);
+    }
+  }
+  return acc;
+}
+
+// Register window of N ring rows starting at absolute row `first`.
+template <int N>
+__device__ __forceinline__ void ring_window(double2 (&w)[N],
+                                            const double2* column,
+                                            const int first, const int shift,
+                                            const int stride) {
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    w[i] = column[ring_row(first + i, shift) * stride];
+  }
+}
+
+// ------------------------------------------------------------- loader
+// Issues the bulk copies of the CTA's chunk sequence (strips blockIdx.x,
+// blockIdx.x + gridDim.x, ...; chunks of kStreamChunk rows each), one
+// chunk per free ring stage.  Run by one thread.
+template <int H, int HD>
+__device__ void loader_init(const StageLaunch& p, StreamLoaderState& L) {
+  L.strip = blockIdx.x;
+  L.c = 0;
+  L.g = 0;
+  L.prev_rs = -1;
+  if (L.strip < p.strip_count) L.sg = strip_geom<H, HD>(p, L.strip, 0);
+}
+
+// Load chunks while ring stages are free.  `released` = chunks handed back
+// so far.  A strip with another row stride starts only on an empty ring
+// (its rows would overlap the live stages' rows otherwise).
+template <int H, int HD>
+__device__ void loader_pump(const StageLaunch& p, StreamLoaderState& L,
+                            unsigned long long* full, double2* U, double2* X,
+                            double2* A, double* CF, const int released) {
+  const double2* src_u;
+  const double2* src_x = nullptr;
+  const double2* src_a = nullptr;
+  switch (p.stage) {
+    case kStage2: src_u = p.y; src_x = p.kA; break;
+    case kStage3: src_u = p.kB; src_x = p.y; src_a = p.acc; break;
+    case kStage4: src_u = p.kA; src_a = p.acc; break;
+    default: src_u = p.y; break;  // stage 1 and the RHS-only evaluation
+  }
+  while (L.strip < p.strip_count && L.g < released + kStreamStages) {
+    const StripGeom& sg = L.sg;
+    if (L.c == 0 && L.prev_rs >= 0 && sg.rs != L.prev_rs && released < L.g) {
+      return;
+    }
+    const int s = L.g % kStreamStages;
+    const int a0 = sg.s0 + L.c * kStreamChunk;
+    const int a1 = min(sg.s1, a0 + kStreamChunk);
+    const unsigned row_bytes = static_cast<unsigned>(sg.rs) * 16u;
+    const unsigned bytes_u = static_cast<unsigned>(a1 - a0) * row_bytes;
+    const unsigned bytes_x = src_x != nullptr ? bytes_u : 0u;
+    const int o0 = max(a0, sg.r0), o1 = min(a1, sg.r1);
+    const unsigned bytes_a = (src_a != nullptr && o1 > o0)
+                                 ? static_cast<unsigned>(o1 - o0) * row_bytes
+                                 : 0u;
+    const unsigned bytes_c =
+        static_cast<unsigned>(a1 - a0) * kCoefCount * sizeof(double);
+    // earlier generic-proxy accesses of the stage come before the copies
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&full[s], bytes_u + bytes_x + bytes_a + bytes_c);
+    const long long gsrc = sg.seg_offset + static_cast<long long>(a0) * sg.rs;
+    const int ra0 = ring_row(a0, sg.shift);
+    bulk_copy_g2s(U + ra0 * sg.rs, src_u + gsrc, bytes_u, &full[s]);
+    if (bytes_x != 0u) bulk_copy_g2s(X + ra0 * sg.rs, src_x + gsrc, bytes_x, &full[s]);
+    if (bytes_a != 0u) {
+      bulk_copy_g2s(A + ring_row(o0, sg.shift) * sg.rs,
+                    src_a + sg.seg_offset + static_cast<long long>(o0) * sg.rs,
+                    bytes_a, &full[s]);
+    }
+    bulk_copy_g2s(CF + ra0 * kCoefCount,
+                  p.coef_table +
+                      static_cast<long long>(sg.coef_row0 + a0) * kCoefCount,
+                  bytes_c, &full[s]);
+    L.prev_rs = sg.rs;
+    ++L.g;
+    if (++L.c == sg.chunks) {
+      L.c = 0;
+      L.strip += gridDim.x;
+      if (L.strip < p.strip_count) L.sg = strip_geom<H, HD>(p, L.strip, L.g);
+    }
+  }
+}
+
+// After an abort: copies still in flight land before the CTA exits.
+__device__ void loader_drain(const StreamLoaderState& L,
+                             unsigned long long* full) {
+  for (int back = 1; back <= kStreamStages && L.g - back >= 0; ++back) {
+    const int gb = L.g - back;
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try_wait(&full[gb % kStreamStages],
+                          static_cast<unsigned>(gb / kStreamStages) & 1u)) {
+      if (global_ns() - t0 > kStreamWaitNs) break;
+    }
+  }
+}
+
+// ------------------------------------------------------------- transforms
+// Node fragments of one transform warp: synthesis node tiles 2h, 2h + 1,
+// analysis ell tile h.
+struct PsiFragments {
+  double fs[2][4];  // S(j = (2h + i) * 8 + group, l = ks * 4 + quad)
+  double fa[8];     // A(l = h * 8 + group, j = ks * 4 + quad)
+  double a2s2[2];   // a^2 sin^2(theta_j)
+  double gcos[2];   // 2 s a cos(theta_j)
+};
+
+// psi_t of the 4-row block at q0 (rows >= qlim skipped): this warp's half
+// of the synthesis and of the analysis.  xw / tw are the block's staging
+// buffers, shared with the partner warp; `bar` synchronises the 256
+// transform threads between the phases.
+template <int SC>
+__device__ __forceinline__ void stream_psi_half(
+    const int q0, const int qlim, const int h, const StripGeom& sg,
+    const double2* U, const double2* QE, const double* CF, double2* PS,
+    double* xw, double* tw, const PsiFragments& F, const int nt,
+    const int mts, const int ksa, const int lane) {
+  const int quad = lane & 3;
+  const int group = lane >> 2;
+  const int ne = sg.ne;
+  const double mm = static_cast<double>(sg.m);
+  {  // stage rows 2h, 2h + 1 of the block: v1 = P + 2K Q - G psi, psi
+    const int rho = 2 * h + (lane >> 4);
+    const int l = lane & 15;
+    const int r = q0 + rho;
+    double2 v1 = make_double2(0.0, 0.0), psi = make_double2(0.0, 0.0);
+    if (r < qlim && l < ne) {
+      const int rr = ring_row(r, sg.shift);
+      const double* cf = CF + rr * kCoefCount;
+      const double2* row = U + rr * sg.rs;
+      const double2 Q = SC ? QE[rr * kStreamNep + l] : row[ne + l];
+      psi = row[2 * ne + l];
+      v1 = csub(cadd(row[l], cscale(2.0 * cf[1], Q)),
+                cmul(make_double2(cf[3], mm * cf[4]), psi));
+    }
+    xw[(rho * 4 + 0) * kStreamXs + l] = v1.x;
+    xw[(rho * 4 + 1) * kStreamXs + l] = v1.y;
+    xw[(rho * 4 + 2) * kStreamXs + l] = psi.x;
+    xw[(rho * 4 + 3) * kStreamXs + l] = psi.y;
+  }
+  named_sync(1, kStreamTThreads);
+  double bx[2][4];
+#pragma unroll
+  for (int n = 0; n < 2; ++n) {
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks) {
+      bx[n][ks] = xw[(n * 8 + group) * kStreamXs + ks * 4 + quad];
+    }
+  }
+  double c0r[2];  // C_T without the sin^2 term, rows 2n + (quad >> 1)
+#pragma unroll
+  for (int n = 0; n < 2; ++n) {
+    const int r = q0 + 2 * n + (quad >> 1);
+    c0r[n] = r < qlim ? CF[ring_row(r, sg.shift) * kCoefCount] : 1.0;
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const int mt = 2 * h + i;
+    if (mt < mts) {
+      double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) {
+#pragma unroll
+        for (int n = 0; n < 2; ++n) {
+          dmma(acc[n][0], acc[n][1], F.fs[i][ks], bx[n][ks]);
+        }
+      }
+      const int j = mt * 8 + group;
+      const bool node = j < nt;
+      double inv[2];
+#pragma unroll
+      for (int n = 0; n < 2; ++n) {
+        const int r = q0 + 2 * n + (quad >> 1);
+        inv[n] = (node && r < qlim) ? 1.0 / (c0r[n] - F.a2s2[i]) : 0.0;
+      }
+#pragma unroll
+      for (int n = 0; n < 2; ++n) {
+        // lane quad 0/2 holds a_j of a row, quad 1/3 holds b_j of that row
+        const double o0 = __shfl_xor_sync(0xffffffffu, acc[n][0], 1);
+        const double o1 = __shfl_xor_sync(0xffffffffu, acc[n][1], 1);
+        if ((quad & 1) == 0) {
+          const int rho = 2 * n + (quad >> 1);
+          tw[(rho * 2 + 0) * kStreamTs + j] =
+              (acc[n][0] + F.gcos[i] * o1) * inv[n];
+          tw[(rho * 2 + 1) * kStreamTs + j] =
+              (acc[n][1] - F.gcos[i] * o0) * inv[n];
+        }
+      }
+    }
+  }
+  named_sync(1, kStreamTThreads);
+  double c[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+  for (int ks = 0; ks < 8; ++ks) {
+    if (ks < ksa) {
+      const double b = tw[group * kStreamTs + ks * 4 + quad];
+      dmma(c[ks & 1][0], c[ks & 1][1], F.fa[ks], b);
+    }
+  }
+  const int l = h * 8 + group;
+  const int r = q0 + quad;
+  if (r < qlim && l < ne) {
+    PS[ring_row(r, sg.shift) * kStreamNep + l] =
+        make_double2(c[0][0] + c[1][0], c[0][1] + c[1][1]);
+  }
+}
+
+template <int DISC, int SC>
+__device__ void stream_transform(const StageLaunch& p,
+                                 unsigned long long* full,
+                                 unsigned long long* ready,
+                                 volatile int* abort_flag, double2* U,
+                                 const double2* X, double2* PS, double2* QE,
+                                 const double* CF, double* xw_all,
+                                 double* tw_all, const int tt) {
+  using T = DiscTraits<DISC>;
+  constexpr int P = T::P, HD = T::HALF;
+  constexpr int H = SC ? (P > 2 * HD ? P : 2 * HD) : P;
+  const int warp = tt >> 5, lane = tt & 31;
+  const int quad = lane & 3, group = lane >> 2;
+  const int blk = warp >> 1, h = warp & 1;
+  double* xw = xw_all + blk * 16 * kStreamXs;
+  double* tw = tw_all + blk * 8 * kStreamTs;
+  // zero the nodal staging once: columns beyond a solve's nodes stay zero
+  for (int i = tt; i < kStreamBlocks * 8 * kStreamTs; i += kStreamTThreads) {
+    tw_all[i] = 0.0;
+  }
+  int g = 0;
+  for (int strip = blockIdx.x; strip < p.strip_count; strip += gridDim.x) {
+    const StripGeom sg = strip_geom<H, HD>(p, strip, g);
+    const InstanceDesc& in = p.instances[sg.instance];
+    const int nt = in.ntheta, ne = sg.ne, nr = sg.nr;
+    const bool kerr = in.spin != 0.0;
+    const double hdt = 0.5 * in.dt;
+    const double inv_h = in.inv_spacing;
+    const double mm = static_cast<double>(sg.m);
+    PsiFragments F;
+    const int mts = (nt + 7) / 8, ksa = (nt + 3) / 4;
+    if (kerr) {
+      const SegmentDesc& seg = p.segments[sg.segment];
+      const double* St = p.matrices + seg.mat_offset;  // St[l][j]
+      const double* At = St + ne * nt;                 // At[j][l]
+      const double a2 = in.spin * in.spin;
+      const double sa2 = 2.0 * (static_cast<double>(kSpinWeight) * in.spin);
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int j = (2 * h + i) * 8 + group;
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks) {
+          const int l = ks * 4 + quad;
+          F.fs[i][ks] = (j < nt && l < ne) ? St[l * nt + j] : 0.0;
+        }
+        const double sj = j < nt ? p.trig[in.trig_offset + j] : 0.0;
+        F.a2s2[i] = a2 * sj * sj;
+        F.gcos[i] = j < nt ? sa2 * p.trig[in.trig_offset + nt + j] : 0.0;
+      }
+      const int l = h * 8 + group;
+#pragma unroll
+      for (int ks = 0; ks < 8; ++ks) {
+        const int j = ks * 4 + quad;
+        F.fa[ks] = (j < nt && l < ne) ? At[j * ne + l] : 0.0;
+      }
+    }
+    int pd = sg.t0;  // psi_t rows done
+    for (int c = 0; c < sg.chunks; ++c, ++g) {
+      const int s = g % kStreamStages;
+      // every transform thread waits; all of them leave together on abort
+      const bool landed =
+          stream_wait(&full[s], static_cast<unsigned>(g / kStreamStages) & 1u,
+                      abort_flag, p.error, 3);
+      if (!named_sync_and(1, kStreamTThreads, landed)) return;
+      const int a0 = sg.s0 + c * kStreamChunk;
+      const int a1 = min(sg.s1, a0 + kStreamChunk);
+      // stage input u = y + dt/2 k, in place
+      if (p.stage == kStage2 || p.stage == kStage3) {
+        const int base = ring_row(a0, sg.shift) * sg.rs;
+        const int count = (a1 - a0) * sg.rs;
+        double2* u = U + base;
+        const double2* x = X + base;
+        if (p.stage == kStage2) {  // U = y, X = k1
+          for (int i = tt; i < count; i += kStreamTThreads) {
+            u[i] = cfma(hdt, x[i], u[i]);
+          }
+        } else {  // U = k2, X = y
+          for (int i = tt; i < count; i += kStreamTThreads) {
+            u[i] = cfma(hdt, u[i], x[i]);
+          }
+        }
+        named_sync(1, kStreamTThreads);
+      }
+      int pe;
+      if (SC) {
+        // effective Q = D psi on rows [pd, qe)
+        const int qe = min(sg.t1, computable_end(a1, nr, T::HALF, T::W, T::BR));
+        const int items = max(0, qe - pd) * kStreamNep;
+        for (int i = tt; i < items; i += kStreamTThreads) {
+          const int r = pd + i / kStreamNep;
+          const int l = i % kStreamNep;
+          if (l < ne) {
+            const double2* col = U + 2 * ne + l;
+            const int shift = sg.shift, rs = sg.rs;
+            auto at = [=](const int q) { return col[ring_row(q, shift) * rs]; };
+            QE[ring_row(r, sg.shift) * kStreamNep + l] =
+                cscale(inv_h, ring_derivative<DISC>(at, r, nr));
+          }
+        }
+        named_sync(1, kStreamTThreads);
+        pe = qe;
+      } else {
+        pe = min(sg.t1, a1);
+      }
+      if (pe > pd) {
+        if (kerr) {
+          for (int q = pd; q < pe; q += 4 * kStreamBlocks) {
+            stream_psi_half<SC>(q + 4 * blk, pe, h, sg, U, QE, CF, PS, xw, tw,
+                                F, nt, mts, ksa, lane);
+          }
+        } else {
+          const int items = (pe - pd) * kStreamNep;
+          for (int i = tt; i < items; i += kStreamTThreads) {
+            const int r = pd + i / kStreamNep;
+            const int l = i % kStreamNep;
+            if (l < ne) {
+              const int rr = ring_row(r, sg.shift);
+              const double* cf = CF + rr * kCoefCount;
+              const double2* row = U + rr * sg.rs;
+              const double2 Q = SC ? QE[rr * kStreamNep + l] : row[ne + l];
+              const double2 psi = row[2 * ne + l];
+              const double2 num =
+                  csub(cadd(row[l], cscale(2.0 * cf[1], Q)),
+                       cmul(make_double2(cf[3], mm * cf[4]), psi));
+              PS[rr * kStreamNep + l] = cscale(cf[9], num);
+            }
+          }
+        }
+        pd = pe;
+      }
+      // the combine wrote ring rows that later bulk copies overwrite
+      fence_proxy_async_smem();
+      mbar_arrive(&ready[s]);
+    }
+  }
+}
+
+// ------------------------------------------------------------- stencils
+// RK update of one field column for `cnt` rows from the stage slope k.
+__device__ __forceinline__ void stream_rk_update(
+    const StageLaunch& p, const StripGeom& sg, const double2* X,
+    const double2* A, const int ra, const int cnt, const int f, const int l,
+    const double2 (&k)[kStreamRB], const double dt, const double dt6) {
+  const long long g0 =
+      sg.seg_offset + static_cast<long long>(ra) * sg.rs + f * sg.ne + l;
+#pragma unroll
+  for (int i = 0; i < kStreamRB; ++i) {
+    if (i >= cnt) break;
+    const long long gi = g0 + static_cast<long long>(i) * sg.rs;
+    const int ri = ring_row(ra + i, sg.shift) * sg.rs + f * sg.ne + l;
+    switch (p.stage) {
+      case kStage2:  // X = k1
+        p.kB[gi] = k[i];
+        p.acc[gi] = cfma(2.0, k[i], X[ri]);
+        break;
+      case kStage3: {  // X = y, A = k1 + 2 k2
+        const double2 y0 = X[ri];
+        p.acc[gi] = cfma(dt6, cfma(2.0, k[i], A[ri]), y0);
+        p.kA[gi] = cfma(dt, k[i], y0);
+        break;
+      }
+      case kStage4:  // A = y + dt/6 (k1 + 2 k2 + 2 k3)
+        p.y[gi] = cfma(dt6, k[i], A[ri]);
+        break;
+      default:  // stage 1 and the RHS-only evaluation
+        p.kA[gi] = k[i];
+        break;
+    }
+  }
+}
+
+template <int DISC, int SC>
+__device__ void stream_stencil(const StageLaunch& p,
+                               unsigned long long* full,
+                               unsigned long long* ready,
+                               volatile int* abort_flag,
+                               StreamLoaderState& loader, double2* U,
+                               double2* X, double2* A, const double2* PS,
+                               const double2* QE, double* CF, double2* xch,
+                               const int st) {
+  using T = DiscTraits<DISC>;
+  constexpr int P = T::P, HD = T::HALF;
+  constexpr int H = SC ? (P > 2 * HD ? P : 2 * HD) : P;
+  constexpr int RB = kStreamRB;
+  constexpr int HALF_THREADS = kStreamSThreads / 2;
+  const int role = st / HALF_THREADS;  // 0: psi, 1: P and Q
+  const int jr = st % HALF_THREADS;
+  const int rb = jr / kStreamNep;
+  const int l = jr % kStreamNep;
+  if (st == 0) {
+    loader_init<H, HD>(p, loader);
+    loader_pump<H, HD>(p, loader, full, U, X, A, CF, 0);
+  }
+  int g = 0;
+  for (int strip = blockIdx.x; strip < p.strip_count; strip += gridDim.x) {
+    const int g0 = g;
+    const StripGeom sg = strip_geom<H, HD>(p, strip, g0);
+    const InstanceDesc& in = p.instances[sg.instance];
+    const int ne = sg.ne, nr = sg.nr, rs = sg.rs;
+    const double inv_h = in.inv_spacing;
+    const double diss_scale = in.dissipation * inv_h;
+    const bool dissipate = in.dissipation > 0.0;
+    const double damping = in.damping;
+    const double dt = in.dt, dt6 = in.dt / 6.0;
+    const double mm = static_cast<double>(sg.m);
+    const int ell = (l < ne) ? (p.segments[sg.segment].ell_min + l) : 0;
+    const double lambda = -static_cast<double>((ell - kSpinWeight) *
+                                               (ell + kSpinWeight + 1));
+    int out_done = sg.r0;
+    int rel = g0;  // next chunk of this strip to hand back
+    for (int c = 0; c < sg.chunks; ++c, ++g) {
+      const int s = g % kStreamStages;
+      const bool done =
+          stream_wait(&ready[s], static_cast<unsigned>(g / kStreamStages) & 1u,
+                      abort_flag, p.error, 4);
+      if (!named_sync_and(2, kStreamSThreads, done)) {
+        if (st == 0) loader_drain(loader, full);
+        return;
+      }
+      const int u_end = min(sg.s1, sg.s0 + (c + 1) * kStreamChunk);
+      int lim = min(sg.r1, computable_end(u_end, nr, T::P, T::SPECIAL + T::P,
+                                          T::SPECIAL));
+      lim = min(lim, computable_end(u_end, nr, T::HALF, T::W, T::BR));
+      int pe;
+      if (SC) {
+        const int qe =
+            min(sg.t1, computable_end(u_end, nr, T::HALF, T::W, T::BR));
+        lim = min(lim, computable_end(qe, nr, T::HALF, T::W, T::BR));
+        pe = qe;
+      } else {
+        pe = min(sg.t1, u_end);
+      }
+      lim = min(lim, computable_end(pe, nr, T::HALF, T::W, T::BR));
+      for (int o = out_done; o < lim; o += kStreamChunk) {
+        const int ra = o + RB * rb;
+        const int cnt = min(RB, lim - ra);
+        const bool active = cnt > 0 && l < ne;
+        const bool interior =
+            cnt == RB && ra >= T::BR && ra + RB + T::BR <= nr;
+        double2 kx[RB], ky[RB];  // psi role: kP_a, kQ_a; P/Q role: kP, kQ
+        double2 kpsi[RB];
+#pragma unroll
+        for (int i = 0; i < RB; ++i) {
+          kx[i] = ky[i] = kpsi[i] = make_double2(0.0, 0.0);
+        }
+        if (active && role == 0) {
+          if (interior) {
+            {
+              double2 w[RB + 2 * P];
+              ring_window(w, U + 2 * ne + l, ra - P, sg.shift, rs);
+#pragma unroll
+              for (int i = 0; i < RB; ++i) {
+                const double* cf = CF + ring_row(ra + i, sg.shift) * kCoefCount;
+                const double2 dpsi =
+                    cscale(inv_h, window_derivative<DISC, RB, P>(w, i));
+                ky[i] = cscale(damping, dpsi);
+                if (dissipate) {
+                  kpsi[i] = cscale(diss_scale,
+                                   window_dissipation<DISC, RB, P>(w, i));
+                }
+                const double2 psi = w[i + P];
+                kx[i] = cadd(cmul(make_double2(cf[7], mm * cf[8]), psi),
+                             cscale(lambda, psi));
+              }
+            }
+            double2 wt[RB + 2 * HD];
+            ring_window(wt, PS + l, ra - HD, sg.shift, kStreamNep);
+#pragma unroll
+            for (int i = 0; i < RB; ++i) {
+              ky[i] = cadd(ky[i], cscale(inv_h,
+                                         window_derivative<DISC, RB, HD>(wt, i)));
+              kpsi[i] = cadd(kpsi[i], wt[i + HD]);
+            }
+          } else {
+            const double2* cpsi = U + 2 * ne + l;
+            const double2* cpt = PS + l;
+            const int shift = sg.shift;
+            auto at_psi = [=](const int q) {
+              return cpsi[ring_row(q, shift) * rs];
+            };
+            auto at_pt = [=](const int q) {
+              return cpt[ring_row(q, shift) * kStreamNep];
+            };
+#pragma unroll
+            for (int i = 0; i < RB; ++i) {
+              if (i >= cnt) break;
+              const int r = ra + i;
+              const double* cf = CF + ring_row(r, sg.shift) * kCoefCount;
+              const double2 psi = at_psi(r);
+              const double2 dpsi =
+                  cscale(inv_h, ring_derivative<DISC>(at_psi, r, nr));
+              ky[i] = cadd(cscale(damping, dpsi),
+                           cscale(inv_h, ring_derivative<DISC>(at_pt, r, nr)));
+              kpsi[i] = at_pt(r);
+              if (dissipate) {
+                kpsi[i] = cfma(diss_scale, ring_dissipation<DISC>(at_psi, r, nr),
+                               kpsi[i]);
+              }
+              kx[i] = cadd(cmul(make_double2(cf[7], mm * cf[8]), psi),
+                           cscale(lambda, psi));
+            }
+          }
+          stream_rk_update(p, sg, X, A, ra, cnt, 2, l, kpsi, dt, dt6);
+#pragma unroll
+          for (int i = 0; i < RB; ++i) {
+            xch[(i * 2 + 0) * HALF_THREADS + jr] = kx[i];
+            xch[(i * 2 + 1) * HALF_THREADS + jr] = ky[i];
+          }
+        } else if (active) {  // role 1: P and Q
+          if (interior) {
+            double2 w[RB + 2 * P];
+            ring_window(w, U + ne + l, ra - P, sg.shift, rs);
+#pragma unroll
+            for (int i = 0; i < RB; ++i) {
+              const double2 Q = w[i + P];
+              ky[i] = cscale(-damping, Q);
+              if (dissipate) {
+                ky[i] = cfma(diss_scale, window_dissipation<DISC, RB, P>(w, i),
+                             ky[i]);
+              }
+              if (!SC) {
+                const double* cf = CF + ring_row(ra + i, sg.shift) * kCoefCount;
+                const double2 dq =
+                    cscale(inv_h, window_derivative<DISC, RB, P>(w, i));
+                kx[i] = cadd(cscale(cf[2], dq),
+                             cmul(make_double2(cf[5], mm * cf[6]), Q));
+              }
+            }
+            if (SC) {
+              double2 wq[RB + 2 * HD];
+              ring_window(wq, QE + l, ra - HD, sg.shift, kStreamNep);
+#pragma unroll
+              for (int i = 0; i < RB; ++i) {
+                const double* cf = CF + ring_row(ra + i, sg.shift) * kCoefCount;
+                const double2 dq =
+                    cscale(inv_h, window_derivative<DISC, RB, HD>(wq, i));
+                kx[i] = cadd(cscale(cf[2], dq),
+                             cmul(make_double2(cf[5], mm * cf[6]), wq[i + HD]));
+              }
+            }
+            if (dissipate) {
+              ring_window(w, U + l, ra - P, sg.shift, rs);
+#pragma unroll
+              for (int i = 0; i < RB; ++i) {
+                kx[i] = cfma(diss_scale, window_dissipation<DISC, RB, P>(w, i),
+                             kx[i]);
+              }
+            }
+          } else {
+            const double2* cq = U + ne + l;
+            const double2* cp = U + l;
+            const double2* cqe = QE + l;
+            const int shift = sg.shift;
+            auto at_q = [=](const int q) { return cq[ring_row(q, shift) * rs]; };
+            auto at_p = [=](const int q) { return cp[ring_row(q, shift) * rs]; };
+            auto at_qe = [=](const int q) {
+              return cqe[ring_row(q, shift) * kStreamNep];
+            };
+#pragma unroll
+            for (int i = 0; i < RB; ++i) {
+              if (i >= cnt) break;
+              const int r = ra + i;
+              const double* cf = CF + ring_row(r, sg.shift) * kCoefCount;
+              const double2 Q = at_q(r);
+              ky[i] = cscale(-damping, Q);
+              if (dissipate) {
+                ky[i] = cfma(diss_scale, ring_dissipation<DISC>(at_q, r, nr),
+                             ky[i]);
+              }
+              if (SC) {
+                const double2 dq =
+                    cscale(inv_h, ring_derivative<DISC>(at_qe, r, nr));
+                kx[i] = cadd(cscale(cf[2], dq),
+                             cmul(make_double2(cf[5], mm * cf[6]), at_qe(r)));
+              } else {
+                const double2 dq =
+                    cscale(inv_h, ring_derivative<DISC>(at_q, r, nr));
+                kx[i] = cadd(cscale(cf[2], dq),
+                             cmul(make_double2(cf[5], mm * cf[6]), Q));
+              }
+              if (dissipate) {
+                kx[i] = cfma(diss_scale, ring_dissipation<DISC>(at_p, r, nr),
+                             kx[i]);
+              }
+            }
+          }
+        }
+        named_sync(2, kStreamSThreads);  // partial sums of the psi role
+        if (active && role == 1) {
+#pragma unroll
+          for (int i = 0; i < RB; ++i) {
+            kx[i] = cadd(xch[(i * 2 + 0) * HALF_THREADS + jr], kx[i]);
+            ky[i] = cadd(xch[(i * 2 + 1) * HALF_THREADS + jr], ky[i]);
+          }
+          stream_rk_update(p, sg, X, A, ra, cnt, 0, l, kx, dt, dt6);
+          stream_rk_update(p, sg, X, A, ra, cnt, 1, l, ky, dt, dt6);
+        }
+        named_sync(2, kStreamSThreads);  // exchange buffer free again
+      }
+      out_done = max(out_done, lim);
+      // rows below `bound` are read by no later work of this strip
+      int bound;
+      if (c == sg.chunks - 1) {
+        bound = 1 << 30;
+      } else if (out_done < T::BR) {
+        bound = 0;
+      } else {
+        bound = min(out_done - H, nr - T::SPECIAL - T::P);
+      }
+      if (st == 0) {
+        while (rel <= g &&
+               min(sg.s1, sg.s0 + (rel - g0 + 1) * kStreamChunk) <= bound) {
+          ++rel;
+        }
+        loader_pump<H, HD>(p, loader, full, U, X, A, CF, rel);
+      }
+    }
+  }
+}
+
+template <int DISC, int SC>
+__global__ void __launch_bounds__(kStreamThreads, 1)
+    stream_stage_kernel(const StageLaunch p) {
+  extern __shared__ __align__(128) unsigned char stream_smem[];
+  const StreamLayout Ls(SC);
+  unsigned long long* full =
+      reinterpret_cast<unsigned long long*>(stream_smem + Ls.bars);
+  unsigned long long* ready = full + kStreamStages;
+  volatile int* abort_flag =
+      reinterpret_cast<volatile int*>(ready + kStreamStages);
+  StreamLoaderState& loader =
+      *reinterpret_cast<StreamLoaderState*>(stream_smem + Ls.loader);
+  double2* U = reinterpret_cast<double2*>(stream_smem + Ls.uring);
+  double2* X = reinterpret_cast<double2*>(stream_smem + Ls.xring);
+  double2* A = reinterpret_cast<double2*>(stream_smem + Ls.aring);
+  double2* PS = reinterpret_cast<double2*>(stream_smem + Ls.pring);
+  double2* QE = reinterpret_cast<double2*>(stream_smem + Ls.qring);
+  double* CF = reinterpret_cast<double*>(stream_smem + Ls.coef);
+  double* xw = reinterpret_cast<double*>(stream_smem + Ls.xw);
+  double* tw = reinterpret_cast<double*>(stream_smem + Ls.tw);
+  double2* xch = reinterpret_cast<double2*>(stream_smem + Ls.xch);
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < kStreamStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&ready[s], kStreamTThreads);
+    }
+    *abort_flag = 0;
+    fence_mbarrier_init();
+  }
+  __syncthreads();
+  if (tid < kStreamTThreads) {
+    stream_transform<DISC, SC>(p, full, ready, abort_flag, U, X, PS, QE, CF,
+                               xw, tw, tid);
+  } else {
+    stream_stencil<DISC, SC>(p, full, ready, abort_flag, loader, U, X, A, PS,
+                             QE, CF, xch, tid - kStreamTThreads);
+  }
+}
+
+// Teukolsky row coefficients of one solve (m = 1 for entries 4, 6, 8).
+__global__ void coefficient_table_kernel(const InstanceDesc* instance,
+                                         const int nr, double* out) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < nr) row_coefficients(*instance, 1, r, out + r * kCoefCount);
+}

@@ -404,6 +404,8 @@ def _load() -> ctypes.CDLL:
         "teuk_b200_batch_set_stream": ([P, P], I),
         "teuk_b200_batch_synchronize": ([P], I),
         "teuk_b200_batch_launches_per_step": ([P, ctypes.POINTER(I)], I),
+        "teuk_b200_batch_stage_kernels": ([P, ctypes.POINTER(I),
+                                           ctypes.POINTER(I)], I),
         "teuk_b200_parse_run_config": ([ctypes.c_char_p,
                                         ctypes.POINTER(ctypes.c_char_p), I,
                                         ctypes.POINTER(RunConfig)], I),
@@ -721,6 +723,15 @@ class Batch:
         _check(_lib.teuk_b200_batch_launches_per_step(self._handle,
                                                       ctypes.byref(n)))
         return n.value
+
+    def stage_kernels(self) -> tuple[int, int]:
+        """(launch groups on the streaming kernel, groups on the tile
+        kernel)."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        _check(_lib.teuk_b200_batch_stage_kernels(self._handle,
+                                                  ctypes.byref(a),
+                                                  ctypes.byref(b)))
+        return a.value, b.value
 
 
 class Server:
