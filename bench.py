@@ -153,12 +153,18 @@ def measured_hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def recorded_traffic(algorithmic_bytes_per_launch: float):
-    """DRAM bytes per stage launch from the committed ncu summary, scaled
-    to this launch by the units processed."""
-    path = REPO / "profiles" / "stage_kernel_traffic.json"
+def recorded_traffic(kernel: str, algorithmic_bytes_per_launch: float):
+    """DRAM bytes per stage launch from the committed ncu summary of
+    `kernel` (key=value lines: dram_bytes_per_launch,
+    algorithmic_bytes_per_launch of the captured case), scaled to this
+    launch by the units processed."""
+    path = REPO / "profiles" / f"{kernel}_kerr_ringdown16_traffic.txt"
     try:
-        data = json.loads(path.read_text())
+        data = {}
+        for line in path.read_text().splitlines():
+            if "=" in line and not line.startswith("#"):
+                k, v = line.split("=", 1)
+                data[k.strip()] = float(v)
         per_unit = data["dram_bytes_per_launch"] / data["algorithmic_bytes_per_launch"]
         return per_unit * algorithmic_bytes_per_launch
     except Exception:
@@ -437,7 +443,9 @@ def b200_arm(args):
     algorithmic_per_launch = bytes_per_step / launches_per_step
     achieved = algorithmic_per_launch / per_launch_s / 1e9
     peak, peak_kind = measured_hbm_peak()
-    traffic = recorded_traffic(algorithmic_per_launch)
+    streaming, _ = batch.stage_kernels()
+    kernel = "stream_stage_kernel" if streaming else "stage_kernel"
+    traffic = recorded_traffic(kernel, algorithmic_per_launch)
 
     # end-to-end through the C ABI with host buffers
     e2e = None
@@ -494,7 +502,7 @@ def b200_arm(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic,
-                         "kernel": "stage_kernel<D10-5, free-damped>",
+                         "kernel": f"{kernel}<D10-5, free-damped>",
                          "peak_source": f"{peak_kind} hbm_gbs",
                          "algorithmic_bytes_per_launch": algorithmic_per_launch},
             "cpu_baseline": cpu,

@@ -13,12 +13,12 @@
 //                 and the RK update of every output row, two rows and one
 //                 ell column per thread, split into a psi role and a P/Q
 //                 role that exchange partial sums through shared memory.
-//                 Their first thread is also the loader: it issues the
-//                 cp.async.bulk copies of each 16-row chunk of the stage
-//                 inputs and of the Teukolsky row coefficients into a
-//                 4-stage ring (completion through mbarrier transaction
-//                 counts) as soon as no later work of the strip reads the
-//                 rows a stage holds.
+//                 They publish how many chunks no later work reads.
+// The first transform thread is also the loader: it issues the
+// cp.async.bulk copies of each 16-row chunk of the stage inputs and of the
+// Teukolsky row coefficients into a 4-stage ring (completion through
+// mbarrier transaction counts) as soon as the stencil warps hand a stage
+// back, at chunk boundaries and while it waits for data.
 // The roles run concurrently on different chunks: the copies of the next
 // chunks, the transforms of the current one and the stencils of the rows it
 // completes overlap.  Every halo row is loaded and transformed once per
@@ -159,6 +159,9 @@ struct StripGeom {
 // Loader state, kept in shared memory (only its one thread touches it).
 struct StreamLoaderState {
   StripGeom sg;  // geometry of `strip`
+  const double2* src_u;  // stage input arrays of this launch
+  const double2* src_x;
+  const double2* src_a;
   int strip;     // strip of the next chunk to load (>= strip_count: done)
   int c;         // its chunk index within the strip
   int g;         // its global chunk index
@@ -173,7 +176,7 @@ struct StreamLayout {
   __host__ __device__ explicit StreamLayout(const int sc) {
     size_t o = 0;
     bars = o;
-    o += 128;  // 2 x stages mbarriers + abort flag
+    o += 128;  // 2 x stages mbarriers, abort flag, released-chunk count
     loader = o;
     o += (sizeof(StreamLoaderState) + 127) / 128 * 128;
     const size_t ring = static_cast<size_t>(kStreamRing) * kRowMax * 16;
@@ -302,12 +305,69 @@ __device__ __forceinline__ void ring_window(double2 (&w)[N],
   }
 }
 
+// Closure rows straight from a ring column: the first K rows (r < BR) or
+// the last K rows (r >= nr - BR) of the radial line, K = SPECIAL + P (the
+// widest closure stencil).  Two partial sums halve the dependency chain;
+// table entries beyond a row's stencil are zero.
+template <int DISC>
+__device__ __forceinline__ double2 edge_derivative(const double2* column,
+                                                   const int r, const int nr,
+                                                   const int shift,
+                                                   const int stride) {
+  using T = DiscTraits<DISC>;
+  double2 a0 = make_double2(0.0, 0.0), a1 = a0;
+  if (r < T::BR) {
+#pragma unroll
+    for (int c = 0; c < T::W; ++c) {
+      const double2 v = column[ring_row(c, shift) * stride];
+      if (c & 1) a1 = cfma(c_sbp.left[DISC][r][c], v, a1);
+      else a0 = cfma(c_sbp.left[DISC][r][c], v, a0);
+    }
+  } else {
+    const int rr = nr - 1 - r;
+#pragma unroll
+    for (int c = 0; c < T::W; ++c) {
+      const double2 v = column[ring_row(nr - 1 - c, shift) * stride];
+      if (c & 1) a1 = cfma(-c_sbp.left[DISC][rr][c], v, a1);
+      else a0 = cfma(-c_sbp.left[DISC][rr][c], v, a0);
+    }
+  }
+  return cadd(a0, a1);
+}
+
+template <int DISC>
+__device__ __forceinline__ double2 edge_dissipation(const double2* column,
+                                                    const int r, const int nr,
+                                                    const int shift,
+                                                    const int stride) {
+  using T = DiscTraits<DISC>;
+  constexpr int K = T::SPECIAL + T::P;
+  double2 a0 = make_double2(0.0, 0.0), a1 = a0;
+  const bool left = r < T::SPECIAL;
+  const int rr = left ? r : nr - 1 - r;
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    const double2 v = column[ring_row(left ? j : nr - 1 - j, shift) * stride];
+    if (j & 1) a1 = cfma(c_sbp.diss_left[DISC][rr][j], v, a1);
+    else a0 = cfma(c_sbp.diss_left[DISC][rr][j], v, a0);
+  }
+  return cadd(a0, a1);
+}
+
 // ------------------------------------------------------------- loader
 // Issues the bulk copies of the CTA's chunk sequence (strips blockIdx.x,
 // blockIdx.x + gridDim.x, ...; chunks of kStreamChunk rows each), one
 // chunk per free ring stage.  Run by one thread.
 template <int H, int HD>
 __device__ void loader_init(const StageLaunch& p, StreamLoaderState& L) {
+  L.src_x = nullptr;
+  L.src_a = nullptr;
+  switch (p.stage) {
+    case kStage2: L.src_u = p.y; L.src_x = p.kA; break;
+    case kStage3: L.src_u = p.kB; L.src_x = p.y; L.src_a = p.acc; break;
+    case kStage4: L.src_u = p.kA; L.src_a = p.acc; break;
+    default: L.src_u = p.y; break;  // stage 1 and the RHS-only evaluation
+  }
   L.strip = blockIdx.x;
   L.c = 0;
   L.g = 0;
@@ -319,45 +379,44 @@ __device__ void loader_init(const StageLaunch& p, StreamLoaderState& L) {
 // so far.  A strip with another row stride starts only on an empty ring
 // (its rows would overlap the live stages' rows otherwise).
 template <int H, int HD>
-__device__ void loader_pump(const StageLaunch& p, StreamLoaderState& L,
+__device__ void loader_pump(const StageLaunch& p, StreamLoaderState& state,
                             unsigned long long* full, double2* U, double2* X,
                             double2* A, double* CF, const int released) {
-  const double2* src_u;
-  const double2* src_x = nullptr;
-  const double2* src_a = nullptr;
-  switch (p.stage) {
-    case kStage2: src_u = p.y; src_x = p.kA; break;
-    case kStage3: src_u = p.kB; src_x = p.y; src_a = p.acc; break;
-    case kStage4: src_u = p.kA; src_a = p.acc; break;
-    default: src_u = p.y; break;  // stage 1 and the RHS-only evaluation
+  if (state.strip >= p.strip_count || state.g >= released + kStreamStages) {
+    return;
   }
+  // Every reader of a released stage finished before the release was
+  // published; order those accesses before the copies' writes.
+  __threadfence_block();
+  fence_proxy_async_smem();
+  StreamLoaderState L = state;
   while (L.strip < p.strip_count && L.g < released + kStreamStages) {
     const StripGeom& sg = L.sg;
     if (L.c == 0 && L.prev_rs >= 0 && sg.rs != L.prev_rs && released < L.g) {
-      return;
+      break;
     }
     const int s = L.g % kStreamStages;
     const int a0 = sg.s0 + L.c * kStreamChunk;
     const int a1 = min(sg.s1, a0 + kStreamChunk);
     const unsigned row_bytes = static_cast<unsigned>(sg.rs) * 16u;
     const unsigned bytes_u = static_cast<unsigned>(a1 - a0) * row_bytes;
-    const unsigned bytes_x = src_x != nullptr ? bytes_u : 0u;
+    const unsigned bytes_x = L.src_x != nullptr ? bytes_u : 0u;
     const int o0 = max(a0, sg.r0), o1 = min(a1, sg.r1);
-    const unsigned bytes_a = (src_a != nullptr && o1 > o0)
+    const unsigned bytes_a = (L.src_a != nullptr && o1 > o0)
                                  ? static_cast<unsigned>(o1 - o0) * row_bytes
                                  : 0u;
     const unsigned bytes_c =
         static_cast<unsigned>(a1 - a0) * kCoefCount * sizeof(double);
-    // earlier generic-proxy accesses of the stage come before the copies
-    fence_proxy_async_smem();
     mbar_arrive_expect_tx(&full[s], bytes_u + bytes_x + bytes_a + bytes_c);
     const long long gsrc = sg.seg_offset + static_cast<long long>(a0) * sg.rs;
     const int ra0 = ring_row(a0, sg.shift);
-    bulk_copy_g2s(U + ra0 * sg.rs, src_u + gsrc, bytes_u, &full[s]);
-    if (bytes_x != 0u) bulk_copy_g2s(X + ra0 * sg.rs, src_x + gsrc, bytes_x, &full[s]);
+    bulk_copy_g2s(U + ra0 * sg.rs, L.src_u + gsrc, bytes_u, &full[s]);
+    if (bytes_x != 0u) {
+      bulk_copy_g2s(X + ra0 * sg.rs, L.src_x + gsrc, bytes_x, &full[s]);
+    }
     if (bytes_a != 0u) {
       bulk_copy_g2s(A + ring_row(o0, sg.shift) * sg.rs,
-                    src_a + sg.seg_offset + static_cast<long long>(o0) * sg.rs,
+                    L.src_a + sg.seg_offset + static_cast<long long>(o0) * sg.rs,
                     bytes_a, &full[s]);
     }
     bulk_copy_g2s(CF + ra0 * kCoefCount,
@@ -372,6 +431,7 @@ __device__ void loader_pump(const StageLaunch& p, StreamLoaderState& L,
       if (L.strip < p.strip_count) L.sg = strip_geom<H, HD>(p, L.strip, L.g);
     }
   }
+  state = L;
 }
 
 // After an abort: copies still in flight land before the CTA exits.
@@ -501,9 +561,11 @@ template <int DISC, int SC>
 __device__ void stream_transform(const StageLaunch& p,
                                  unsigned long long* full,
                                  unsigned long long* ready,
-                                 volatile int* abort_flag, double2* U,
-                                 const double2* X, double2* PS, double2* QE,
-                                 const double* CF, double* xw_all,
+                                 volatile int* abort_flag,
+                                 volatile int* released,
+                                 StreamLoaderState& loader, double2* U,
+                                 double2* X, double2* A, double2* PS,
+                                 double2* QE, double* CF, double* xw_all,
                                  double* tw_all, const int tt) {
   using T = DiscTraits<DISC>;
   constexpr int P = T::P, HD = T::HALF;
@@ -516,6 +578,10 @@ __device__ void stream_transform(const StageLaunch& p,
   // zero the nodal staging once: columns beyond a solve's nodes stay zero
   for (int i = tt; i < kStreamBlocks * 8 * kStreamTs; i += kStreamTThreads) {
     tw_all[i] = 0.0;
+  }
+  if (tt == 0) {
+    loader_init<H, HD>(p, loader);
+    loader_pump<H, HD>(p, loader, full, U, X, A, CF, 0);
   }
   int g = 0;
   for (int strip = blockIdx.x; strip < p.strip_count; strip += gridDim.x) {
@@ -556,11 +622,33 @@ __device__ void stream_transform(const StageLaunch& p,
     int pd = sg.t0;  // psi_t rows done
     for (int c = 0; c < sg.chunks; ++c, ++g) {
       const int s = g % kStreamStages;
-      // every transform thread waits; all of them leave together on abort
-      const bool landed =
-          stream_wait(&full[s], static_cast<unsigned>(g / kStreamStages) & 1u,
-                      abort_flag, p.error, 3);
-      if (!named_sync_and(1, kStreamTThreads, landed)) return;
+      const unsigned parity = static_cast<unsigned>(g / kStreamStages) & 1u;
+      // every transform thread waits; all of them leave together on abort.
+      // The loader thread issues the copies of released stages meanwhile.
+      bool landed;
+      if (tt == 0) {
+        landed = false;
+        const unsigned long long t0 = global_ns();
+        while (true) {
+          loader_pump<H, HD>(p, loader, full, U, X, A, CF, *released);
+          if (mbar_try_wait(&full[s], parity)) {
+            landed = true;
+            break;
+          }
+          if (*abort_flag != 0) break;
+          if (global_ns() - t0 > kStreamWaitNs) {
+            *abort_flag = 1;
+            if (p.error != nullptr) atomicExch(p.error, 3);
+            break;
+          }
+        }
+      } else {
+        landed = stream_wait(&full[s], parity, abort_flag, p.error, 3);
+      }
+      if (!named_sync_and(1, kStreamTThreads, landed)) {
+        if (tt == 0) loader_drain(loader, full);
+        return;
+      }
       const int a0 = sg.s0 + c * kStreamChunk;
       const int a1 = min(sg.s1, a0 + kStreamChunk);
       // stage input u = y + dt/2 k, in place
@@ -670,13 +758,12 @@ __device__ __forceinline__ void stream_rk_update(
 
 template <int DISC, int SC>
 __device__ void stream_stencil(const StageLaunch& p,
-                               unsigned long long* full,
                                unsigned long long* ready,
                                volatile int* abort_flag,
-                               StreamLoaderState& loader, double2* U,
-                               double2* X, double2* A, const double2* PS,
-                               const double2* QE, double* CF, double2* xch,
-                               const int st) {
+                               volatile int* released, const double2* U,
+                               const double2* X, const double2* A,
+                               const double2* PS, const double2* QE,
+                               const double* CF, double2* xch, const int st) {
   using T = DiscTraits<DISC>;
   constexpr int P = T::P, HD = T::HALF;
   constexpr int H = SC ? (P > 2 * HD ? P : 2 * HD) : P;
@@ -686,10 +773,6 @@ __device__ void stream_stencil(const StageLaunch& p,
   const int jr = st % HALF_THREADS;
   const int rb = jr / kStreamNep;
   const int l = jr % kStreamNep;
-  if (st == 0) {
-    loader_init<H, HD>(p, loader);
-    loader_pump<H, HD>(p, loader, full, U, X, A, CF, 0);
-  }
   int g = 0;
   for (int strip = blockIdx.x; strip < p.strip_count; strip += gridDim.x) {
     const int g0 = g;
@@ -712,10 +795,7 @@ __device__ void stream_stencil(const StageLaunch& p,
       const bool done =
           stream_wait(&ready[s], static_cast<unsigned>(g / kStreamStages) & 1u,
                       abort_flag, p.error, 4);
-      if (!named_sync_and(2, kStreamSThreads, done)) {
-        if (st == 0) loader_drain(loader, full);
-        return;
-      }
+      if (!named_sync_and(2, kStreamSThreads, done)) return;
       const int u_end = min(sg.s1, sg.s0 + (c + 1) * kStreamChunk);
       int lim = min(sg.r1, computable_end(u_end, nr, T::P, T::SPECIAL + T::P,
                                           T::SPECIAL));
@@ -773,28 +853,35 @@ __device__ void stream_stencil(const StageLaunch& p,
           } else {
             const double2* cpsi = U + 2 * ne + l;
             const double2* cpt = PS + l;
-            const int shift = sg.shift;
-            auto at_psi = [=](const int q) {
-              return cpsi[ring_row(q, shift) * rs];
-            };
-            auto at_pt = [=](const int q) {
-              return cpt[ring_row(q, shift) * kStreamNep];
-            };
 #pragma unroll
             for (int i = 0; i < RB; ++i) {
               if (i >= cnt) break;
               const int r = ra + i;
-              const double* cf = CF + ring_row(r, sg.shift) * kCoefCount;
-              const double2 psi = at_psi(r);
-              const double2 dpsi =
-                  cscale(inv_h, ring_derivative<DISC>(at_psi, r, nr));
-              ky[i] = cadd(cscale(damping, dpsi),
-                           cscale(inv_h, ring_derivative<DISC>(at_pt, r, nr)));
-              kpsi[i] = at_pt(r);
-              if (dissipate) {
-                kpsi[i] = cfma(diss_scale, ring_dissipation<DISC>(at_psi, r, nr),
-                               kpsi[i]);
+              const int rr = ring_row(r, sg.shift);
+              const double* cf = CF + rr * kCoefCount;
+              const double2 psi = cpsi[rr * rs];
+              double2 dpsi, dpt, diss = make_double2(0.0, 0.0);
+              if (r < T::BR || r + T::BR >= nr) {
+                dpsi = edge_derivative<DISC>(cpsi, r, nr, sg.shift, rs);
+                if (dissipate) {
+                  diss = edge_dissipation<DISC>(cpsi, r, nr, sg.shift, rs);
+                }
+                dpt = edge_derivative<DISC>(cpt, r, nr, sg.shift, kStreamNep);
+              } else {
+                {
+                  double2 w[1 + 2 * P];
+                  ring_window(w, cpsi, r - P, sg.shift, rs);
+                  dpsi = window_derivative<DISC, 1, P>(w, 0);
+                  if (dissipate) diss = window_dissipation<DISC, 1, P>(w, 0);
+                }
+                double2 wt[1 + 2 * HD];
+                ring_window(wt, cpt, r - HD, sg.shift, kStreamNep);
+                dpt = window_derivative<DISC, 1, HD>(wt, 0);
               }
+              ky[i] = cadd(cscale(damping, cscale(inv_h, dpsi)),
+                           cscale(inv_h, dpt));
+              kpsi[i] = cpt[rr * kStreamNep];
+              if (dissipate) kpsi[i] = cfma(diss_scale, diss, kpsi[i]);
               kx[i] = cadd(cmul(make_double2(cf[7], mm * cf[8]), psi),
                            cscale(lambda, psi));
             }
@@ -849,38 +936,48 @@ __device__ void stream_stencil(const StageLaunch& p,
             const double2* cq = U + ne + l;
             const double2* cp = U + l;
             const double2* cqe = QE + l;
-            const int shift = sg.shift;
-            auto at_q = [=](const int q) { return cq[ring_row(q, shift) * rs]; };
-            auto at_p = [=](const int q) { return cp[ring_row(q, shift) * rs]; };
-            auto at_qe = [=](const int q) {
-              return cqe[ring_row(q, shift) * kStreamNep];
-            };
 #pragma unroll
             for (int i = 0; i < RB; ++i) {
               if (i >= cnt) break;
               const int r = ra + i;
-              const double* cf = CF + ring_row(r, sg.shift) * kCoefCount;
-              const double2 Q = at_q(r);
-              ky[i] = cscale(-damping, Q);
-              if (dissipate) {
-                ky[i] = cfma(diss_scale, ring_dissipation<DISC>(at_q, r, nr),
-                             ky[i]);
-              }
-              if (SC) {
-                const double2 dq =
-                    cscale(inv_h, ring_derivative<DISC>(at_qe, r, nr));
-                kx[i] = cadd(cscale(cf[2], dq),
-                             cmul(make_double2(cf[5], mm * cf[6]), at_qe(r)));
+              const int rr = ring_row(r, sg.shift);
+              const double* cf = CF + rr * kCoefCount;
+              const double2 Q = cq[rr * rs];
+              const bool edge = r < T::BR || r + T::BR >= nr;
+              double2 dq, qp = Q, dissq = make_double2(0.0, 0.0),
+                              dissp = make_double2(0.0, 0.0);
+              if (edge) {
+                if (dissipate) {
+                  dissq = edge_dissipation<DISC>(cq, r, nr, sg.shift, rs);
+                  dissp = edge_dissipation<DISC>(cp, r, nr, sg.shift, rs);
+                }
+                if (SC) {
+                  dq = edge_derivative<DISC>(cqe, r, nr, sg.shift, kStreamNep);
+                  qp = cqe[rr * kStreamNep];
+                } else {
+                  dq = edge_derivative<DISC>(cq, r, nr, sg.shift, rs);
+                }
               } else {
-                const double2 dq =
-                    cscale(inv_h, ring_derivative<DISC>(at_q, r, nr));
-                kx[i] = cadd(cscale(cf[2], dq),
-                             cmul(make_double2(cf[5], mm * cf[6]), Q));
+                double2 w[1 + 2 * P];
+                ring_window(w, cq, r - P, sg.shift, rs);
+                if (dissipate) dissq = window_dissipation<DISC, 1, P>(w, 0);
+                if (!SC) dq = window_derivative<DISC, 1, P>(w, 0);
+                if (dissipate) {
+                  ring_window(w, cp, r - P, sg.shift, rs);
+                  dissp = window_dissipation<DISC, 1, P>(w, 0);
+                }
+                if (SC) {
+                  double2 wq[1 + 2 * HD];
+                  ring_window(wq, cqe, r - HD, sg.shift, kStreamNep);
+                  dq = window_derivative<DISC, 1, HD>(wq, 0);
+                  qp = wq[HD];
+                }
               }
-              if (dissipate) {
-                kx[i] = cfma(diss_scale, ring_dissipation<DISC>(at_p, r, nr),
-                             kx[i]);
-              }
+              ky[i] = cscale(-damping, Q);
+              if (dissipate) ky[i] = cfma(diss_scale, dissq, ky[i]);
+              kx[i] = cadd(cscale(cf[2], cscale(inv_h, dq)),
+                           cmul(make_double2(cf[5], mm * cf[6]), qp));
+              if (dissipate) kx[i] = cfma(diss_scale, dissp, kx[i]);
             }
           }
         }
@@ -906,12 +1003,13 @@ __device__ void stream_stencil(const StageLaunch& p,
       } else {
         bound = min(out_done - H, nr - T::SPECIAL - T::P);
       }
-      if (st == 0) {
-        while (rel <= g &&
-               min(sg.s1, sg.s0 + (rel - g0 + 1) * kStreamChunk) <= bound) {
-          ++rel;
-        }
-        loader_pump<H, HD>(p, loader, full, U, X, A, CF, rel);
+      while (rel <= g &&
+             min(sg.s1, sg.s0 + (rel - g0 + 1) * kStreamChunk) <= bound) {
+        ++rel;
+      }
+      if (st == 0 && rel > *released) {
+        __threadfence_block();
+        *released = rel;
       }
     }
   }
@@ -927,6 +1025,7 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
   unsigned long long* ready = full + kStreamStages;
   volatile int* abort_flag =
       reinterpret_cast<volatile int*>(ready + kStreamStages);
+  volatile int* released = abort_flag + 1;  // chunks the stencils are done with
   StreamLoaderState& loader =
       *reinterpret_cast<StreamLoaderState*>(stream_smem + Ls.loader);
   double2* U = reinterpret_cast<double2*>(stream_smem + Ls.uring);
@@ -945,15 +1044,16 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
       mbar_init(&ready[s], kStreamTThreads);
     }
     *abort_flag = 0;
+    *released = 0;
     fence_mbarrier_init();
   }
   __syncthreads();
   if (tid < kStreamTThreads) {
-    stream_transform<DISC, SC>(p, full, ready, abort_flag, U, X, PS, QE, CF,
-                               xw, tw, tid);
+    stream_transform<DISC, SC>(p, full, ready, abort_flag, released, loader,
+                               U, X, A, PS, QE, CF, xw, tw, tid);
   } else {
-    stream_stencil<DISC, SC>(p, full, ready, abort_flag, loader, U, X, A, PS,
-                             QE, CF, xch, tid - kStreamTThreads);
+    stream_stencil<DISC, SC>(p, ready, abort_flag, released, U, X, A, PS, QE,
+                             CF, xch, tid - kStreamTThreads);
   }
 }
 
