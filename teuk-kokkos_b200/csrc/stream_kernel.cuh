@@ -10,10 +10,9 @@
 //                 per 4-row block (each takes half of the node tiles of the
 //                 synthesis and one ell tile of the analysis);
 //   warps 8-15    stencil warps: SBP derivatives, dissipation, RHS assembly
-//                 and the RK update of every output row, two rows and one
-//                 ell column per thread, split into a psi role and a P/Q
-//                 role that exchange partial sums through shared memory.
-//                 They publish how many chunks no later work reads.
+//                 and the RK update of every output row, one (row, ell)
+//                 point and all three fields per thread.  They publish how
+//                 many chunks no later work reads.
 // The first transform thread is also the loader: it issues the
 // cp.async.bulk copies of each 16-row chunk of the stage inputs and of the
 // Teukolsky row coefficients into a 4-stage ring (completion through
@@ -38,15 +37,14 @@ constexpr int kStreamSWarps = 8;
 constexpr int kStreamThreads = 32 * (kStreamTWarps + kStreamSWarps);
 constexpr int kStreamTThreads = 32 * kStreamTWarps;
 constexpr int kStreamSThreads = 32 * kStreamSWarps;
-constexpr int kStreamRB = 2;     // rows per stencil thread
 constexpr int kStreamBlocks = 4;  // 4-row transform blocks per 16 rows
 constexpr unsigned long long kStreamWaitNs = 2000000000ull;
 static_assert(kStreamNep == kStreamMaxEll, "ell lanes");
 static_assert(kStreamMaxTheta == kStreamMaxNodes, "node tiles");
 static_assert(kStripMinRows >= 2 * 17, "strip edges clear of closures");
 static_assert(kCoefRecord == kCoefCount, "coefficient record");
-static_assert(kStreamSThreads == 2 * kStreamNep * kStreamChunk / kStreamRB,
-              "one stencil thread per (role, row pair, ell)");
+static_assert(kStreamSThreads == kStreamNep * kStreamChunk,
+              "one stencil thread per (row, ell) of a chunk");
 static_assert(kStreamTWarps == 2 * kStreamBlocks, "two warps per block");
 constexpr int kStreamXs = 20;  // padded staging strides (bank-conflict free)
 constexpr int kStreamTs = 36;
@@ -171,7 +169,7 @@ struct StreamLoaderState {
 // Shared-memory carve-up (bytes), identical on host and device.
 struct StreamLayout {
   static constexpr int kRowMax = 3 * kStreamNep;  // complex per ring row
-  size_t bars, loader, uring, xring, aring, pring, qring, coef, xw, tw, xch,
+  size_t bars, loader, uring, xring, aring, pring, qring, coef, xw, tw,
       total;
   __host__ __device__ explicit StreamLayout(const int sc) {
     size_t o = 0;
@@ -196,8 +194,6 @@ struct StreamLayout {
     o += static_cast<size_t>(kStreamBlocks) * 16 * kStreamXs * 8;
     tw = o;
     o += static_cast<size_t>(kStreamBlocks) * 8 * kStreamTs * 8;
-    xch = o;
-    o += static_cast<size_t>(kStreamSThreads / 2) * 2 * kStreamRB * 16;
     total = o;
   }
 };
@@ -723,39 +719,32 @@ __device__ void stream_transform(const StageLaunch& p,
 }
 
 // ------------------------------------------------------------- stencils
-// RK update of one field column for `cnt` rows from the stage slope k.
+// RK update of field f of one row from the stage slope k (global stores).
 __device__ __forceinline__ void stream_rk_update(
     const StageLaunch& p, const StripGeom& sg, const double2* X,
-    const double2* A, const int ra, const int cnt, const int f, const int l,
-    const double2 (&k)[kStreamRB], const double dt, const double dt6) {
-  const long long g0 =
-      sg.seg_offset + static_cast<long long>(ra) * sg.rs + f * sg.ne + l;
-#pragma unroll
-  for (int i = 0; i < kStreamRB; ++i) {
-    if (i >= cnt) break;
-    const long long gi = g0 + static_cast<long long>(i) * sg.rs;
-    const int ri = ring_row(ra + i, sg.shift) * sg.rs + f * sg.ne + l;
-    switch (p.stage) {
-      case kStage2:  // X = k1
-        p.kB[gi] = k[i];
-        p.acc[gi] = cfma(2.0, k[i], X[ri]);
-        break;
-      case kStage3: {  // X = y, A = k1 + 2 k2
-        const double2 y0 = X[ri];
-        p.acc[gi] = cfma(dt6, cfma(2.0, k[i], A[ri]), y0);
-        p.kA[gi] = cfma(dt, k[i], y0);
-        break;
-      }
-      case kStage4:  // A = y + dt/6 (k1 + 2 k2 + 2 k3)
-        p.y[gi] = cfma(dt6, k[i], A[ri]);
-        break;
-      default:  // stage 1 and the RHS-only evaluation
-        p.kA[gi] = k[i];
-        break;
+    const double2* A, const long long gi, const int ri, const double2 k,
+    const double dt, const double dt6) {
+  switch (p.stage) {
+    case kStage2:  // X = k1
+      p.kB[gi] = k;
+      p.acc[gi] = cfma(2.0, k, X[ri]);
+      break;
+    case kStage3: {  // X = y, A = k1 + 2 k2
+      const double2 y0 = X[ri];
+      p.acc[gi] = cfma(dt6, cfma(2.0, k, A[ri]), y0);
+      p.kA[gi] = cfma(dt, k, y0);
+      break;
     }
+    case kStage4:  // A = y + dt/6 (k1 + 2 k2 + 2 k3)
+      p.y[gi] = cfma(dt6, k, A[ri]);
+      break;
+    default:  // stage 1 and the RHS-only evaluation
+      p.kA[gi] = k;
+      break;
   }
 }
 
+// One thread per (output row, ell): all three fields, no exchange.
 template <int DISC, int SC>
 __device__ void stream_stencil(const StageLaunch& p,
                                unsigned long long* ready,
@@ -763,17 +752,14 @@ __device__ void stream_stencil(const StageLaunch& p,
                                volatile int* released, const double2* U,
                                const double2* X, const double2* A,
                                const double2* PS, const double2* QE,
-                               const double* CF, double2* xch, const int st) {
+                               const double* CF, const int st) {
   using T = DiscTraits<DISC>;
   constexpr int P = T::P, HD = T::HALF;
   constexpr int H = SC ? (P > 2 * HD ? P : 2 * HD) : P;
-  constexpr int RB = kStreamRB;
-  constexpr int HALF_THREADS = kStreamSThreads / 2;
-  const int role = st / HALF_THREADS;  // 0: psi, 1: P and Q
-  const int jr = st % HALF_THREADS;
-  const int rb = jr / kStreamNep;
-  const int l = jr % kStreamNep;
+  const int rrow = st / kStreamNep;  // row within a 16-row block
+  const int l = st % kStreamNep;
   int g = 0;
+  int published = 0;  // chunks handed back so far
   for (int strip = blockIdx.x; strip < p.strip_count; strip += gridDim.x) {
     const int g0 = g;
     const StripGeom sg = strip_geom<H, HD>(p, strip, g0);
@@ -788,6 +774,11 @@ __device__ void stream_stencil(const StageLaunch& p,
     const int ell = (l < ne) ? (p.segments[sg.segment].ell_min + l) : 0;
     const double lambda = -static_cast<double>((ell - kSpinWeight) *
                                                (ell + kSpinWeight + 1));
+    const double2* cP = U + l;
+    const double2* cQ = U + ne + l;
+    const double2* cpsi = U + 2 * ne + l;
+    const double2* cpt = PS + l;
+    const double2* cqe = QE + l;
     int out_done = sg.r0;
     int rel = g0;  // next chunk of this strip to hand back
     for (int c = 0; c < sg.chunks; ++c, ++g) {
@@ -810,188 +801,89 @@ __device__ void stream_stencil(const StageLaunch& p,
         pe = min(sg.t1, u_end);
       }
       lim = min(lim, computable_end(pe, nr, T::HALF, T::W, T::BR));
-      for (int o = out_done; o < lim; o += kStreamChunk) {
-        const int ra = o + RB * rb;
-        const int cnt = min(RB, lim - ra);
-        const bool active = cnt > 0 && l < ne;
-        const bool interior =
-            cnt == RB && ra >= T::BR && ra + RB + T::BR <= nr;
-        double2 kx[RB], ky[RB];  // psi role: kP_a, kQ_a; P/Q role: kP, kQ
-        double2 kpsi[RB];
-#pragma unroll
-        for (int i = 0; i < RB; ++i) {
-          kx[i] = ky[i] = kpsi[i] = make_double2(0.0, 0.0);
-        }
-        if (active && role == 0) {
-          if (interior) {
-            {
-              double2 w[RB + 2 * P];
-              ring_window(w, U + 2 * ne + l, ra - P, sg.shift, rs);
-#pragma unroll
-              for (int i = 0; i < RB; ++i) {
-                const double* cf = CF + ring_row(ra + i, sg.shift) * kCoefCount;
-                const double2 dpsi =
-                    cscale(inv_h, window_derivative<DISC, RB, P>(w, i));
-                ky[i] = cscale(damping, dpsi);
-                if (dissipate) {
-                  kpsi[i] = cscale(diss_scale,
-                                   window_dissipation<DISC, RB, P>(w, i));
-                }
-                const double2 psi = w[i + P];
-                kx[i] = cadd(cmul(make_double2(cf[7], mm * cf[8]), psi),
-                             cscale(lambda, psi));
-              }
-            }
-            double2 wt[RB + 2 * HD];
-            ring_window(wt, PS + l, ra - HD, sg.shift, kStreamNep);
-#pragma unroll
-            for (int i = 0; i < RB; ++i) {
-              ky[i] = cadd(ky[i], cscale(inv_h,
-                                         window_derivative<DISC, RB, HD>(wt, i)));
-              kpsi[i] = cadd(kpsi[i], wt[i + HD]);
-            }
-          } else {
-            const double2* cpsi = U + 2 * ne + l;
-            const double2* cpt = PS + l;
-#pragma unroll
-            for (int i = 0; i < RB; ++i) {
-              if (i >= cnt) break;
-              const int r = ra + i;
-              const int rr = ring_row(r, sg.shift);
-              const double* cf = CF + rr * kCoefCount;
-              const double2 psi = cpsi[rr * rs];
-              double2 dpsi, dpt, diss = make_double2(0.0, 0.0);
-              if (r < T::BR || r + T::BR >= nr) {
-                dpsi = edge_derivative<DISC>(cpsi, r, nr, sg.shift, rs);
-                if (dissipate) {
-                  diss = edge_dissipation<DISC>(cpsi, r, nr, sg.shift, rs);
-                }
-                dpt = edge_derivative<DISC>(cpt, r, nr, sg.shift, kStreamNep);
-              } else {
-                {
-                  double2 w[1 + 2 * P];
-                  ring_window(w, cpsi, r - P, sg.shift, rs);
-                  dpsi = window_derivative<DISC, 1, P>(w, 0);
-                  if (dissipate) diss = window_dissipation<DISC, 1, P>(w, 0);
-                }
-                double2 wt[1 + 2 * HD];
-                ring_window(wt, cpt, r - HD, sg.shift, kStreamNep);
-                dpt = window_derivative<DISC, 1, HD>(wt, 0);
-              }
-              ky[i] = cadd(cscale(damping, cscale(inv_h, dpsi)),
-                           cscale(inv_h, dpt));
-              kpsi[i] = cpt[rr * kStreamNep];
-              if (dissipate) kpsi[i] = cfma(diss_scale, diss, kpsi[i]);
-              kx[i] = cadd(cmul(make_double2(cf[7], mm * cf[8]), psi),
-                           cscale(lambda, psi));
-            }
+      for (int r = out_done + rrow; r < lim; r += kStreamChunk) {
+        if (l >= ne) continue;
+        const int rr = ring_row(r, sg.shift);
+        const double* cf = CF + rr * kCoefCount;
+        double2 kP, kQ, kpsi;
+        if (r >= T::BR && r + T::BR < nr) {
+          {  // psi: D psi (constraint), dissipation, (c_psi + lambda) psi
+            double2 w[1 + 2 * P];
+            ring_window(w, cpsi, r - P, sg.shift, rs);
+            const double2 psi = w[P];
+            kQ = cscale(damping, cscale(inv_h, window_derivative<DISC, 1, P>(w, 0)));
+            kpsi = dissipate
+                       ? cscale(diss_scale, window_dissipation<DISC, 1, P>(w, 0))
+                       : make_double2(0.0, 0.0);
+            kP = cadd(cmul(make_double2(cf[7], mm * cf[8]), psi),
+                      cscale(lambda, psi));
           }
-          stream_rk_update(p, sg, X, A, ra, cnt, 2, l, kpsi, dt, dt6);
-#pragma unroll
-          for (int i = 0; i < RB; ++i) {
-            xch[(i * 2 + 0) * HALF_THREADS + jr] = kx[i];
-            xch[(i * 2 + 1) * HALF_THREADS + jr] = ky[i];
+          {  // psi_t: D psi_t into Q_t, psi_t itself
+            double2 w[1 + 2 * HD];
+            ring_window(w, cpt, r - HD, sg.shift, kStreamNep);
+            kQ = cadd(kQ, cscale(inv_h, window_derivative<DISC, 1, HD>(w, 0)));
+            kpsi = cadd(kpsi, w[HD]);
           }
-        } else if (active) {  // role 1: P and Q
-          if (interior) {
-            double2 w[RB + 2 * P];
-            ring_window(w, U + ne + l, ra - P, sg.shift, rs);
-#pragma unroll
-            for (int i = 0; i < RB; ++i) {
-              const double2 Q = w[i + P];
-              ky[i] = cscale(-damping, Q);
-              if (dissipate) {
-                ky[i] = cfma(diss_scale, window_dissipation<DISC, RB, P>(w, i),
-                             ky[i]);
-              }
-              if (!SC) {
-                const double* cf = CF + ring_row(ra + i, sg.shift) * kCoefCount;
-                const double2 dq =
-                    cscale(inv_h, window_derivative<DISC, RB, P>(w, i));
-                kx[i] = cadd(cscale(cf[2], dq),
-                             cmul(make_double2(cf[5], mm * cf[6]), Q));
-              }
-            }
-            if (SC) {
-              double2 wq[RB + 2 * HD];
-              ring_window(wq, QE + l, ra - HD, sg.shift, kStreamNep);
-#pragma unroll
-              for (int i = 0; i < RB; ++i) {
-                const double* cf = CF + ring_row(ra + i, sg.shift) * kCoefCount;
-                const double2 dq =
-                    cscale(inv_h, window_derivative<DISC, RB, HD>(wq, i));
-                kx[i] = cadd(cscale(cf[2], dq),
-                             cmul(make_double2(cf[5], mm * cf[6]), wq[i + HD]));
-              }
-            }
+          {  // Q: -gamma Q, dissipation; free-damped: H_R D Q + q Q
+            double2 w[1 + 2 * P];
+            ring_window(w, cQ, r - P, sg.shift, rs);
+            const double2 Q = w[P];
+            kQ = csub(kQ, cscale(damping, Q));
             if (dissipate) {
-              ring_window(w, U + l, ra - P, sg.shift, rs);
-#pragma unroll
-              for (int i = 0; i < RB; ++i) {
-                kx[i] = cfma(diss_scale, window_dissipation<DISC, RB, P>(w, i),
-                             kx[i]);
-              }
+              kQ = cfma(diss_scale, window_dissipation<DISC, 1, P>(w, 0), kQ);
             }
-          } else {
-            const double2* cq = U + ne + l;
-            const double2* cp = U + l;
-            const double2* cqe = QE + l;
-#pragma unroll
-            for (int i = 0; i < RB; ++i) {
-              if (i >= cnt) break;
-              const int r = ra + i;
-              const int rr = ring_row(r, sg.shift);
-              const double* cf = CF + rr * kCoefCount;
-              const double2 Q = cq[rr * rs];
-              const bool edge = r < T::BR || r + T::BR >= nr;
-              double2 dq, qp = Q, dissq = make_double2(0.0, 0.0),
-                              dissp = make_double2(0.0, 0.0);
-              if (edge) {
-                if (dissipate) {
-                  dissq = edge_dissipation<DISC>(cq, r, nr, sg.shift, rs);
-                  dissp = edge_dissipation<DISC>(cp, r, nr, sg.shift, rs);
-                }
-                if (SC) {
-                  dq = edge_derivative<DISC>(cqe, r, nr, sg.shift, kStreamNep);
-                  qp = cqe[rr * kStreamNep];
-                } else {
-                  dq = edge_derivative<DISC>(cq, r, nr, sg.shift, rs);
-                }
-              } else {
-                double2 w[1 + 2 * P];
-                ring_window(w, cq, r - P, sg.shift, rs);
-                if (dissipate) dissq = window_dissipation<DISC, 1, P>(w, 0);
-                if (!SC) dq = window_derivative<DISC, 1, P>(w, 0);
-                if (dissipate) {
-                  ring_window(w, cp, r - P, sg.shift, rs);
-                  dissp = window_dissipation<DISC, 1, P>(w, 0);
-                }
-                if (SC) {
-                  double2 wq[1 + 2 * HD];
-                  ring_window(wq, cqe, r - HD, sg.shift, kStreamNep);
-                  dq = window_derivative<DISC, 1, HD>(wq, 0);
-                  qp = wq[HD];
-                }
-              }
-              ky[i] = cscale(-damping, Q);
-              if (dissipate) ky[i] = cfma(diss_scale, dissq, ky[i]);
-              kx[i] = cadd(cscale(cf[2], cscale(inv_h, dq)),
-                           cmul(make_double2(cf[5], mm * cf[6]), qp));
-              if (dissipate) kx[i] = cfma(diss_scale, dissp, kx[i]);
+            if (!SC) {
+              const double2 dq =
+                  cscale(inv_h, window_derivative<DISC, 1, P>(w, 0));
+              kP = cadd(kP, cadd(cscale(cf[2], dq),
+                                 cmul(make_double2(cf[5], mm * cf[6]), Q)));
             }
           }
-        }
-        named_sync(2, kStreamSThreads);  // partial sums of the psi role
-        if (active && role == 1) {
-#pragma unroll
-          for (int i = 0; i < RB; ++i) {
-            kx[i] = cadd(xch[(i * 2 + 0) * HALF_THREADS + jr], kx[i]);
-            ky[i] = cadd(xch[(i * 2 + 1) * HALF_THREADS + jr], ky[i]);
+          if (SC) {  // stage-constrained effective Q = D psi
+            double2 w[1 + 2 * HD];
+            ring_window(w, cqe, r - HD, sg.shift, kStreamNep);
+            const double2 dq =
+                cscale(inv_h, window_derivative<DISC, 1, HD>(w, 0));
+            kP = cadd(kP, cadd(cscale(cf[2], dq),
+                               cmul(make_double2(cf[5], mm * cf[6]), w[HD])));
           }
-          stream_rk_update(p, sg, X, A, ra, cnt, 0, l, kx, dt, dt6);
-          stream_rk_update(p, sg, X, A, ra, cnt, 1, l, ky, dt, dt6);
+          if (dissipate) {  // P: dissipation only
+            double2 w[1 + 2 * P];
+            ring_window(w, cP, r - P, sg.shift, rs);
+            kP = cfma(diss_scale, window_dissipation<DISC, 1, P>(w, 0), kP);
+          }
+        } else {  // closure rows
+          const double2 psi = cpsi[rr * rs];
+          const double2 Q = cQ[rr * rs];
+          kQ = cadd(cscale(damping, cscale(inv_h, edge_derivative<DISC>(
+                                                      cpsi, r, nr, sg.shift, rs))),
+                    cscale(inv_h, edge_derivative<DISC>(cpt, r, nr, sg.shift,
+                                                        kStreamNep)));
+          kQ = csub(kQ, cscale(damping, Q));
+          kpsi = cpt[rr * kStreamNep];
+          kP = cadd(cmul(make_double2(cf[7], mm * cf[8]), psi),
+                    cscale(lambda, psi));
+          const double2 qp = SC ? cqe[rr * kStreamNep] : Q;
+          const double2 dq =
+              SC ? edge_derivative<DISC>(cqe, r, nr, sg.shift, kStreamNep)
+                 : edge_derivative<DISC>(cQ, r, nr, sg.shift, rs);
+          kP = cadd(kP, cadd(cscale(cf[2], cscale(inv_h, dq)),
+                             cmul(make_double2(cf[5], mm * cf[6]), qp)));
+          if (dissipate) {
+            kpsi = cfma(diss_scale,
+                        edge_dissipation<DISC>(cpsi, r, nr, sg.shift, rs), kpsi);
+            kQ = cfma(diss_scale,
+                      edge_dissipation<DISC>(cQ, r, nr, sg.shift, rs), kQ);
+            kP = cfma(diss_scale,
+                      edge_dissipation<DISC>(cP, r, nr, sg.shift, rs), kP);
+          }
         }
-        named_sync(2, kStreamSThreads);  // exchange buffer free again
+        const long long gi =
+            sg.seg_offset + static_cast<long long>(r) * rs + l;
+        const int ri = rr * rs + l;
+        stream_rk_update(p, sg, X, A, gi, ri, kP, dt, dt6);
+        stream_rk_update(p, sg, X, A, gi + ne, ri + ne, kQ, dt, dt6);
+        stream_rk_update(p, sg, X, A, gi + 2 * ne, ri + 2 * ne, kpsi, dt, dt6);
       }
       out_done = max(out_done, lim);
       // rows below `bound` are read by no later work of this strip
@@ -1007,9 +899,10 @@ __device__ void stream_stencil(const StageLaunch& p,
              min(sg.s1, sg.s0 + (rel - g0 + 1) * kStreamChunk) <= bound) {
         ++rel;
       }
-      if (st == 0 && rel > *released) {
-        __threadfence_block();
-        *released = rel;
+      if (rel > published) {  // the same decision in every stencil thread
+        named_sync(2, kStreamSThreads);  // every read of those rows is done
+        if (st == 0) *released = rel;
+        published = rel;
       }
     }
   }
@@ -1036,7 +929,6 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
   double* CF = reinterpret_cast<double*>(stream_smem + Ls.coef);
   double* xw = reinterpret_cast<double*>(stream_smem + Ls.xw);
   double* tw = reinterpret_cast<double*>(stream_smem + Ls.tw);
-  double2* xch = reinterpret_cast<double2*>(stream_smem + Ls.xch);
   const int tid = threadIdx.x;
   if (tid == 0) {
     for (int s = 0; s < kStreamStages; ++s) {
@@ -1053,7 +945,7 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
                                U, X, A, PS, QE, CF, xw, tw, tid);
   } else {
     stream_stencil<DISC, SC>(p, ready, abort_flag, released, U, X, A, PS, QE,
-                             CF, xch, tid - kStreamTThreads);
+                             CF, tid - kStreamTThreads);
   }
 }
 
