@@ -346,6 +346,7 @@ def reference_arm(args):
                                     warmup=args.warmup, steps=args.steps)
     meta = dict(meta)
     meta["solves_per_gpu"] = 1
+    meta["l2"] = "host run: one solve's band state, 6.3 MB per buffer"
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup,
