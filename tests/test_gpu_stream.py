@@ -32,6 +32,14 @@ LONG = {
     # Schwarzschild D4-2 (pointwise psi_t)
     "schw_d42_long": replace(CASES["schw_d84"], discretization=tb.D42,
                              radial_points=203, dissipation=0.01),
+    # D10-5 stage-constrained Kerr (effective-Q lag of 2 x 5 rows)
+    "kerr_d105_sc_long": replace(CASES["kerr_d105"], radial_points=280,
+                                 reduction=tb.STAGE_CONSTRAINED,
+                                 theta_nodes=21, ell_max_first=10,
+                                 ell_max_second=10),
+    # D8-4 free-damped Schwarzschild without dissipation, odd nr
+    "schw_d84_long": replace(CASES["schw_d84"], radial_points=331,
+                             dissipation=0.0),
 }
 
 

@@ -46,6 +46,16 @@ static_assert(kCoefRecord == kCoefCount, "coefficient record");
 static_assert(kStreamSThreads == kStreamNep * kStreamChunk,
               "one stencil thread per (row, ell) of a chunk");
 static_assert(kStreamTWarps == 2 * kStreamBlocks, "two warps per block");
+// Register split between the roles (setmaxnreg): the launch gives every
+// thread 128 registers; the transform warpgroups raise theirs to 160 (their
+// MMA fragments and accumulators stay in registers) and the stencil
+// warpgroups drop to 96.  256 x 160 + 256 x 96 = 512 x 128, so the raise is
+// always satisfiable.
+constexpr int kStreamTRegs = 160;
+constexpr int kStreamSRegs = 96;
+static_assert(kStreamTThreads * kStreamTRegs + kStreamSThreads * kStreamSRegs ==
+                  kStreamThreads * 128,
+              "register split uses exactly the launch's registers");
 constexpr int kStreamXs = 20;  // padded staging strides (bank-conflict free)
 constexpr int kStreamTs = 36;
 
@@ -941,9 +951,11 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
   }
   __syncthreads();
   if (tid < kStreamTThreads) {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" : : "n"(kStreamTRegs));
     stream_transform<DISC, SC>(p, full, ready, abort_flag, released, loader,
                                U, X, A, PS, QE, CF, xw, tw, tid);
   } else {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" : : "n"(kStreamSRegs));
     stream_stencil<DISC, SC>(p, ready, abort_flag, released, U, X, A, PS, QE,
                              CF, tid - kStreamTThreads);
   }
