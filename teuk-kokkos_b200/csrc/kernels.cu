@@ -985,6 +985,18 @@ cudaError_t launch_stream_typed(const StageLaunch& p, cudaStream_t stream) {
     }
     if (err != cudaSuccess) return err;
   }
+  // The warpgroups' setmaxnreg requests must fit the registers the CTA is
+  // launched with; a larger request would never be granted.
+  static int launch_regs = -1;
+  if (launch_regs < 0) {
+    cudaFuncAttributes attributes{};
+    const cudaError_t err = cudaFuncGetAttributes(&attributes, kernel);
+    if (err != cudaSuccess) return err;
+    launch_regs = attributes.numRegs;
+  }
+  if (launch_regs * kStreamThreads < kStreamRegisterDemand) {
+    return cudaErrorInvalidConfiguration;
+  }
   const int grid = p.strip_count < sms ? p.strip_count : sms;
   kernel<<<grid, kStreamThreads, bytes, stream>>>(p);
   return cudaGetLastError();

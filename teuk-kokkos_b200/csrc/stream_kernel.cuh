@@ -53,8 +53,9 @@ static_assert(kStreamTWarps == 2 * kStreamBlocks, "two warps per block");
 // always satisfiable.
 constexpr int kStreamTRegs = 160;
 constexpr int kStreamSRegs = 96;
-static_assert(kStreamTThreads * kStreamTRegs + kStreamSThreads * kStreamSRegs ==
-                  kStreamThreads * 128,
+constexpr int kStreamRegisterDemand =
+    kStreamTThreads * kStreamTRegs + kStreamSThreads * kStreamSRegs;
+static_assert(kStreamRegisterDemand == kStreamThreads * 128,
               "register split uses exactly the launch's registers");
 constexpr int kStreamXs = 20;  // padded staging strides (bank-conflict free)
 constexpr int kStreamTs = 36;
