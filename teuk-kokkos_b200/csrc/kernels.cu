@@ -994,7 +994,8 @@ cudaError_t launch_stream_typed(const StageLaunch& p, cudaStream_t stream) {
     if (err != cudaSuccess) return err;
     launch_regs = attributes.numRegs;
   }
-  if (launch_regs * kStreamThreads < kStreamRegisterDemand) {
+  if (launch_regs != kStreamLaunchRegs ||
+      launch_regs * kStreamThreads < kStreamRegisterDemand) {
     return cudaErrorInvalidConfiguration;
   }
   const int grid = p.strip_count < sms ? p.strip_count : sms;

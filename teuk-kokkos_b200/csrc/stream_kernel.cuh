@@ -3,7 +3,7 @@
 // Included by kernels.cu inside its anonymous namespace (it shares the SBP
 // constant tables, the complex helpers and the FP64 MMA wrapper).
 //
-// Per CTA (one per SM, 512 threads):
+// Per CTA (one per SM, 640 threads):
 //   warps 0-7     transform warps: stage combine u = y + c k in place,
 //                 effective Q (stage-constrained reduction) and
 //                 psi_t = A diag(.) S (.) on the FP64 tensor path, two warps
@@ -13,15 +13,15 @@
 //                 and the RK update of every output row, one (row, ell)
 //                 point and all three fields per thread.  They publish how
 //                 many chunks no later work reads.
-// The first transform thread is also the loader: it issues the
-// cp.async.bulk copies of each 16-row chunk of the stage inputs and of the
-// Teukolsky row coefficients into a 4-stage ring (completion through
-// mbarrier transaction counts) as soon as the stencil warps hand a stage
-// back, at chunk boundaries and while it waits for data.
+//   warps 16-19   producer warpgroup (24 registers): one thread issues the
+//                 cp.async.bulk copies of each 16-row chunk of the stage
+//                 inputs and of the Teukolsky row coefficients into a
+//                 4-stage ring (completion through mbarrier transaction
+//                 counts) as soon as the stencil warps hand a stage back.
 // The roles run concurrently on different chunks: the copies of the next
 // chunks, the transforms of the current one and the stencils of the rows it
 // completes overlap.  Every halo row is loaded and transformed once per
-// strip.  Four warps per SM sub-partition, 128 registers per thread.
+// strip.  Five warps per SM sub-partition.
 //
 // Every wait on an mbarrier gives up after kStreamWaitNs: the waiting role
 // raises the CTA's abort flag and records an error code that the host reads
@@ -34,7 +34,8 @@ constexpr int kStreamStages = 4;                            // ring stages
 constexpr int kStreamRing = kStreamChunk * kStreamStages;  // ring rows
 constexpr int kStreamTWarps = 8;
 constexpr int kStreamSWarps = 8;
-constexpr int kStreamThreads = 32 * (kStreamTWarps + kStreamSWarps);
+constexpr int kStreamPWarps = 4;  // producer warpgroup (one thread loads)
+constexpr int kStreamThreads = 32 * (kStreamTWarps + kStreamSWarps + kStreamPWarps);
 constexpr int kStreamTThreads = 32 * kStreamTWarps;
 constexpr int kStreamSThreads = 32 * kStreamSWarps;
 constexpr int kStreamBlocks = 4;  // 4-row transform blocks per 16 rows
@@ -46,17 +47,21 @@ static_assert(kCoefRecord == kCoefCount, "coefficient record");
 static_assert(kStreamSThreads == kStreamNep * kStreamChunk,
               "one stencil thread per (row, ell) of a chunk");
 static_assert(kStreamTWarps == 2 * kStreamBlocks, "two warps per block");
-// Register split between the roles (setmaxnreg): the launch gives every
-// thread 128 registers; the transform warpgroups raise theirs to 160 (their
-// MMA fragments and accumulators stay in registers) and the stencil
-// warpgroups drop to 96.  256 x 160 + 256 x 96 = 512 x 128, so the raise is
-// always satisfiable.
-constexpr int kStreamTRegs = 160;
+// Register split between the warpgroups (setmaxnreg): the launch gives
+// every thread 96 registers; the producer warpgroup drops to 24, the
+// transform warpgroups raise theirs to 128 (their MMA fragments and
+// accumulators stay in registers) and the stencil warpgroups keep 96.
+// 128 x 24 + 256 x 128 + 256 x 96 = 60416 <= 640 x 96, so the raise is
+// always satisfiable; the launcher checks the launch allocation.
+constexpr int kStreamLaunchRegs = 96;
+constexpr int kStreamTRegs = 128;
 constexpr int kStreamSRegs = 96;
+constexpr int kStreamPRegs = 24;
 constexpr int kStreamRegisterDemand =
-    kStreamTThreads * kStreamTRegs + kStreamSThreads * kStreamSRegs;
-static_assert(kStreamRegisterDemand == kStreamThreads * 128,
-              "register split uses exactly the launch's registers");
+    kStreamTThreads * kStreamTRegs + kStreamSThreads * kStreamSRegs +
+    32 * kStreamPWarps * kStreamPRegs;
+static_assert(kStreamRegisterDemand <= kStreamThreads * kStreamLaunchRegs,
+              "register split fits the launch's registers");
 constexpr int kStreamXs = 20;  // padded staging strides (bank-conflict free)
 constexpr int kStreamTs = 36;
 
@@ -586,10 +591,7 @@ __device__ void stream_transform(const StageLaunch& p,
   for (int i = tt; i < kStreamBlocks * 8 * kStreamTs; i += kStreamTThreads) {
     tw_all[i] = 0.0;
   }
-  if (tt == 0) {
-    loader_init<H, HD>(p, loader);
-    loader_pump<H, HD>(p, loader, full, U, X, A, CF, 0);
-  }
+
   int g = 0;
   for (int strip = blockIdx.x; strip < p.strip_count; strip += gridDim.x) {
     const StripGeom sg = strip_geom<H, HD>(p, strip, g);
@@ -630,32 +632,9 @@ __device__ void stream_transform(const StageLaunch& p,
     for (int c = 0; c < sg.chunks; ++c, ++g) {
       const int s = g % kStreamStages;
       const unsigned parity = static_cast<unsigned>(g / kStreamStages) & 1u;
-      // every transform thread waits; all of them leave together on abort.
-      // The loader thread issues the copies of released stages meanwhile.
-      bool landed;
-      if (tt == 0) {
-        landed = false;
-        const unsigned long long t0 = global_ns();
-        while (true) {
-          loader_pump<H, HD>(p, loader, full, U, X, A, CF, *released);
-          if (mbar_try_wait(&full[s], parity)) {
-            landed = true;
-            break;
-          }
-          if (*abort_flag != 0) break;
-          if (global_ns() - t0 > kStreamWaitNs) {
-            *abort_flag = 1;
-            if (p.error != nullptr) atomicExch(p.error, 3);
-            break;
-          }
-        }
-      } else {
-        landed = stream_wait(&full[s], parity, abort_flag, p.error, 3);
-      }
-      if (!named_sync_and(1, kStreamTThreads, landed)) {
-        if (tt == 0) loader_drain(loader, full);
-        return;
-      }
+      // every transform thread waits; all of them leave together on abort
+      const bool landed = stream_wait(&full[s], parity, abort_flag, p.error, 3);
+      if (!named_sync_and(1, kStreamTThreads, landed)) return;
       const int a0 = sg.s0 + c * kStreamChunk;
       const int a1 = min(sg.s1, a0 + kStreamChunk);
       // stage input u = y + dt/2 k, in place
@@ -919,6 +898,45 @@ __device__ void stream_stencil(const StageLaunch& p,
   }
 }
 
+// Registers per thread of the calling warpgroup: raised or lowered from
+// the launch's allocation (setmaxnreg.inc only raises, .dec only lowers).
+template <int N>
+__device__ __forceinline__ void set_max_registers() {
+  static_assert(N % 8 == 0 && N >= 24 && N <= 256, "setmaxnreg range");
+  if constexpr (N > kStreamLaunchRegs) {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" : : "n"(N));
+  } else {  // also at N == launch: every warpgroup sets its count
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" : : "n"(N));
+  }
+}
+
+// Producer: issues every chunk's copies as soon as its stage is free.
+template <int H, int HD>
+__device__ void stream_producer(const StageLaunch& p, StreamLoaderState& L,
+                                unsigned long long* full, double2* U,
+                                double2* X, double2* A, double* CF,
+                                volatile int* released,
+                                volatile int* abort_flag) {
+  loader_init<H, HD>(p, L);
+  unsigned long long t_last = global_ns();
+  while (L.strip < p.strip_count) {
+    const int before = L.g;
+    loader_pump<H, HD>(p, L, full, U, X, A, CF, *released);
+    if (L.g != before) {
+      t_last = global_ns();
+      continue;
+    }
+    if (*abort_flag != 0) break;
+    if (global_ns() - t_last > kStreamWaitNs) {
+      *abort_flag = 1;
+      if (p.error != nullptr) atomicExch(p.error, 5);
+      break;
+    }
+    __nanosleep(128);
+  }
+  if (*abort_flag != 0) loader_drain(L, full);
+}
+
 template <int DISC, int SC>
 __global__ void __launch_bounds__(kStreamThreads, 1)
     stream_stage_kernel(const StageLaunch p) {
@@ -951,14 +969,22 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
     fence_mbarrier_init();
   }
   __syncthreads();
+  using T = DiscTraits<DISC>;
+  constexpr int H = SC ? (T::P > 2 * T::HALF ? T::P : 2 * T::HALF) : T::P;
   if (tid < kStreamTThreads) {
-    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" : : "n"(kStreamTRegs));
+    set_max_registers<kStreamTRegs>();
     stream_transform<DISC, SC>(p, full, ready, abort_flag, released, loader,
                                U, X, A, PS, QE, CF, xw, tw, tid);
-  } else {
-    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" : : "n"(kStreamSRegs));
+  } else if (tid < kStreamTThreads + kStreamSThreads) {
+    set_max_registers<kStreamSRegs>();
     stream_stencil<DISC, SC>(p, ready, abort_flag, released, U, X, A, PS, QE,
                              CF, tid - kStreamTThreads);
+  } else {
+    set_max_registers<kStreamPRegs>();
+    if (tid == kStreamTThreads + kStreamSThreads) {
+      stream_producer<H, T::HALF>(p, loader, full, U, X, A, CF, released,
+                                  abort_flag);
+    }
   }
 }
 
