@@ -573,12 +573,11 @@ template <int DISC, int SC>
 __device__ void stream_transform(const StageLaunch& p,
                                  unsigned long long* full,
                                  unsigned long long* ready,
-                                 volatile int* abort_flag,
-                                 volatile int* released,
-                                 StreamLoaderState& loader, double2* U,
-                                 double2* X, double2* A, double2* PS,
-                                 double2* QE, double* CF, double* xw_all,
-                                 double* tw_all, const int tt) {
+                                 volatile int* abort_flag, double2* U,
+                                 const double2* X, double2* PS, double2* QE,
+                                 const double* CF,
+                                 double* xw_all, double* tw_all,
+                                 const int tt) {
   using T = DiscTraits<DISC>;
   constexpr int P = T::P, HD = T::HALF;
   constexpr int H = SC ? (P > 2 * HD ? P : 2 * HD) : P;
@@ -973,8 +972,8 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
   constexpr int H = SC ? (T::P > 2 * T::HALF ? T::P : 2 * T::HALF) : T::P;
   if (tid < kStreamTThreads) {
     set_max_registers<kStreamTRegs>();
-    stream_transform<DISC, SC>(p, full, ready, abort_flag, released, loader,
-                               U, X, A, PS, QE, CF, xw, tw, tid);
+    stream_transform<DISC, SC>(p, full, ready, abort_flag, U, X, PS, QE, CF,
+                               xw, tw, tid);
   } else if (tid < kStreamTThreads + kStreamSThreads) {
     set_max_registers<kStreamSRegs>();
     stream_stencil<DISC, SC>(p, ready, abort_flag, released, U, X, A, PS, QE,
