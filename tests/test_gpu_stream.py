@@ -118,3 +118,23 @@ def test_mixed_batch_matches_solo(require_gpu):
         solo.initialize_gaussian(pulses[i])
         solo.step(0.0, dts[i], 5)
         assert np.array_equal(batch.get_state(i), solo.get_state()), i
+
+
+def test_solve_split_between_stage_kernels(require_gpu):
+    """ell <= 18 with m = -4..4: the m = +-2, +-1, 0 bands (n_ell >= 17) run
+    the tile kernel, the m = +-3, +-4 bands the streaming kernel, in the
+    same step; the result matches the reference."""
+    config = replace(CASES["kerr_d105"], radial_points=220, theta_nodes=29,
+                     ell_max_first=18, ell_max_second=18)
+    batch = tb.Batch([config])
+    assert batch.stage_kernels() == (1, 1)
+    ref = RefPipeline(config)
+    pulse = pulse_for(config, 13)
+    batch.initialize_gaussian(0, pulse)
+    ref.initialize_gaussian(pulse)
+    dt = step_size(config, 0.1)
+    batch.step([dt], 6)
+    ref.step(0.0, dt, 6)
+    g, r = batch.get_state(0), ref.get_state()
+    for f in range(3):
+        assert relative_error(g[:, f], r[:, f]) < TOL, f"field {f}"

@@ -341,18 +341,32 @@ struct Batch {
     }
     total_complex = static_cast<size_t>(offset);
 
-    // Radial tiles, grouped by (disc, reduction).
+    // Launch groups by (disc, reduction) and stage kernel: segments with
+    // n_ell <= 16 of solves with at most 32 nodes run the streaming kernel
+    // (radial strips), the others the tile kernel (radial tiles).  Segments
+    // do not couple, so a solve may have segments in both.
+    const char* forced = std::getenv("TEUK_B200_STAGE_KERNEL");
+    const bool tile_only = forced != nullptr && std::string(forced) == "tile";
+    const auto streamable = [&](const size_t s) {
+      const InstanceDesc& in = h_inst[static_cast<size_t>(h_seg[s].instance)];
+      return !tile_only && h_seg[s].n_ell <= kStreamMaxEll &&
+             in.ntheta <= kStreamMaxNodes;
+    };
     for (int disc = 0; disc < 3; ++disc) {
       for (int red = 0; red < 2; ++red) {
+       for (int kind = 0; kind < 2; ++kind) {  // 0 streaming, 1 tile
         StageLaunch g{};
         g.disc = disc;
         g.reduction = red;
         const int first_tile = static_cast<int>(h_tiles.size());
         const int H = slab_halo(disc, red);
         const int HD = disc_info(disc).interior_half;
+        std::vector<int> group_segments;
         for (size_t s = 0; s < h_seg.size(); ++s) {
           const InstanceDesc& in = h_inst[static_cast<size_t>(h_seg[s].instance)];
           if (in.disc != disc || in.reduction != red) continue;
+          if (streamable(s) != (kind == 0)) continue;
+          group_segments.push_back(static_cast<int>(s));
           const int ne = h_seg[s].n_ell;
           const int nr = in.nr;
           // at most one (row pair, ell) work item per thread, so the stage
@@ -379,14 +393,18 @@ struct Batch {
         }
         g.tile_count = static_cast<int>(h_tiles.size()) - first_tile;
         if (g.tile_count > 0) {
-          if (stage_smem_bytes(g) > kSmemBudget) {
+          if (kind == 1 && stage_smem_bytes(g) > kSmemBudget) {
             throw std::invalid_argument(
                 "solve shape exceeds the stage kernel's shared-memory tile");
           }
-          group_first_strip.push_back(plan_strips(g, disc, red));
+          g.strips = nullptr;
+          g.strip_count = 0;
+          group_first_strip.push_back(kind == 0 ? plan_strips(g, group_segments)
+                                                : -1);
           groups.push_back(g);
           group_first_tile.push_back(first_tile);
         }
+       }
       }
     }
 
@@ -489,27 +507,21 @@ struct Batch {
     }
   }
 
-  // Radial strips of a launch group for the streaming kernel, sorted by
-  // n_ell (largest first) so that a CTA's consecutive strips mostly share
-  // one ring row stride.  Returns the group's first strip index, or -1 when
-  // the group's shape needs the tile kernel.
-  int plan_strips(StageLaunch& g, const int disc, const int red) {
-    g.strips = nullptr;
-    g.strip_count = 0;
-    if (g.max_ell > kStreamMaxEll || g.max_theta > kStreamMaxNodes) return -1;
-    const char* forced = std::getenv("TEUK_B200_STAGE_KERNEL");
-    if (forced != nullptr && std::string(forced) == "tile") return -1;
+  // Radial strips of a streaming launch group (its segments `segs`),
+  // sorted by n_ell (largest first) so that a CTA's consecutive strips
+  // mostly share one ring row stride.  Returns the group's first strip
+  // index.
+  int plan_strips(StageLaunch& g, std::vector<int> segs) {
+    if (g.max_ell > kStreamMaxEll || g.max_theta > kStreamMaxNodes) {
+      throw std::logic_error("segment outside the streaming kernel's shapes");
+    }
     int device = 0, sms = 0;
     check(cudaGetDevice(&device), "cudaGetDevice");
     check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device),
           "SM count");
-    std::vector<int> segs;
     long long rows = 0;
-    for (size_t s = 0; s < h_seg.size(); ++s) {
-      const InstanceDesc& in = h_inst[static_cast<size_t>(h_seg[s].instance)];
-      if (in.disc != disc || in.reduction != red) continue;
-      segs.push_back(static_cast<int>(s));
-      rows += in.nr;
+    for (const int s : segs) {
+      rows += h_inst[static_cast<size_t>(h_seg[static_cast<size_t>(s)].instance)].nr;
     }
     const long long want = static_cast<long long>(std::max(sms, 1)) * kStripsPerCta;
     const int target = static_cast<int>(std::min<long long>(
