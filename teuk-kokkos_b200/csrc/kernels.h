@@ -60,8 +60,8 @@ cudaError_t launch_coefficient_table(const InstanceDesc* instance_device,
                                      int nr, int row0, double* table,
                                      cudaStream_t stream);
 
-// Streaming kernel eligibility of a launch group: n_ell <= 16 and at most 32
-// Gauss-Legendre nodes per row.
+// Streaming kernel eligibility of a band (segment): n_ell <= 16, and at
+// most 32 Gauss-Legendre nodes per row in its solve.
 inline constexpr int kStreamMaxEll = 16;
 inline constexpr int kStreamMaxNodes = 32;
 inline constexpr int kStripMinRows = 64;
