@@ -138,3 +138,27 @@ def test_solve_split_between_stage_kernels(require_gpu):
     g, r = batch.get_state(0), ref.get_state()
     for f in range(3):
         assert relative_error(g[:, f], r[:, f]) < TOL, f"field {f}"
+
+
+def test_stage_wait_timeout_is_reported(require_gpu, monkeypatch):
+    """Failure detection without a GPU fault: with the test hook
+    TEUK_B200_WITHHOLD_CHUNK the producer of one CTA never loads a chunk in
+    stage-1 launches, so the transform warps' bounded wait runs out (2 s),
+    every warp role leaves its loop, and the step reports the timeout.  The
+    device context stays usable: a new pipeline then steps like the
+    reference."""
+    config = LONG["kerr_d105_long"]
+    dt = step_size(config, 0.1)
+    monkeypatch.setenv("TEUK_B200_WITHHOLD_CHUNK", "2")
+    broken = tb.Pipeline(config)
+    monkeypatch.delenv("TEUK_B200_WITHHOLD_CHUNK")
+    broken.initialize_gaussian(pulse_for(config, 19))
+    with pytest.raises(tb.TeukError, match="timed out"):
+        broken.step(0.0, dt, 1)
+    broken.close()
+    config, gpu, ref = _pair("kerr_d105_long")
+    gpu.step(0.0, dt, 2)
+    ref.step(0.0, dt, 2)
+    g, r = gpu.get_state(), ref.get_state()
+    for f in range(3):
+        assert relative_error(g[:, f], r[:, f]) < TOL, f"field {f}"

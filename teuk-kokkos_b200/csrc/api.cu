@@ -219,6 +219,7 @@ struct Batch {
   DeviceArray<TileDesc> d_strips;
   DeviceArray<int> d_error;  // streaming-kernel wait timeouts
   DeviceArray<double> d_coef;  // Teukolsky row coefficients per solve row
+  int withhold_chunk_ = -1;    // failure-detection test hook
   int coef_rows = 0;
   DeviceArray<double> d_mat, d_trig;
   DeviceArray<double2> d_nodal;     // one instance's nodal state (lazy)
@@ -347,6 +348,9 @@ struct Batch {
     // do not couple, so a solve may have segments in both.
     const char* forced = std::getenv("TEUK_B200_STAGE_KERNEL");
     const bool tile_only = forced != nullptr && std::string(forced) == "tile";
+    // failure-detection test hook (StageLaunch::withhold_chunk)
+    const char* withhold = std::getenv("TEUK_B200_WITHHOLD_CHUNK");
+    withhold_chunk_ = withhold != nullptr ? std::atoi(withhold) : -1;
     const auto streamable = [&](const size_t s) {
       const InstanceDesc& in = h_inst[static_cast<size_t>(h_seg[s].instance)];
       return !tile_only && h_seg[s].n_ell <= kStreamMaxEll &&
@@ -490,6 +494,7 @@ struct Batch {
       g.tiles = d_tiles.ptr + group_first_tile[gi];
       g.error = d_error.ptr;
       g.coef_table = d_coef.ptr;
+      g.withhold_chunk = withhold_chunk_;
       if (group_first_strip[gi] >= 0) {
         g.strips = d_strips.ptr + group_first_strip[gi];
       } else {

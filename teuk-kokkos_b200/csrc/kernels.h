@@ -52,6 +52,10 @@ struct StageLaunch {
   // radial row (coefficient_table_kernel); the m-dependent imaginary parts
   // (entries 4, 6, 8) are stored for m = 1 and scaled by m where used.
   const double* coef_table;
+  // Failure-detection test hook (-1: off): in stage-1 launches the producer
+  // of CTA 0 never issues this chunk, so the waits for it run out and the
+  // launch reports a timeout through `error`.
+  int withhold_chunk;
 };
 
 inline constexpr int kCoefRecord = 10;

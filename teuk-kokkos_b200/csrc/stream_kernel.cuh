@@ -419,22 +419,26 @@ __device__ void loader_pump(const StageLaunch& p, StreamLoaderState& state,
                                  : 0u;
     const unsigned bytes_c =
         static_cast<unsigned>(a1 - a0) * kCoefCount * sizeof(double);
-    mbar_arrive_expect_tx(&full[s], bytes_u + bytes_x + bytes_a + bytes_c);
-    const long long gsrc = sg.seg_offset + static_cast<long long>(a0) * sg.rs;
-    const int ra0 = ring_row(a0, sg.shift);
-    bulk_copy_g2s(U + ra0 * sg.rs, L.src_u + gsrc, bytes_u, &full[s]);
-    if (bytes_x != 0u) {
-      bulk_copy_g2s(X + ra0 * sg.rs, L.src_x + gsrc, bytes_x, &full[s]);
+    const bool withheld = L.g == p.withhold_chunk && p.stage == kStage1 &&
+                          blockIdx.x == 0;  // failure-detection test hook
+    if (!withheld) {
+      mbar_arrive_expect_tx(&full[s], bytes_u + bytes_x + bytes_a + bytes_c);
+      const long long gsrc = sg.seg_offset + static_cast<long long>(a0) * sg.rs;
+      const int ra0 = ring_row(a0, sg.shift);
+      bulk_copy_g2s(U + ra0 * sg.rs, L.src_u + gsrc, bytes_u, &full[s]);
+      if (bytes_x != 0u) {
+        bulk_copy_g2s(X + ra0 * sg.rs, L.src_x + gsrc, bytes_x, &full[s]);
+      }
+      if (bytes_a != 0u) {
+        bulk_copy_g2s(A + ring_row(o0, sg.shift) * sg.rs,
+                      L.src_a + sg.seg_offset + static_cast<long long>(o0) * sg.rs,
+                      bytes_a, &full[s]);
+      }
+      bulk_copy_g2s(CF + ra0 * kCoefCount,
+                    p.coef_table +
+                        static_cast<long long>(sg.coef_row0 + a0) * kCoefCount,
+                    bytes_c, &full[s]);
     }
-    if (bytes_a != 0u) {
-      bulk_copy_g2s(A + ring_row(o0, sg.shift) * sg.rs,
-                    L.src_a + sg.seg_offset + static_cast<long long>(o0) * sg.rs,
-                    bytes_a, &full[s]);
-    }
-    bulk_copy_g2s(CF + ra0 * kCoefCount,
-                  p.coef_table +
-                      static_cast<long long>(sg.coef_row0 + a0) * kCoefCount,
-                  bytes_c, &full[s]);
     L.prev_rs = sg.rs;
     ++L.g;
     if (++L.c == sg.chunks) {
