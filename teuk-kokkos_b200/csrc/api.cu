@@ -219,6 +219,7 @@ struct Batch {
   DeviceArray<TileDesc> d_strips;
   DeviceArray<int> d_error;  // streaming-kernel wait timeouts
   DeviceArray<double> d_coef;  // Teukolsky row coefficients per solve row
+  DeviceArray<double> d_nodes;  // 1 / C_T on the nodes per solve row
   int withhold_chunk_ = -1;    // failure-detection test hook
   int coef_rows = 0;
   DeviceArray<double> d_mat, d_trig;
@@ -438,6 +439,7 @@ struct Batch {
     d_error.allocate(1);
     check(cudaMemset(d_error.ptr, 0, sizeof(int)), "memset error word");
     d_coef.allocate(static_cast<size_t>(std::max(coef_rows, 1)) * kCoefRecord);
+    d_nodes.allocate(static_cast<size_t>(std::max(coef_rows, 1)) * kNodeRecord);
     d_mat.allocate(std::max<size_t>(h_mat.size(), 1));
     d_trig.allocate(h_trig.size());
     nodal_max = 0;
@@ -461,11 +463,6 @@ struct Batch {
           "cudaStreamCreate");
     stream = own_stream;
     upload_descriptors();
-    for (size_t i = 0; i < h_inst.size(); ++i) {
-      check(launch_coefficient_table(d_inst.ptr + i, h_inst[i].nr,
-                                     h_inst[i].coef_row0, d_coef.ptr, stream),
-            "coefficient table");
-    }
     check(cudaMemcpy(d_seg.ptr, h_seg.data(), h_seg.size() * sizeof(SegmentDesc),
                      cudaMemcpyHostToDevice),
           "upload segments");
@@ -489,11 +486,18 @@ struct Batch {
     check(cudaMemcpy(d_trig.ptr, h_trig.data(), h_trig.size() * sizeof(double),
                      cudaMemcpyHostToDevice),
           "upload trig");
+    for (size_t i = 0; i < h_inst.size(); ++i) {
+      check(launch_coefficient_table(d_inst.ptr + i, d_trig.ptr, h_inst[i].nr,
+                                     h_inst[i].coef_row0, d_coef.ptr,
+                                     d_nodes.ptr, stream),
+            "coefficient table");
+    }
     for (size_t gi = 0; gi < groups.size(); ++gi) {
       StageLaunch& g = groups[gi];
       g.tiles = d_tiles.ptr + group_first_tile[gi];
       g.error = d_error.ptr;
       g.coef_table = d_coef.ptr;
+      g.node_table = d_nodes.ptr;
       g.withhold_chunk = withhold_chunk_;
       if (group_first_strip[gi] >= 0) {
         g.strips = d_strips.ptr + group_first_strip[gi];
@@ -991,6 +995,7 @@ struct Batch {
            h_mat.size() * sizeof(double) + h_trig.size() * sizeof(double) +
            h_tiles.size() * sizeof(TileDesc) + h_seg.size() * sizeof(SegmentDesc) +
            h_strips.size() * sizeof(TileDesc) + d_coef.count * sizeof(double) +
+           d_nodes.count * sizeof(double) +
            d_endpoint.count * sizeof(double2);
   }
 };
@@ -1173,8 +1178,8 @@ size_t linear_footprint(const teuk_b200::InstancePlan& plan) {
     matrix += 2 * static_cast<size_t>(mp.n_ell * plan.config.ntheta);
   }
   return 4 * complex_count * sizeof(double2) + matrix * sizeof(double) +
-         static_cast<size_t>(plan.config.nr) * teuk_b200::kCoefRecord *
-             sizeof(double) +
+         static_cast<size_t>(plan.config.nr) *
+             (teuk_b200::kCoefRecord + teuk_b200::kNodeRecord) * sizeof(double) +
          plan.value_count() * sizeof(double2);
 }
 

@@ -55,7 +55,7 @@ struct InstanceDesc {
   double dt;
   int nr;
   int ntheta;
-  int trig_offset;  // doubles into the trig pool: sin^2(theta)[nt], cos[nt]
+  int trig_offset;  // doubles into the trig pool: sin(theta)[nt], cos(theta)[nt]
   int reduction;    // 0 free damped, 1 stage constrained
   int disc;
   int coef_row0;    // first row of this solve in the coefficient table

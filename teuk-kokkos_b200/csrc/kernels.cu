@@ -1159,11 +1159,14 @@ size_t stage_smem_bytes(const StageLaunch& p) {
 }
 
 cudaError_t launch_coefficient_table(const InstanceDesc* instance_device,
-                                     const int nr, const int row0,
-                                     double* table, cudaStream_t stream) {
+                                     const double* trig, const int nr,
+                                     const int row0, double* table,
+                                     double* node_table, cudaStream_t stream) {
   if (nr <= 0) return cudaSuccess;
   coefficient_table_kernel<<<(nr + 127) / 128, 128, 0, stream>>>(
-      instance_device, nr, table + static_cast<long long>(row0) * kCoefCount);
+      instance_device, trig, nr,
+      table + static_cast<long long>(row0) * kCoefCount,
+      node_table + static_cast<long long>(row0) * kNodeRecord);
   return cudaGetLastError();
 }
 

@@ -52,22 +52,29 @@ struct StageLaunch {
   // radial row (coefficient_table_kernel); the m-dependent imaginary parts
   // (entries 4, 6, 8) are stored for m = 1 and scaled by m where used.
   const double* coef_table;
+  // 1 / C_T(r, theta_j) of every solve on its Gauss-Legendre nodes,
+  // kNodeRecord doubles per radial row (zero beyond the solve's nodes)
+  const double* node_table;
   // Failure-detection test hook (-1: off): in stage-1 launches the producer
   // of CTA 0 never issues this chunk, so the waits for it run out and the
   // launch reports a timeout through `error`.
   int withhold_chunk;
 };
 
-inline constexpr int kCoefRecord = 10;
-// Fills the coefficient table rows of one solve: table[(row0 + r) * 10 + k].
-cudaError_t launch_coefficient_table(const InstanceDesc* instance_device,
-                                     int nr, int row0, double* table,
-                                     cudaStream_t stream);
-
 // Streaming kernel eligibility of a band (segment): n_ell <= 16, and at
 // most 32 Gauss-Legendre nodes per row in its solve.
 inline constexpr int kStreamMaxEll = 16;
 inline constexpr int kStreamMaxNodes = 32;
+
+inline constexpr int kCoefRecord = 10;
+inline constexpr int kNodeRecord = kStreamMaxNodes;
+// Fills the coefficient table rows of one solve, table[(row0 + r) * 10 + k],
+// and its node-inverse rows, node_table[(row0 + r) * kNodeRecord + j];
+// `trig` is the device trig pool the instance's trig_offset points into.
+cudaError_t launch_coefficient_table(const InstanceDesc* instance_device,
+                                     const double* trig, int nr, int row0,
+                                     double* table, double* node_table,
+                                     cudaStream_t stream);
 inline constexpr int kStripMinRows = 64;
 // Radial strips per CTA the host aims for when it splits segments.
 inline constexpr int kStripsPerCta = 8;

@@ -15,7 +15,8 @@
 //                 many chunks no later work reads.
 //   warps 16-19   producer warpgroup (24 registers): one thread issues the
 //                 cp.async.bulk copies of each 16-row chunk of the stage
-//                 inputs and of the Teukolsky row coefficients into a
+//                 inputs, of the Teukolsky row coefficients and (Kerr) of
+//                 the rows' 1 / C_T node values into a
 //                 4-stage ring (completion through mbarrier transaction
 //                 counts) as soon as the stencil warps hand a stage back.
 // The roles run concurrently on different chunks: the copies of the next
@@ -163,6 +164,7 @@ __device__ bool stream_wait(unsigned long long* bar, const unsigned parity,
 struct StripGeom {
   long long seg_offset;  // complex offset of row 0 of the segment
   int segment, instance, m, ne, rs, nr, coef_row0;
+  int kerr;  // the transform reads 1 / C_T node rows
   int r0, r1;  // output rows
   int s0, s1;  // input rows (with halo)
   int t0, t1;  // psi_t / effective-Q rows
@@ -185,8 +187,8 @@ struct StreamLoaderState {
 // Shared-memory carve-up (bytes), identical on host and device.
 struct StreamLayout {
   static constexpr int kRowMax = 3 * kStreamNep;  // complex per ring row
-  size_t bars, loader, uring, xring, aring, pring, qring, coef, xw, tw,
-      total;
+  size_t bars, loader, uring, xring, aring, pring, qring, coef, nodes, xw,
+      tw, total;
   __host__ __device__ explicit StreamLayout(const int sc) {
     size_t o = 0;
     bars = o;
@@ -206,6 +208,8 @@ struct StreamLayout {
     if (sc) o += static_cast<size_t>(kStreamRing) * kStreamNep * 16;
     coef = o;
     o += static_cast<size_t>(kStreamRing) * kCoefCount * 8;
+    nodes = o;
+    o += static_cast<size_t>(kStreamRing) * kNodeRecord * 8;
     xw = o;
     o += static_cast<size_t>(kStreamBlocks) * 16 * kStreamXs * 8;
     tw = o;
@@ -230,6 +234,7 @@ __device__ __forceinline__ StripGeom strip_geom(const StageLaunch& p,
   g.rs = 3 * seg.n_ell;
   g.nr = in.nr;
   g.coef_row0 = in.coef_row0;
+  g.kerr = in.spin != 0.0 ? 1 : 0;
   g.r0 = t.r0;
   g.r1 = t.r1;
   g.s0 = max(0, t.r0 - H);
@@ -303,18 +308,6 @@ __device__ __forceinline__ double2 ring_dissipation(const Row& at, const int r,
     }
   }
   return acc;
-}
-
-// Register window of N ring rows starting at absolute row `first`.
-template <int N>
-__device__ __forceinline__ void ring_window(double2 (&w)[N],
-                                            const double2* column,
-                                            const int first, const int shift,
-                                            const int stride) {
-#pragma unroll
-  for (int i = 0; i < N; ++i) {
-    w[i] = column[ring_row(first + i, shift) * stride];
-  }
 }
 
 // Closure rows straight from a ring column: the first K rows (r < BR) or
@@ -393,7 +386,8 @@ __device__ void loader_init(const StageLaunch& p, StreamLoaderState& L) {
 template <int H, int HD>
 __device__ void loader_pump(const StageLaunch& p, StreamLoaderState& state,
                             unsigned long long* full, double2* U, double2* X,
-                            double2* A, double* CF, const int released) {
+                            double2* A, double* CF, double* NI,
+                            const int released) {
   if (state.strip >= p.strip_count || state.g >= released + kStreamStages) {
     return;
   }
@@ -419,10 +413,14 @@ __device__ void loader_pump(const StageLaunch& p, StreamLoaderState& state,
                                  : 0u;
     const unsigned bytes_c =
         static_cast<unsigned>(a1 - a0) * kCoefCount * sizeof(double);
+    const unsigned bytes_n =
+        sg.kerr ? static_cast<unsigned>(a1 - a0) * kNodeRecord * sizeof(double)
+                : 0u;
     const bool withheld = L.g == p.withhold_chunk && p.stage == kStage1 &&
                           blockIdx.x == 0;  // failure-detection test hook
     if (!withheld) {
-      mbar_arrive_expect_tx(&full[s], bytes_u + bytes_x + bytes_a + bytes_c);
+      mbar_arrive_expect_tx(&full[s],
+                            bytes_u + bytes_x + bytes_a + bytes_c + bytes_n);
       const long long gsrc = sg.seg_offset + static_cast<long long>(a0) * sg.rs;
       const int ra0 = ring_row(a0, sg.shift);
       bulk_copy_g2s(U + ra0 * sg.rs, L.src_u + gsrc, bytes_u, &full[s]);
@@ -438,6 +436,12 @@ __device__ void loader_pump(const StageLaunch& p, StreamLoaderState& state,
                     p.coef_table +
                         static_cast<long long>(sg.coef_row0 + a0) * kCoefCount,
                     bytes_c, &full[s]);
+      if (bytes_n != 0u) {
+        bulk_copy_g2s(NI + ra0 * kNodeRecord,
+                      p.node_table + static_cast<long long>(sg.coef_row0 + a0) *
+                                         kNodeRecord,
+                      bytes_n, &full[s]);
+      }
     }
     L.prev_rs = sg.rs;
     ++L.g;
@@ -469,7 +473,6 @@ __device__ void loader_drain(const StreamLoaderState& L,
 struct PsiFragments {
   double fs[2][4];  // S(j = (2h + i) * 8 + group, l = ks * 4 + quad)
   double fa[8];     // A(l = h * 8 + group, j = ks * 4 + quad)
-  double a2s2[2];   // a^2 sin^2(theta_j)
   double gcos[2];   // 2 s a cos(theta_j)
 };
 
@@ -480,8 +483,8 @@ struct PsiFragments {
 template <int SC>
 __device__ __forceinline__ void stream_psi_half(
     const int q0, const int qlim, const int h, const StripGeom& sg,
-    const double2* U, const double2* QE, const double* CF, double2* PS,
-    double* xw, double* tw, const PsiFragments& F, const int nt,
+    const double2* U, const double2* QE, const double* CF, const double* NI,
+    double2* PS, double* xw, double* tw, const PsiFragments& F,
     const int mts, const int ksa, const int lane) {
   const int quad = lane & 3;
   const int group = lane >> 2;
@@ -515,12 +518,6 @@ __device__ __forceinline__ void stream_psi_half(
       bx[n][ks] = xw[(n * 8 + group) * kStreamXs + ks * 4 + quad];
     }
   }
-  double c0r[2];  // C_T without the sin^2 term, rows 2n + (quad >> 1)
-#pragma unroll
-  for (int n = 0; n < 2; ++n) {
-    const int r = q0 + 2 * n + (quad >> 1);
-    c0r[n] = r < qlim ? CF[ring_row(r, sg.shift) * kCoefCount] : 1.0;
-  }
 #pragma unroll
   for (int i = 0; i < 2; ++i) {
     const int mt = 2 * h + i;
@@ -534,12 +531,11 @@ __device__ __forceinline__ void stream_psi_half(
         }
       }
       const int j = mt * 8 + group;
-      const bool node = j < nt;
-      double inv[2];
+      double inv[2];  // 1 / C_T(r, theta_j); zero beyond the solve's nodes
 #pragma unroll
       for (int n = 0; n < 2; ++n) {
         const int r = q0 + 2 * n + (quad >> 1);
-        inv[n] = (node && r < qlim) ? 1.0 / (c0r[n] - F.a2s2[i]) : 0.0;
+        inv[n] = r < qlim ? NI[ring_row(r, sg.shift) * kNodeRecord + j] : 0.0;
       }
 #pragma unroll
       for (int n = 0; n < 2; ++n) {
@@ -579,7 +575,7 @@ __device__ void stream_transform(const StageLaunch& p,
                                  unsigned long long* ready,
                                  volatile int* abort_flag, double2* U,
                                  const double2* X, double2* PS, double2* QE,
-                                 const double* CF,
+                                 const double* CF, const double* NI,
                                  double* xw_all, double* tw_all,
                                  const int tt) {
   using T = DiscTraits<DISC>;
@@ -610,7 +606,6 @@ __device__ void stream_transform(const StageLaunch& p,
       const SegmentDesc& seg = p.segments[sg.segment];
       const double* St = p.matrices + seg.mat_offset;  // St[l][j]
       const double* At = St + ne * nt;                 // At[j][l]
-      const double a2 = in.spin * in.spin;
       const double sa2 = 2.0 * (static_cast<double>(kSpinWeight) * in.spin);
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
@@ -620,8 +615,6 @@ __device__ void stream_transform(const StageLaunch& p,
           const int l = ks * 4 + quad;
           F.fs[i][ks] = (j < nt && l < ne) ? St[l * nt + j] : 0.0;
         }
-        const double sj = j < nt ? p.trig[in.trig_offset + j] : 0.0;
-        F.a2s2[i] = a2 * sj * sj;
         F.gcos[i] = j < nt ? sa2 * p.trig[in.trig_offset + nt + j] : 0.0;
       }
       const int l = h * 8 + group;
@@ -681,8 +674,8 @@ __device__ void stream_transform(const StageLaunch& p,
       if (pe > pd) {
         if (kerr) {
           for (int q = pd; q < pe; q += 4 * kStreamBlocks) {
-            stream_psi_half<SC>(q + 4 * blk, pe, h, sg, U, QE, CF, PS, xw, tw,
-                                F, nt, mts, ksa, lane);
+            stream_psi_half<SC>(q + 4 * blk, pe, h, sg, U, QE, CF, NI, PS, xw,
+                                tw, F, mts, ksa, lane);
           }
         } else {
           const int items = (pe - pd) * kStreamNep;
@@ -800,51 +793,56 @@ __device__ void stream_stencil(const StageLaunch& p,
         const double* cf = CF + rr * kCoefCount;
         double2 kP, kQ, kpsi;
         if (r >= T::BR && r + T::BR < nr) {
-          {  // psi: D psi (constraint), dissipation, (c_psi + lambda) psi
-            double2 w[1 + 2 * P];
-            ring_window(w, cpsi, r - P, sg.shift, rs);
-            const double2 psi = w[P];
-            kQ = cscale(damping, cscale(inv_h, window_derivative<DISC, 1, P>(w, 0)));
-            kpsi = dissipate
-                       ? cscale(diss_scale, window_dissipation<DISC, 1, P>(w, 0))
-                       : make_double2(0.0, 0.0);
-            kP = cadd(cmul(make_double2(cf[7], mm * cf[8]), psi),
-                      cscale(lambda, psi));
-          }
-          {  // psi_t: D psi_t into Q_t, psi_t itself
-            double2 w[1 + 2 * HD];
-            ring_window(w, cpt, r - HD, sg.shift, kStreamNep);
-            kQ = cadd(kQ, cscale(inv_h, window_derivative<DISC, 1, HD>(w, 0)));
-            kpsi = cadd(kpsi, w[HD]);
-          }
-          {  // Q: -gamma Q, dissipation; free-damped: H_R D Q + q Q
-            double2 w[1 + 2 * P];
-            ring_window(w, cQ, r - P, sg.shift, rs);
-            const double2 Q = w[P];
-            kQ = csub(kQ, cscale(damping, Q));
-            if (dissipate) {
-              kQ = cfma(diss_scale, window_dissipation<DISC, 1, P>(w, 0), kQ);
+          // One pass over the tap offsets k = P..1: the two ring rows r +- k
+          // are addressed once for every field; dissipation taps of psi, Q,
+          // P at every k, derivative taps of psi, Q (or effective Q) and
+          // psi_t for k <= HALF.  Seven independent accumulations.
+          const double2 psi = cpsi[rr * rs];
+          const double2 Q = cQ[rr * rs];
+          const double e0 = c_sbp.diss_interior[DISC][0];
+          double2 spsi = cscale(e0, psi), sQ = cscale(e0, Q),
+                  sP = cscale(e0, cP[rr * rs]);
+          double2 dpsi = make_double2(0.0, 0.0), dq = dpsi, dpt = dpsi;
+#pragma unroll
+          for (int k = P; k >= 1; --k) {
+            const int ra = ring_row(r + k, sg.shift);
+            const int rb = ring_row(r - k, sg.shift);
+            const double ek = c_sbp.diss_interior[DISC][k];
+            const double2 pa = cpsi[ra * rs], pb = cpsi[rb * rs];
+            const double2 qa = cQ[ra * rs], qb = cQ[rb * rs];
+            const double2 fa = cP[ra * rs], fb = cP[rb * rs];
+            spsi = cfma(ek, cadd(pa, pb), spsi);
+            sQ = cfma(ek, cadd(qa, qb), sQ);
+            sP = cfma(ek, cadd(fa, fb), sP);
+            if (k <= HD) {
+              const double ck = c_sbp.interior[DISC][k];
+              dpsi = cfma(ck, csub(pa, pb), dpsi);
+              dpt = cfma(ck, csub(cpt[ra * kStreamNep], cpt[rb * kStreamNep]),
+                         dpt);
+              if (SC) {
+                dq = cfma(ck, csub(cqe[ra * kStreamNep], cqe[rb * kStreamNep]),
+                          dq);
+              } else {
+                dq = cfma(ck, csub(qa, qb), dq);
+              }
             }
-            if (!SC) {
-              const double2 dq =
-                  cscale(inv_h, window_derivative<DISC, 1, P>(w, 0));
-              kP = cadd(kP, cadd(cscale(cf[2], dq),
-                                 cmul(make_double2(cf[5], mm * cf[6]), Q)));
-            }
           }
-          if (SC) {  // stage-constrained effective Q = D psi
-            double2 w[1 + 2 * HD];
-            ring_window(w, cqe, r - HD, sg.shift, kStreamNep);
-            const double2 dq =
-                cscale(inv_h, window_derivative<DISC, 1, HD>(w, 0));
-            kP = cadd(kP, cadd(cscale(cf[2], dq),
-                               cmul(make_double2(cf[5], mm * cf[6]), w[HD])));
-          }
-          if (dissipate) {  // P: dissipation only
-            double2 w[1 + 2 * P];
-            ring_window(w, cP, r - P, sg.shift, rs);
-            kP = cfma(diss_scale, window_dissipation<DISC, 1, P>(w, 0), kP);
-          }
+          // psi: D psi (constraint), dissipation, (c_psi + lambda) psi
+          kQ = cscale(damping, cscale(inv_h, dpsi));
+          kpsi = dissipate ? cscale(diss_scale, spsi) : make_double2(0.0, 0.0);
+          kP = cadd(cmul(make_double2(cf[7], mm * cf[8]), psi),
+                    cscale(lambda, psi));
+          // psi_t: D psi_t into Q_t, psi_t itself
+          kQ = cadd(kQ, cscale(inv_h, dpt));
+          kpsi = cadd(kpsi, cpt[rr * kStreamNep]);
+          // Q: -gamma Q, dissipation; H_R D Q + q Q with Q the evolved Q
+          // (free-damped) or the effective Q = D psi (stage-constrained)
+          kQ = csub(kQ, cscale(damping, Q));
+          if (dissipate) kQ = cfma(diss_scale, sQ, kQ);
+          const double2 qp = SC ? cqe[rr * kStreamNep] : Q;
+          kP = cadd(kP, cadd(cscale(cf[2], cscale(inv_h, dq)),
+                             cmul(make_double2(cf[5], mm * cf[6]), qp)));
+          if (dissipate) kP = cfma(diss_scale, sP, kP);
         } else {  // closure rows
           const double2 psi = cpsi[rr * rs];
           const double2 Q = cQ[rr * rs];
@@ -918,13 +916,13 @@ template <int H, int HD>
 __device__ void stream_producer(const StageLaunch& p, StreamLoaderState& L,
                                 unsigned long long* full, double2* U,
                                 double2* X, double2* A, double* CF,
-                                volatile int* released,
+                                double* NI, volatile int* released,
                                 volatile int* abort_flag) {
   loader_init<H, HD>(p, L);
   unsigned long long t_last = global_ns();
   while (L.strip < p.strip_count) {
     const int before = L.g;
-    loader_pump<H, HD>(p, L, full, U, X, A, CF, *released);
+    loader_pump<H, HD>(p, L, full, U, X, A, CF, NI, *released);
     if (L.g != before) {
       t_last = global_ns();
       continue;
@@ -959,6 +957,7 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
   double2* PS = reinterpret_cast<double2*>(stream_smem + Ls.pring);
   double2* QE = reinterpret_cast<double2*>(stream_smem + Ls.qring);
   double* CF = reinterpret_cast<double*>(stream_smem + Ls.coef);
+  double* NI = reinterpret_cast<double*>(stream_smem + Ls.nodes);
   double* xw = reinterpret_cast<double*>(stream_smem + Ls.xw);
   double* tw = reinterpret_cast<double*>(stream_smem + Ls.tw);
   const int tid = threadIdx.x;
@@ -977,7 +976,7 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
   if (tid < kStreamTThreads) {
     set_max_registers<kStreamTRegs>();
     stream_transform<DISC, SC>(p, full, ready, abort_flag, U, X, PS, QE, CF,
-                               xw, tw, tid);
+                               NI, xw, tw, tid);
   } else if (tid < kStreamTThreads + kStreamSThreads) {
     set_max_registers<kStreamSRegs>();
     stream_stencil<DISC, SC>(p, ready, abort_flag, released, U, X, A, PS, QE,
@@ -985,15 +984,33 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
   } else {
     set_max_registers<kStreamPRegs>();
     if (tid == kStreamTThreads + kStreamSThreads) {
-      stream_producer<H, T::HALF>(p, loader, full, U, X, A, CF, released,
+      stream_producer<H, T::HALF>(p, loader, full, U, X, A, CF, NI, released,
                                   abort_flag);
     }
   }
 }
 
-// Teukolsky row coefficients of one solve (m = 1 for entries 4, 6, 8).
+// Teukolsky row coefficients of one solve (m = 1 for entries 4, 6, 8) and
+// the inverse of C_T(r, theta_j) = C_T0(r) - a^2 sin^2(theta_j) on its
+// nodes (the diagonal of the implicit ell-coupling, A diag(1/C_T) S).
 __global__ void coefficient_table_kernel(const InstanceDesc* instance,
-                                         const int nr, double* out) {
+                                         const double* trig, const int nr,
+                                         double* out, double* node_out) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r < nr) row_coefficients(*instance, 1, r, out + r * kCoefCount);
+  if (r >= nr) return;
+  const InstanceDesc in = *instance;
+  double cf[kCoefCount];
+  row_coefficients(in, 1, r, cf);
+#pragma unroll
+  for (int k = 0; k < kCoefCount; ++k) out[r * kCoefCount + k] = cf[k];
+  const double a2 = in.spin * in.spin;
+  double* inv = node_out + static_cast<long long>(r) * kNodeRecord;
+  for (int j = 0; j < kNodeRecord; ++j) {
+    double v = 0.0;
+    if (j < in.ntheta) {
+      const double s = trig[in.trig_offset + j];
+      v = 1.0 / __dsub_rn(cf[0], __dmul_rn(__dmul_rn(a2, s), s));
+    }
+    inv[j] = v;
+  }
 }
