@@ -3,17 +3,18 @@
 // Included by kernels.cu inside its anonymous namespace (it shares the SBP
 // constant tables, the complex helpers and the FP64 MMA wrapper).
 //
-// Per CTA (one per SM, 640 threads):
+// Per CTA (one per SM, 512 threads):
 //   warps 0-7     transform warps: stage combine u = y + c k in place,
 //                 effective Q (stage-constrained reduction) and
 //                 psi_t = A diag(.) S (.) on the FP64 tensor path, two warps
 //                 per 4-row block (each takes half of the node tiles of the
 //                 synthesis and one ell tile of the analysis);
-//   warps 8-15    stencil warps: SBP derivatives, dissipation, RHS assembly
-//                 and the RK update of every output row, one (row, ell)
-//                 point and all three fields per thread.  They publish how
+//   warps 8-11    stencil warps: SBP derivatives, dissipation, RHS assembly
+//                 and the RK update of every output row, two adjacent rows
+//                 of one ell and all three fields per thread (one register
+//                 window per field serves both rows).  They publish how
 //                 many chunks no later work reads.
-//   warps 16-19   producer warpgroup (24 registers): one thread issues the
+//   warps 12-15   producer warpgroup (24 registers): one thread issues the
 //                 cp.async.bulk copies of each 16-row chunk of the stage
 //                 inputs, of the Teukolsky row coefficients and (Kerr) of
 //                 the rows' 1 / C_T node values into a
@@ -22,7 +23,7 @@
 // The roles run concurrently on different chunks: the copies of the next
 // chunks, the transforms of the current one and the stencils of the rows it
 // completes overlap.  Every halo row is loaded and transformed once per
-// strip.  Five warps per SM sub-partition.
+// strip.  Four warps per SM sub-partition.
 //
 // Every wait on an mbarrier gives up after kStreamWaitNs: the waiting role
 // raises the CTA's abort flag and records an error code that the host reads
@@ -34,7 +35,7 @@ constexpr int kStreamChunk = 16;                            // rows per copy
 constexpr int kStreamStages = 4;                            // ring stages
 constexpr int kStreamRing = kStreamChunk * kStreamStages;  // ring rows
 constexpr int kStreamTWarps = 8;
-constexpr int kStreamSWarps = 8;
+constexpr int kStreamSWarps = 4;
 constexpr int kStreamPWarps = 4;  // producer warpgroup (one thread loads)
 constexpr int kStreamThreads = 32 * (kStreamTWarps + kStreamSWarps + kStreamPWarps);
 constexpr int kStreamTThreads = 32 * kStreamTWarps;
@@ -45,18 +46,20 @@ static_assert(kStreamNep == kStreamMaxEll, "ell lanes");
 static_assert(kStreamMaxTheta == kStreamMaxNodes, "node tiles");
 static_assert(kStripMinRows >= 2 * 17, "strip edges clear of closures");
 static_assert(kCoefRecord == kCoefCount, "coefficient record");
-static_assert(kStreamSThreads == kStreamNep * kStreamChunk,
-              "one stencil thread per (row, ell) of a chunk");
+static_assert(2 * kStreamSThreads == kStreamNep * kStreamChunk,
+              "one stencil thread per (row pair, ell) of a chunk");
 static_assert(kStreamTWarps == 2 * kStreamBlocks, "two warps per block");
 // Register split between the warpgroups (setmaxnreg): the launch gives
-// every thread 96 registers; the producer warpgroup drops to 24, the
-// transform warpgroups raise theirs to 128 (their MMA fragments and
-// accumulators stay in registers) and the stencil warpgroups keep 96.
-// 128 x 24 + 256 x 128 + 256 x 96 = 60416 <= 640 x 96, so the raise is
-// always satisfiable; the launcher checks the launch allocation.
-constexpr int kStreamLaunchRegs = 96;
+// every thread 128 registers; the producer warpgroup drops to 24, the
+// transform warpgroups keep 128 (their MMA fragments and accumulators stay
+// in registers) and the stencil warpgroup raises its count to 232 (two rows'
+// terms, one 14-row window and the loads hoisted ahead of their use; from
+// 184 up nothing spills, and more is faster).  128 x 24 + 256 x 128 +
+// 128 x 232 = 65536 = 512 x 128, so the raise is always satisfiable; the
+// launcher checks the launch allocation.
+constexpr int kStreamLaunchRegs = 128;
 constexpr int kStreamTRegs = 128;
-constexpr int kStreamSRegs = 96;
+constexpr int kStreamSRegs = 232;
 constexpr int kStreamPRegs = 24;
 constexpr int kStreamRegisterDemand =
     kStreamTThreads * kStreamTRegs + kStreamSThreads * kStreamSRegs +
@@ -730,7 +733,181 @@ __device__ __forceinline__ void stream_rk_update(
   }
 }
 
-// One thread per (output row, ell): all three fields, no exchange.
+// Interior-row terms of the Teukolsky RHS: centre values, dissipation sums
+// (centre tap first, then k = P..1) and derivative sums (k = HALF..1).
+// A row gets the same sums, in the same order, alone or in a pair.
+struct StencilTerms {
+  double2 psi, Q, pt, qe;  // qe: effective Q (stage-constrained)
+  double2 spsi, sQ, sP;    // dissipation sums
+  double2 dpsi, dq, dpt;   // derivative sums (dq: of Q or of the effective Q)
+};
+
+template <int DISC, int N>
+__device__ __forceinline__ double2 taps_dissipation(const double2 (&w)[N],
+                                                    const int c) {
+  using T = DiscTraits<DISC>;
+  double2 acc = cscale(c_sbp.diss_interior[DISC][0], w[c]);
+#pragma unroll
+  for (int k = T::P; k >= 1; --k) {
+    acc = cfma(c_sbp.diss_interior[DISC][k], cadd(w[c + k], w[c - k]), acc);
+  }
+  return acc;
+}
+
+template <int DISC, int N>
+__device__ __forceinline__ double2 taps_derivative(const double2 (&w)[N],
+                                                   const int c) {
+  using T = DiscTraits<DISC>;
+  double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+  for (int k = T::HALF; k >= 1; --k) {
+    acc = cfma(c_sbp.interior[DISC][k], csub(w[c + k], w[c - k]), acc);
+  }
+  return acc;
+}
+
+// Terms of interior rows r and r + 1: one window of 2P + 2 ring rows per
+// field serves both rows (12 of the 14 rows overlap for D10-5).
+template <int DISC, int SC>
+__device__ __forceinline__ void pair_terms(
+    StencilTerms (&t)[2], const double2* cpsi, const double2* cQ,
+    const double2* cP, const double2* cpt, const double2* cqe, const int r,
+    const int shift, const int rs) {
+  using T = DiscTraits<DISC>;
+  constexpr int P = T::P, HD = T::HALF, N = 2 * P + 2, M = 2 * HD + 2;
+  int rows[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) rows[i] = ring_row(r - P + i, shift);
+  {
+    double2 w[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) w[i] = cpsi[rows[i] * rs];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      t[j].psi = w[P + j];
+      t[j].spsi = taps_dissipation<DISC>(w, P + j);
+      t[j].dpsi = taps_derivative<DISC>(w, P + j);
+    }
+  }
+  {
+    double2 w[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) w[i] = cQ[rows[i] * rs];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      t[j].Q = w[P + j];
+      t[j].sQ = taps_dissipation<DISC>(w, P + j);
+      if (!SC) t[j].dq = taps_derivative<DISC>(w, P + j);
+    }
+  }
+  {
+    double2 w[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) w[i] = cP[rows[i] * rs];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) t[j].sP = taps_dissipation<DISC>(w, P + j);
+  }
+  {
+    double2 w[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) w[i] = cpt[rows[P - HD + i] * kStreamNep];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      t[j].pt = w[HD + j];
+      t[j].dpt = taps_derivative<DISC>(w, HD + j);
+    }
+  }
+  if (SC) {
+    double2 w[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) w[i] = cqe[rows[P - HD + i] * kStreamNep];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      t[j].qe = w[HD + j];
+      t[j].dq = taps_derivative<DISC>(w, HD + j);
+    }
+  } else {
+    t[0].qe = t[1].qe = make_double2(0.0, 0.0);
+  }
+}
+
+// Terms of one interior row (the same sums as pair_terms gives it).
+template <int DISC, int SC>
+__device__ __forceinline__ void row_terms(
+    StencilTerms& t, const double2* cpsi, const double2* cQ,
+    const double2* cP, const double2* cpt, const double2* cqe, const int r,
+    const int shift, const int rs) {
+  using T = DiscTraits<DISC>;
+  constexpr int P = T::P, HD = T::HALF, N = 2 * P + 1, M = 2 * HD + 1;
+  int rows[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) rows[i] = ring_row(r - P + i, shift);
+  {
+    double2 w[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) w[i] = cpsi[rows[i] * rs];
+    t.psi = w[P];
+    t.spsi = taps_dissipation<DISC>(w, P);
+    t.dpsi = taps_derivative<DISC>(w, P);
+  }
+  {
+    double2 w[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) w[i] = cQ[rows[i] * rs];
+    t.Q = w[P];
+    t.sQ = taps_dissipation<DISC>(w, P);
+    if (!SC) t.dq = taps_derivative<DISC>(w, P);
+  }
+  {
+    double2 w[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) w[i] = cP[rows[i] * rs];
+    t.sP = taps_dissipation<DISC>(w, P);
+  }
+  {
+    double2 w[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) w[i] = cpt[rows[P - HD + i] * kStreamNep];
+    t.pt = w[HD];
+    t.dpt = taps_derivative<DISC>(w, HD);
+  }
+  if (SC) {
+    double2 w[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) w[i] = cqe[rows[P - HD + i] * kStreamNep];
+    t.qe = w[HD];
+    t.dq = taps_derivative<DISC>(w, HD);
+  } else {
+    t.qe = make_double2(0.0, 0.0);
+  }
+}
+
+// RHS of an interior row from its terms: psi -> D psi (constraint),
+// dissipation, (c_psi + lambda) psi; psi_t -> D psi_t into Q_t, psi_t
+// itself; Q -> -gamma Q, dissipation, H_R D Q + q Q with Q the evolved Q
+// (free-damped) or the effective Q (stage-constrained); P -> dissipation.
+template <int SC>
+__device__ __forceinline__ void assemble_interior(
+    const StencilTerms& t, const double* cf, const double mm,
+    const double lambda, const double damping, const double inv_h,
+    const double diss_scale, const bool dissipate, double2& kP, double2& kQ,
+    double2& kpsi) {
+  kQ = cscale(damping, cscale(inv_h, t.dpsi));
+  kpsi = dissipate ? cscale(diss_scale, t.spsi) : make_double2(0.0, 0.0);
+  kP = cadd(cmul(make_double2(cf[7], mm * cf[8]), t.psi),
+            cscale(lambda, t.psi));
+  kQ = cadd(kQ, cscale(inv_h, t.dpt));
+  kpsi = cadd(kpsi, t.pt);
+  kQ = csub(kQ, cscale(damping, t.Q));
+  if (dissipate) kQ = cfma(diss_scale, t.sQ, kQ);
+  const double2 qp = SC ? t.qe : t.Q;
+  kP = cadd(kP, cadd(cscale(cf[2], cscale(inv_h, t.dq)),
+                     cmul(make_double2(cf[5], mm * cf[6]), qp)));
+  if (dissipate) kP = cfma(diss_scale, t.sP, kP);
+}
+
+// One thread per (output row pair, ell): all three fields of two adjacent
+// rows, no exchange.
 template <int DISC, int SC>
 __device__ void stream_stencil(const StageLaunch& p,
                                unsigned long long* ready,
@@ -742,7 +919,7 @@ __device__ void stream_stencil(const StageLaunch& p,
   using T = DiscTraits<DISC>;
   constexpr int P = T::P, HD = T::HALF;
   constexpr int H = SC ? (P > 2 * HD ? P : 2 * HD) : P;
-  const int rrow = st / kStreamNep;  // row within a 16-row block
+  const int pair = st / kStreamNep;  // row pair within a 16-row block
   const int l = st % kStreamNep;
   int g = 0;
   int published = 0;  // chunks handed back so far
@@ -787,94 +964,72 @@ __device__ void stream_stencil(const StageLaunch& p,
         pe = min(sg.t1, u_end);
       }
       lim = min(lim, computable_end(pe, nr, T::HALF, T::W, T::BR));
-      for (int r = out_done + rrow; r < lim; r += kStreamChunk) {
+      for (int r = out_done + 2 * pair; r < lim; r += kStreamChunk) {
         if (l >= ne) continue;
-        const int rr = ring_row(r, sg.shift);
-        const double* cf = CF + rr * kCoefCount;
-        double2 kP, kQ, kpsi;
-        if (r >= T::BR && r + T::BR < nr) {
-          // One pass over the tap offsets k = P..1: the two ring rows r +- k
-          // are addressed once for every field; dissipation taps of psi, Q,
-          // P at every k, derivative taps of psi, Q (or effective Q) and
-          // psi_t for k <= HALF.  Seven independent accumulations.
-          const double2 psi = cpsi[rr * rs];
-          const double2 Q = cQ[rr * rs];
-          const double e0 = c_sbp.diss_interior[DISC][0];
-          double2 spsi = cscale(e0, psi), sQ = cscale(e0, Q),
-                  sP = cscale(e0, cP[rr * rs]);
-          double2 dpsi = make_double2(0.0, 0.0), dq = dpsi, dpt = dpsi;
+        const int count = r + 1 < lim ? 2 : 1;  // rows r, r + 1 of this pass
+        auto update = [&](const int q, const double2 kP, const double2 kQ,
+                          const double2 kpsi) {
+          const long long gi =
+              sg.seg_offset + static_cast<long long>(q) * rs + l;
+          const int ri = ring_row(q, sg.shift) * rs + l;
+          stream_rk_update(p, sg, X, A, gi, ri, kP, dt, dt6);
+          stream_rk_update(p, sg, X, A, gi + ne, ri + ne, kQ, dt, dt6);
+          stream_rk_update(p, sg, X, A, gi + 2 * ne, ri + 2 * ne, kpsi, dt,
+                           dt6);
+        };
+        if (count == 2 && r >= T::BR && r + 1 + T::BR < nr) {
+          // two interior rows from one register window per field
+          StencilTerms t[2];
+          pair_terms<DISC, SC>(t, cpsi, cQ, cP, cpt, cqe, r, sg.shift, rs);
 #pragma unroll
-          for (int k = P; k >= 1; --k) {
-            const int ra = ring_row(r + k, sg.shift);
-            const int rb = ring_row(r - k, sg.shift);
-            const double ek = c_sbp.diss_interior[DISC][k];
-            const double2 pa = cpsi[ra * rs], pb = cpsi[rb * rs];
-            const double2 qa = cQ[ra * rs], qb = cQ[rb * rs];
-            const double2 fa = cP[ra * rs], fb = cP[rb * rs];
-            spsi = cfma(ek, cadd(pa, pb), spsi);
-            sQ = cfma(ek, cadd(qa, qb), sQ);
-            sP = cfma(ek, cadd(fa, fb), sP);
-            if (k <= HD) {
-              const double ck = c_sbp.interior[DISC][k];
-              dpsi = cfma(ck, csub(pa, pb), dpsi);
-              dpt = cfma(ck, csub(cpt[ra * kStreamNep], cpt[rb * kStreamNep]),
-                         dpt);
-              if (SC) {
-                dq = cfma(ck, csub(cqe[ra * kStreamNep], cqe[rb * kStreamNep]),
-                          dq);
-              } else {
-                dq = cfma(ck, csub(qa, qb), dq);
-              }
+          for (int j = 0; j < 2; ++j) {
+            double2 kP, kQ, kpsi;
+            assemble_interior<SC>(t[j],
+                                  CF + ring_row(r + j, sg.shift) * kCoefCount,
+                                  mm, lambda, damping, inv_h, diss_scale,
+                                  dissipate, kP, kQ, kpsi);
+            update(r + j, kP, kQ, kpsi);
+          }
+          continue;
+        }
+#pragma unroll 1
+        for (int q = r; q < r + count; ++q) {
+          const int rr = ring_row(q, sg.shift);
+          const double* cf = CF + rr * kCoefCount;
+          double2 kP, kQ, kpsi;
+          if (q >= T::BR && q + T::BR < nr) {
+            StencilTerms t;
+            row_terms<DISC, SC>(t, cpsi, cQ, cP, cpt, cqe, q, sg.shift, rs);
+            assemble_interior<SC>(t, cf, mm, lambda, damping, inv_h,
+                                  diss_scale, dissipate, kP, kQ, kpsi);
+          } else {  // closure rows
+            const double2 psi = cpsi[rr * rs];
+            const double2 Q = cQ[rr * rs];
+            kQ = cadd(cscale(damping, cscale(inv_h, edge_derivative<DISC>(
+                                                        cpsi, q, nr, sg.shift, rs))),
+                      cscale(inv_h, edge_derivative<DISC>(cpt, q, nr, sg.shift,
+                                                          kStreamNep)));
+            kQ = csub(kQ, cscale(damping, Q));
+            kpsi = cpt[rr * kStreamNep];
+            kP = cadd(cmul(make_double2(cf[7], mm * cf[8]), psi),
+                      cscale(lambda, psi));
+            const double2 qp = SC ? cqe[rr * kStreamNep] : Q;
+            const double2 dq =
+                SC ? edge_derivative<DISC>(cqe, q, nr, sg.shift, kStreamNep)
+                   : edge_derivative<DISC>(cQ, q, nr, sg.shift, rs);
+            kP = cadd(kP, cadd(cscale(cf[2], cscale(inv_h, dq)),
+                               cmul(make_double2(cf[5], mm * cf[6]), qp)));
+            if (dissipate) {
+              kpsi = cfma(diss_scale,
+                          edge_dissipation<DISC>(cpsi, q, nr, sg.shift, rs), kpsi);
+              kQ = cfma(diss_scale,
+                        edge_dissipation<DISC>(cQ, q, nr, sg.shift, rs), kQ);
+              kP = cfma(diss_scale,
+                        edge_dissipation<DISC>(cP, q, nr, sg.shift, rs), kP);
             }
           }
-          // psi: D psi (constraint), dissipation, (c_psi + lambda) psi
-          kQ = cscale(damping, cscale(inv_h, dpsi));
-          kpsi = dissipate ? cscale(diss_scale, spsi) : make_double2(0.0, 0.0);
-          kP = cadd(cmul(make_double2(cf[7], mm * cf[8]), psi),
-                    cscale(lambda, psi));
-          // psi_t: D psi_t into Q_t, psi_t itself
-          kQ = cadd(kQ, cscale(inv_h, dpt));
-          kpsi = cadd(kpsi, cpt[rr * kStreamNep]);
-          // Q: -gamma Q, dissipation; H_R D Q + q Q with Q the evolved Q
-          // (free-damped) or the effective Q = D psi (stage-constrained)
-          kQ = csub(kQ, cscale(damping, Q));
-          if (dissipate) kQ = cfma(diss_scale, sQ, kQ);
-          const double2 qp = SC ? cqe[rr * kStreamNep] : Q;
-          kP = cadd(kP, cadd(cscale(cf[2], cscale(inv_h, dq)),
-                             cmul(make_double2(cf[5], mm * cf[6]), qp)));
-          if (dissipate) kP = cfma(diss_scale, sP, kP);
-        } else {  // closure rows
-          const double2 psi = cpsi[rr * rs];
-          const double2 Q = cQ[rr * rs];
-          kQ = cadd(cscale(damping, cscale(inv_h, edge_derivative<DISC>(
-                                                      cpsi, r, nr, sg.shift, rs))),
-                    cscale(inv_h, edge_derivative<DISC>(cpt, r, nr, sg.shift,
-                                                        kStreamNep)));
-          kQ = csub(kQ, cscale(damping, Q));
-          kpsi = cpt[rr * kStreamNep];
-          kP = cadd(cmul(make_double2(cf[7], mm * cf[8]), psi),
-                    cscale(lambda, psi));
-          const double2 qp = SC ? cqe[rr * kStreamNep] : Q;
-          const double2 dq =
-              SC ? edge_derivative<DISC>(cqe, r, nr, sg.shift, kStreamNep)
-                 : edge_derivative<DISC>(cQ, r, nr, sg.shift, rs);
-          kP = cadd(kP, cadd(cscale(cf[2], cscale(inv_h, dq)),
-                             cmul(make_double2(cf[5], mm * cf[6]), qp)));
-          if (dissipate) {
-            kpsi = cfma(diss_scale,
-                        edge_dissipation<DISC>(cpsi, r, nr, sg.shift, rs), kpsi);
-            kQ = cfma(diss_scale,
-                      edge_dissipation<DISC>(cQ, r, nr, sg.shift, rs), kQ);
-            kP = cfma(diss_scale,
-                      edge_dissipation<DISC>(cP, r, nr, sg.shift, rs), kP);
-          }
+          update(q, kP, kQ, kpsi);
         }
-        const long long gi =
-            sg.seg_offset + static_cast<long long>(r) * rs + l;
-        const int ri = rr * rs + l;
-        stream_rk_update(p, sg, X, A, gi, ri, kP, dt, dt6);
-        stream_rk_update(p, sg, X, A, gi + ne, ri + ne, kQ, dt, dt6);
-        stream_rk_update(p, sg, X, A, gi + 2 * ne, ri + 2 * ne, kpsi, dt, dt6);
       }
       out_done = max(out_done, lim);
       // rows below `bound` are read by no later work of this strip
