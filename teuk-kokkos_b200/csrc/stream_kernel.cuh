@@ -41,6 +41,10 @@ constexpr int kStreamThreads = 32 * (kStreamTWarps + kStreamSWarps + kStreamPWar
 constexpr int kStreamTThreads = 32 * kStreamTWarps;
 constexpr int kStreamSThreads = 32 * kStreamSWarps;
 constexpr int kStreamBlocks = 4;  // 4-row transform blocks per 16 rows
+// Named barriers: 1 all transform warps, 2 the stencil warps, 3 + b the two
+// warps of transform block b.
+constexpr int kStreamBlockBar = 3;
+static_assert(kStreamBlockBar + kStreamBlocks <= 16, "named barrier ids");
 constexpr unsigned long long kStreamWaitNs = 2000000000ull;
 static_assert(kStreamNep == kStreamMaxEll, "ell lanes");
 static_assert(kStreamMaxTheta == kStreamMaxNodes, "node tiles");
@@ -481,14 +485,14 @@ struct PsiFragments {
 
 // psi_t of the 4-row block at q0 (rows >= qlim skipped): this warp's half
 // of the synthesis and of the analysis.  xw / tw are the block's staging
-// buffers, shared with the partner warp; `bar` synchronises the 256
-// transform threads between the phases.
+// buffers, shared with the partner warp; named barrier `bar` (one per
+// block) synchronises the block's two warps between the phases.
 template <int SC>
 __device__ __forceinline__ void stream_psi_half(
     const int q0, const int qlim, const int h, const StripGeom& sg,
     const double2* U, const double2* QE, const double* CF, const double* NI,
     double2* PS, double* xw, double* tw, const PsiFragments& F,
-    const int mts, const int ksa, const int lane) {
+    const int mts, const int ksa, const int bar, const int lane) {
   const int quad = lane & 3;
   const int group = lane >> 2;
   const int ne = sg.ne;
@@ -512,7 +516,7 @@ __device__ __forceinline__ void stream_psi_half(
     xw[(rho * 4 + 2) * kStreamXs + l] = psi.x;
     xw[(rho * 4 + 3) * kStreamXs + l] = psi.y;
   }
-  named_sync(1, kStreamTThreads);
+  named_sync(bar, 64);
   double bx[2][4];
 #pragma unroll
   for (int n = 0; n < 2; ++n) {
@@ -555,7 +559,7 @@ __device__ __forceinline__ void stream_psi_half(
       }
     }
   }
-  named_sync(1, kStreamTThreads);
+  named_sync(bar, 64);
   double c[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
 #pragma unroll
   for (int ks = 0; ks < 8; ++ks) {
@@ -678,7 +682,7 @@ __device__ void stream_transform(const StageLaunch& p,
         if (kerr) {
           for (int q = pd; q < pe; q += 4 * kStreamBlocks) {
             stream_psi_half<SC>(q + 4 * blk, pe, h, sg, U, QE, CF, NI, PS, xw,
-                                tw, F, mts, ksa, lane);
+                                tw, F, mts, ksa, kStreamBlockBar + blk, lane);
           }
         } else {
           const int items = (pe - pd) * kStreamNep;
