@@ -402,7 +402,12 @@ int teuk_b200_resolved_config(const char* text, const char* const* overrides,
  * admitted solve keeps its state on the device and advances inside the
  * shared batched RK4 step; a solve that reaches its step count leaves the
  * batch with its endpoint waveform records, and its memory and tile slots
- * go to the next queued requests.  Linear (disabled-source) solves only. */
+ * go to the next queued requests.  Linear (disabled-source) solves only.
+ * Device memory: every buffer of the batch comes from the server's own
+ * CUDA memory pool (stream-ordered on the server's stream), warmed with
+ * min(budget, 4 GiB) at creation; memory a layout change frees stays in the
+ * pool until teuk_b200_server_destroy, so a membership change makes no
+ * driver allocation and no device-wide free. */
 typedef struct teuk_b200_server teuk_b200_server;
 
 typedef struct teuk_b200_server_options {

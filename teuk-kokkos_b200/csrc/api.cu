@@ -128,14 +128,19 @@ struct DeviceArray {
   T* ptr = nullptr;
   size_t count = 0;
   bool owned = true;  // false: memory lent by a longer-lived owner
+  // non-null: allocated from a memory pool, freed stream-ordered on this
+  // stream (the stream every use of the memory is ordered on)
+  cudaStream_t pool_stream = nullptr;
   DeviceArray() = default;
   DeviceArray(const DeviceArray&) = delete;
   DeviceArray& operator=(const DeviceArray&) = delete;
   DeviceArray(DeviceArray&& other) noexcept
-      : ptr(other.ptr), count(other.count), owned(other.owned) {
+      : ptr(other.ptr), count(other.count), owned(other.owned),
+        pool_stream(other.pool_stream) {
     other.ptr = nullptr;
     other.count = 0;
     other.owned = true;
+    other.pool_stream = nullptr;
   }
   DeviceArray& operator=(DeviceArray&& other) noexcept {
     if (this != &other) {
@@ -143,9 +148,11 @@ struct DeviceArray {
       ptr = other.ptr;
       count = other.count;
       owned = other.owned;
+      pool_stream = other.pool_stream;
       other.ptr = nullptr;
       other.count = 0;
       other.owned = true;
+      other.pool_stream = nullptr;
     }
     return *this;
   }
@@ -156,6 +163,16 @@ struct DeviceArray {
           "cudaMalloc");
     count = n;
   }
+  void allocate_from_pool(const size_t n, cudaMemPool_t pool,
+                          cudaStream_t stream) {
+    release();
+    if (n == 0) return;
+    check(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ptr),
+                                  n * sizeof(T), pool, stream),
+          "cudaMallocFromPoolAsync");
+    count = n;
+    pool_stream = stream;
+  }
   void borrow(T* p, const size_t n) {
     release();
     ptr = p;
@@ -163,23 +180,47 @@ struct DeviceArray {
     owned = false;
   }
   void release() {
-    if (ptr != nullptr && owned) cudaFree(ptr);
+    if (ptr != nullptr && owned) {
+      if (pool_stream != nullptr) {
+        cudaFreeAsync(ptr, pool_stream);
+      } else {
+        cudaFree(ptr);
+      }
+    }
     ptr = nullptr;
     count = 0;
     owned = true;
+    pool_stream = nullptr;
   }
   ~DeviceArray() { release(); }
 };
 
 // Band buffers that outlive one batch layout: two state buffers (the live
 // one and the next layout's) and the three RK slope buffers, grown on
-// demand and lent to each Batch a server builds.
+// demand and lent to each Batch a server builds.  With a pool, growth is a
+// stream-ordered pool allocation: the pool keeps freed blocks (release
+// threshold: never), so a layout change does not return memory to the
+// driver or wait on a device-wide free.  Capacity grows geometrically (at
+// least doubling), capped at what the HBM budget lets one buffer hold.
 struct StateArena {
   DeviceArray<double2> y[2];
   DeviceArray<double2> kA, kB, acc;
-  int current = 0;  // y[current] holds the live batch's state
-  static void grow(DeviceArray<double2>& a, const size_t n) {
-    if (a.count < n) a.allocate(n + n / 4);
+  int current = 0;                // y[current] holds the live batch's state
+  cudaMemPool_t pool = nullptr;   // null: plain cudaMalloc
+  cudaStream_t stream = nullptr;  // every use of the buffers is ordered on it
+  size_t cap = ~size_t{0};        // complex values one buffer may grow to
+  void grow(DeviceArray<double2>& a, const size_t n) {
+    if (a.count >= n) return;
+    const size_t want =
+        std::max(n, std::min(std::max(n + n / 4, 2 * a.count), cap));
+    if (pool != nullptr) {
+      a.allocate_from_pool(want, pool, stream);
+    } else {
+      a.allocate(want);
+    }
+  }
+  void release() {
+    for (auto* a : {&y[0], &y[1], &kA, &kB, &acc}) a->release();
   }
 };
 
@@ -233,6 +274,10 @@ struct Batch {
 
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
+  // a server's memory pool and stream (null: cudaMalloc): where the
+  // batch's device buffers come from
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t pool_stream = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   cudaStream_t graph_stream = nullptr;
@@ -258,8 +303,19 @@ struct Batch {
   }
 
   double2* nodal_scratch() {
-    if (d_nodal.ptr == nullptr) d_nodal.allocate(nodal_max);
+    if (d_nodal.ptr == nullptr) alloc(d_nodal, nodal_max);
     return d_nodal.ptr;
+  }
+
+  // A device buffer of this batch: from the server's pool (stream-ordered
+  // on the server's stream, the stream this batch runs on) or cudaMalloc.
+  template <class T>
+  void alloc(DeviceArray<T>& a, const size_t n) {
+    if (pool != nullptr) {
+      a.allocate_from_pool(n, pool, pool_stream);
+    } else {
+      a.allocate(n);
+    }
   }
 
   // Layout and device buffers for already validated plans.  With an arena
@@ -413,13 +469,19 @@ struct Batch {
       }
     }
 
-    // Device allocations.
+    // Device allocations: from the server's memory pool when a server
+    // builds the batch (no driver allocation or device-wide free on a
+    // layout change), plain cudaMalloc otherwise.
+    if (arena != nullptr && arena->pool != nullptr) {
+      pool = arena->pool;
+      pool_stream = arena->stream;
+    }
     if (arena != nullptr) {
       DeviceArray<double2>& next = arena->y[1 - arena->current];
-      StateArena::grow(next, total_complex);
-      StateArena::grow(arena->kA, total_complex);
-      StateArena::grow(arena->kB, total_complex);
-      StateArena::grow(arena->acc, total_complex);
+      arena->grow(next, total_complex);
+      arena->grow(arena->kA, total_complex);
+      arena->grow(arena->kB, total_complex);
+      arena->grow(arena->acc, total_complex);
       y.borrow(next.ptr, total_complex);
       kA.borrow(arena->kA.ptr, total_complex);
       kB.borrow(arena->kB.ptr, total_complex);
@@ -430,34 +492,37 @@ struct Batch {
       kB.allocate(total_complex);
       acc.allocate(total_complex);
     }
-    check(cudaMemset(y.ptr, 0, total_complex * sizeof(double2)), "memset y");
-    d_inst.allocate(h_inst.size());
-    d_seg.allocate(h_seg.size());
-    d_seg_mode.allocate(seg_mode.size());
-    d_tiles.allocate(h_tiles.size());
-    d_strips.allocate(std::max<size_t>(h_strips.size(), 1));
-    d_error.allocate(1);
-    check(cudaMemset(d_error.ptr, 0, sizeof(int)), "memset error word");
-    d_coef.allocate(static_cast<size_t>(std::max(coef_rows, 1)) * kCoefRecord);
-    d_nodes.allocate(static_cast<size_t>(std::max(coef_rows, 1)) * kNodeRecord);
-    d_mat.allocate(std::max<size_t>(h_mat.size(), 1));
-    d_trig.allocate(h_trig.size());
     nodal_max = 0;
     for (const InstancePlan& plan : plans) {
       nodal_max = std::max(nodal_max, plan.value_count());
     }
-    d_endpoint.allocate(std::max<size_t>(h_seg.size(), 1) * 2 *
-                        static_cast<size_t>(max_ell));
     std::vector<int> mask;
     for (const InstancePlan& plan : plans) {
       parent_mask_offset.push_back(mask.size());
       for (const ModePlan& mp : plan.modes) mask.push_back(mp.parent ? 1 : 0);
     }
-    d_parent_mask.allocate(mask.size());
+    alloc(d_inst, h_inst.size());
+    alloc(d_seg, h_seg.size());
+    alloc(d_seg_mode, seg_mode.size());
+    alloc(d_tiles, h_tiles.size());
+    alloc(d_strips, std::max<size_t>(h_strips.size(), 1));
+    alloc(d_error, 1);
+    alloc(d_coef, static_cast<size_t>(std::max(coef_rows, 1)) * kCoefRecord);
+    alloc(d_nodes, static_cast<size_t>(std::max(coef_rows, 1)) * kNodeRecord);
+    alloc(d_mat, std::max<size_t>(h_mat.size(), 1));
+    alloc(d_trig, h_trig.size());
+    alloc(d_endpoint,
+          std::max<size_t>(h_seg.size(), 1) * 2 * static_cast<size_t>(max_ell));
+    alloc(d_parent_mask, mask.size());
+    alloc(d_flag, 1);
+    // pool memory is usable from every stream once the allocating stream
+    // has been reached
+    if (pool != nullptr) check(cudaStreamSynchronize(pool_stream), "pool allocations");
+    check(cudaMemset(y.ptr, 0, total_complex * sizeof(double2)), "memset y");
+    check(cudaMemset(d_error.ptr, 0, sizeof(int)), "memset error word");
     check(cudaMemcpy(d_parent_mask.ptr, mask.data(), mask.size() * sizeof(int),
                      cudaMemcpyHostToDevice),
           "upload parent mask");
-    d_flag.allocate(1);
     frozen_dev.resize(plans.size());
     check(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking),
           "cudaStreamCreate");
@@ -636,7 +701,7 @@ struct Batch {
     check(cudaStreamSynchronize(stream), "set_state");
     auto& frozen = frozen_dev[static_cast<size_t>(instance)];
     if (flag != 0) {
-      if (frozen.count != count) frozen.allocate(count);
+      if (frozen.count != count) alloc(frozen, count);
       check(cudaMemcpyAsync(frozen.ptr, source, bytes, cudaMemcpyDeviceToDevice,
                             stream),
             "frozen copy");
@@ -823,9 +888,9 @@ struct Batch {
     DeviceArray<double2> d_seeds;
     DeviceArray<double> d_profile;
     DeviceArray<unsigned long long> d_worst;
-    d_seeds.allocate(seeds.size());
-    d_profile.allocate(profile.size());
-    d_worst.allocate(1);
+    alloc(d_seeds, seeds.size());
+    alloc(d_profile, profile.size());
+    alloc(d_worst, 1);
     check(cudaMemcpyAsync(d_seeds.ptr, seeds.data(), seeds.size() * sizeof(double2),
                           cudaMemcpyHostToDevice, stream),
           "upload seeds");
@@ -1224,12 +1289,40 @@ class Server {
     require_device();
     teuk_b200::check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking),
                      "cudaStreamCreate");
+    // The band arena's own memory pool: blocks it frees stay reserved for
+    // the next layout (no release back to the driver until the server
+    // ends).
+    int device = 0;
+    teuk_b200::check(cudaGetDevice(&device), "cudaGetDevice");
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    teuk_b200::check(cudaMemPoolCreate(&pool_, &props), "cudaMemPoolCreate");
+    unsigned long long keep = ~0ull;
+    teuk_b200::check(
+        cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep),
+        "memory pool release threshold");
+    arena_.pool = pool_;
+    arena_.stream = stream_;
+    arena_.cap = std::max<size_t>(
+        1, o.hbm_budget_bytes / (4 * sizeof(double2)));
+    // Warm the pool: map its first block now instead of inside the first
+    // layout changes (a driver allocation can take tens to hundreds of ms).
+    const size_t warm = std::min<size_t>(o.hbm_budget_bytes, size_t{4} << 30);
+    void* block = nullptr;
+    teuk_b200::check(cudaMallocFromPoolAsync(&block, warm, pool_, stream_),
+                     "memory pool warm-up");
+    teuk_b200::check(cudaFreeAsync(block, stream_), "memory pool warm-up");
+    teuk_b200::check(cudaStreamSynchronize(stream_), "memory pool warm-up");
   }
   ~Server() {
     batch_.reset();
+    arena_.release();  // stream-ordered frees into the pool
     if (stream_ != nullptr) cudaStreamSynchronize(stream_);
     for (cudaEvent_t e : events_) cudaEventDestroy(e);
     if (stream_ != nullptr) cudaStreamDestroy(stream_);
+    if (pool_ != nullptr) cudaMemPoolDestroy(pool_);
   }
 
   uint64_t submit(const teuk_b200_config& raw, const teuk_b200_gaussian& pulse,
@@ -1335,6 +1428,9 @@ class Server {
     for (const auto& r : active_) plans.push_back(r->plan);
     auto next = std::make_unique<Batch>();
     next->build_planned(std::move(plans), &arena_);
+    // the coefficient tables were computed on the batch's build stream:
+    // finish them before the server's stream takes over
+    teuk_b200::check(cudaStreamSynchronize(next->stream), "batch build");
     next->stream = stream_;
     for (size_t i = 0; i < active_.size(); ++i) {
       ServerRequest& r = *active_[i];
@@ -1432,6 +1528,7 @@ class Server {
   cudaStream_t stream_ = nullptr;
   std::vector<cudaEvent_t> events_;  // start / stop pairs of pending steps
   teuk_b200::StateArena arena_;      // band buffers reused across layouts
+  cudaMemPool_t pool_ = nullptr;     // the arena's memory pool
   int pending_ = 0;
   std::unique_ptr<Batch> batch_;
   std::deque<std::shared_ptr<ServerRequest>> queue_;
