@@ -334,6 +334,7 @@ struct AngularOpParams {
 __global__ void angular_op_kernel(const Geo g, const Trig tr,
                                   const AngularOpParams p) {
   __shared__ double2 modal[kBlock / 32][kMaxNodes];
+  __shared__ double2 row_in[kBlock / 32][kMaxNodes];  // the input row
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long rows = static_cast<long long>(g.modes) * g.nr;
   for (long long row = blockIdx.x * (kBlock / 32) + warp; row < rows;
@@ -345,13 +346,17 @@ __global__ void angular_op_kernel(const Geo g, const Trig tr,
       for (int j = lane; j < g.nt; j += 32) out[j] = make_double2(0.0, 0.0);
       continue;
     }
+    // one coalesced read of the input row (every lane needs all of it)
     const double2* in = p.in.at(g, mode, p.in_slot, r, 0);
+    double2* x = row_in[warp];
+    for (int j = lane; j < g.nt; j += 32) x[j] = in[j];
+    __syncwarp();
     const int ne = p.ne[mode];
     const double* A = p.pool + p.a_off[mode];
     const double* diag = p.pool + p.diag_off[mode];
     for (int l = lane; l < ne; l += 32) {
       C2 v = mk(0.0, 0.0);
-      for (int j = 0; j < g.nt; ++j) v = v + A[l * g.nt + j] * ld(in[j]);
+      for (int j = 0; j < g.nt; ++j) v = v + A[j * ne + l] * ld(x[j]);
       if (p.kind != kProject) v = diag[l] * v;
       modal[warp][l] = st(v);
     }
@@ -364,20 +369,21 @@ __global__ void angular_op_kernel(const Geo g, const Trig tr,
       C2 v = mk(0.0, 0.0);
       for (int l = 0; l < ne_o; ++l) {
         const int src = l + shift;  // align onto the output band
-        if (src >= 0 && src < ne) v = v + S[j * ne_o + l] * ld(modal[warp][src]);
+        if (src >= 0 && src < ne) v = v + S[l * g.nt + j] * ld(modal[warp][src]);
       }
       if (p.kind == kEth || p.kind == kEthPrime) {
         const double2* dtv = p.dt.at(g, mode, p.dt_slot, r, 0);
         const double R = g.spacing * static_cast<double>(r);
         v = p.kind == kEth
-                ? eth_point(g, ld(in[j]), ld(dtv[j]), v, p.spin, p.boost, R,
+                ? eth_point(g, ld(x[j]), ld(dtv[j]), v, p.spin, p.boost, R,
                             tr.grid_sin[j], tr.grid_cos[j])
-                : ethprime_point(g, ld(in[j]), ld(dtv[j]), v, p.spin,
+                : ethprime_point(g, ld(x[j]), ld(dtv[j]), v, p.spin,
                                  p.boost, R, tr.grid_sin[j], tr.grid_cos[j]);
       }
       result[k] = st(v);
     }
-    __syncwarp();  // every lane has read the input row (in-place projection)
+    // in-place projection: every lane read the input row before the stores;
+    // the next row's staging waits for every lane's reads of this one
     for (int k = 0, j = lane; j < g.nt; j += 32, ++k) out[j] = result[k];
     __syncwarp();
   }
@@ -1304,11 +1310,14 @@ void NodalPipeline::build_coordinators() {
       for (int l = 0; l < ne; ++l) {
         const double basis = spin_weighted_harmonic_theta(
             ell_min + l, m, spin, plan_.theta[static_cast<size_t>(j)]);
+        // stored so that a warp's lanes read consecutive entries: the
+        // analysis (lanes over ell) node-major, the synthesis (lanes over
+        // nodes) ell-major
         if (analysis) {
-          matrices_[static_cast<size_t>(off + l * nt + j)] =
+          matrices_[static_cast<size_t>(off + j * ne + l)] =
               2.0 * pi * plan_.weights[static_cast<size_t>(j)] * basis;
         } else {
-          matrices_[static_cast<size_t>(off + j * ne + l)] = basis;
+          matrices_[static_cast<size_t>(off + l * nt + j)] = basis;
         }
       }
     }
