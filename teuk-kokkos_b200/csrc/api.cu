@@ -246,6 +246,11 @@ struct Batch {
   std::vector<double> h_mat;
   std::vector<double> h_trig;
   std::vector<StageLaunch> groups;  // one per (disc, reduction)
+  // Launch groups of one stage touch disjoint segments: groups after the
+  // first run on these streams, forked from and joined back into `stream`
+  // (inside a captured step they become parallel graph branches).
+  std::vector<cudaStream_t> group_streams;
+  std::vector<cudaEvent_t> group_events;  // [0] fork, [i] join of stream i
   std::vector<int> group_first_tile;
   std::vector<TileDesc> h_strips;       // streaming-kernel strips
   std::vector<int> group_first_strip;   // -1: group runs the tile kernel
@@ -286,6 +291,8 @@ struct Batch {
   ~Batch() {
     if (graph_exec != nullptr) cudaGraphExecDestroy(graph_exec);
     if (graph != nullptr) cudaGraphDestroy(graph);
+    for (cudaStream_t s : group_streams) cudaStreamDestroy(s);
+    for (cudaEvent_t e : group_events) cudaEventDestroy(e);
     if (own_stream != nullptr) cudaStreamDestroy(own_stream);
   }
 
@@ -751,10 +758,38 @@ struct Batch {
   }
 
   void launch_stage_kind(const int kind, double2* input) {
-    for (StageLaunch g : groups) {
+    if (groups.size() <= 1) {
+      for (StageLaunch g : groups) {
+        g.stage = kind;
+        if (input != nullptr) g.y = input;
+        check(launch_stage(g, stream), "stage kernel");
+      }
+      return;
+    }
+    while (group_streams.size() + 1 < groups.size()) {
+      cudaStream_t s = nullptr;
+      check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking),
+            "cudaStreamCreate");
+      group_streams.push_back(s);
+    }
+    while (group_events.size() < groups.size()) {
+      cudaEvent_t e = nullptr;
+      check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming),
+            "cudaEventCreate");
+      group_events.push_back(e);
+    }
+    check(cudaEventRecord(group_events[0], stream), "fork");
+    for (size_t i = 0; i < groups.size(); ++i) {
+      StageLaunch g = groups[i];
       g.stage = kind;
       if (input != nullptr) g.y = input;
-      check(launch_stage(g, stream), "stage kernel");
+      cudaStream_t s = i == 0 ? stream : group_streams[i - 1];
+      if (i > 0) check(cudaStreamWaitEvent(s, group_events[0], 0), "fork");
+      check(launch_stage(g, s), "stage kernel");
+      if (i > 0) {
+        check(cudaEventRecord(group_events[i], s), "join");
+        check(cudaStreamWaitEvent(stream, group_events[i], 0), "join");
+      }
     }
   }
 
