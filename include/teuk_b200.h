@@ -226,9 +226,21 @@ int teuk_b200_step(teuk_b200_pipeline* pipeline, double time, double dt,
  * - The array is shared by every pipeline on a device: calls that overlap
  *   in time on one device (other threads, other streams) race on it.
  *   Serialize them.
- * - Nothing in the array needs to start at zero. */
+ * - Nothing in the array needs to start at zero.
+ * - The array's device address is cached per device for the life of the
+ *   process.  A cudaDeviceReset in the host process frees the array with
+ *   the context and leaves that address stale: do not call this entry
+ *   point on a device after resetting it. */
 int teuk_b200_step_static_scratch(teuk_b200_pipeline* pipeline, double time,
                                   double dt, int steps);
+
+/* Failure-detection test hook, not for production use.  Batches and
+ * pipelines built after a call with chunk >= 0 withhold that chunk from CTA
+ * 0 of their stage-1 streaming launches: the kernel's bounded waits for it
+ * run out (about 2 s) and the step reports TEUK_B200_ERR_CUDA ("stage kernel
+ * pipeline wait timed out") with the CUDA context still usable.  chunk = -1
+ * (the initial value) switches it off.  Process-wide. */
+int teuk_b200_test_withhold_chunk(int chunk);
 int teuk_b200_initialize_gaussian(teuk_b200_pipeline* pipeline,
                                   const teuk_b200_gaussian* pulse);
 /* Records for the scri then horizon endpoints of the first-order field and
@@ -307,6 +319,48 @@ int teuk_b200_footprint_bytes(const teuk_b200_config* config,
 /* ---- batched solves: one set of stage launches for all instances ----- */
 int teuk_b200_batch_create(const teuk_b200_config* configs, int count,
                            teuk_b200_batch** out);
+
+/* Launch choices of a batch.  None of them changes a result bit: bands do
+ * not couple, every radial row gets the same sums in the same order however
+ * the rows are split into strips, and the split-precision transforms are a
+ * separate, stated precision (TEUK_B200_PRECISION_SPLIT).  No counterpart in
+ * the reference (kernel selection and tuning of this engine). */
+enum teuk_b200_stage_kernel_choice {
+  TEUK_B200_KERNEL_AUTO = 0, /* streaming kernel for every band that fits */
+  TEUK_B200_KERNEL_TILE = 1  /* tile kernel for every band */
+};
+enum teuk_b200_precision {
+  /* FP64 transforms and ell-coupling (the reference's arithmetic) */
+  TEUK_B200_PRECISION_FP64 = 0,
+  /* split-precision tensor-core transforms: FP64 operands cut into BF16
+   * slices, FP32 accumulation, FP64 recombination; everything else FP64 */
+  TEUK_B200_PRECISION_SPLIT = 1
+};
+typedef struct teuk_b200_batch_options {
+  int abi_version;  /* TEUK_B200_ABI_VERSION */
+  int stage_kernel; /* teuk_b200_stage_kernel_choice */
+  int precision;    /* teuk_b200_precision */
+  /* streaming-kernel strip length in radial rows (0: the autotuner's or the
+   * built-in choice; otherwise at least 64) */
+  int strip_rows;
+  /* 1: time the candidate strip lengths of every streaming launch group at
+   * build and keep the fastest (cached per shape class for the process) */
+  int autotune;
+} teuk_b200_batch_options;
+/* teuk_b200_create with launch choices (one solve; the second-order
+ * pipeline reads `precision` only). */
+int teuk_b200_create_with_options(const teuk_b200_config* config,
+                                  const teuk_b200_batch_options* options,
+                                  teuk_b200_pipeline** out);
+int teuk_b200_batch_create_with_options(const teuk_b200_config* configs,
+                                        int count,
+                                        const teuk_b200_batch_options* options,
+                                        teuk_b200_batch** out);
+/* Strip length (rows) each streaming launch group of the batch uses, in
+ * launch-group order; `count` gets the number of groups written (at most
+ * `capacity`).  Groups that run the tile kernel report 0. */
+int teuk_b200_batch_strip_rows(const teuk_b200_batch* batch, int* rows,
+                               int capacity, int* count);
 int teuk_b200_batch_destroy(teuk_b200_batch* batch);
 int teuk_b200_batch_size(const teuk_b200_batch* batch, int* count);
 int teuk_b200_batch_shape(const teuk_b200_batch* batch, int instance,

@@ -3,7 +3,7 @@ radial strips, against the reference build and against the tile kernel.
 
 The engine runs launch groups with n_ell <= 16 and at most 32 Gauss-Legendre
 nodes through the streaming kernel (persistent CTAs, bulk-copy ring);
-TEUK_B200_STAGE_KERNEL=tile makes a pipeline built while it is set use the
+LaunchOptions(stage_kernel=KERNEL_TILE) makes a pipeline use the
 tile kernel instead.  Segments of one launch differ in n_ell (m = -4..4), so
 the ring also changes its row stride between strips.
 Tolerance: 1e-10 relative to the field's max norm against the reference;
@@ -77,13 +77,11 @@ def test_long_rk4_matches_reference(require_gpu, name):
 
 
 @pytest.mark.parametrize("name", sorted(LONG) + ["kerr_d105", "kerr_d42_sc"])
-def test_stream_kernel_equals_tile_kernel(require_gpu, monkeypatch, name):
+def test_stream_kernel_equals_tile_kernel(require_gpu, name):
     config = LONG.get(name, CASES.get(name))
     pulse = pulse_for(config, 5)
     stream = tb.Batch([config])
-    monkeypatch.setenv("TEUK_B200_STAGE_KERNEL", "tile")
-    tile = tb.Batch([config])
-    monkeypatch.delenv("TEUK_B200_STAGE_KERNEL")
+    tile = tb.Batch([config], tb.LaunchOptions(stage_kernel=tb.KERNEL_TILE))
     assert stream.stage_kernels() == (1, 0)
     assert tile.stage_kernels() == (0, 1)
     for p in (stream, tile):
@@ -140,18 +138,20 @@ def test_solve_split_between_stage_kernels(require_gpu):
         assert relative_error(g[:, f], r[:, f]) < TOL, f"field {f}"
 
 
-def test_stage_wait_timeout_is_reported(require_gpu, monkeypatch):
+def test_stage_wait_timeout_is_reported(require_gpu):
     """Failure detection without a GPU fault: with the test hook
-    TEUK_B200_WITHHOLD_CHUNK the producer of one CTA never loads a chunk in
+    teuk_b200_test_withhold_chunk the producer of one CTA never loads a chunk in
     stage-1 launches, so the transform warps' bounded wait runs out (2 s),
     every warp role leaves its loop, and the step reports the timeout.  The
     device context stays usable: a new pipeline then steps like the
     reference."""
     config = LONG["kerr_d105_long"]
     dt = step_size(config, 0.1)
-    monkeypatch.setenv("TEUK_B200_WITHHOLD_CHUNK", "2")
-    broken = tb.Pipeline(config)
-    monkeypatch.delenv("TEUK_B200_WITHHOLD_CHUNK")
+    tb.test_withhold_chunk(2)
+    try:
+        broken = tb.Pipeline(config)
+    finally:
+        tb.test_withhold_chunk(-1)
     broken.initialize_gaussian(pulse_for(config, 19))
     with pytest.raises(tb.TeukError, match="timed out"):
         broken.step(0.0, dt, 1)

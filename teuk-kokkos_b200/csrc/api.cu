@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <deque>
 #include <cmath>
@@ -34,6 +35,11 @@ namespace teuk_b200 {
 namespace {
 
 thread_local std::string g_last_error;
+
+// Failure-detection test hook (teuk_b200_test_withhold_chunk): the chunk
+// that CTA 0's producer skips in stage-1 launches of batches built while it
+// is set; -1 (the default) disables it.
+std::atomic<int> g_test_withhold_chunk{-1};
 
 struct CudaError : std::runtime_error {
   using std::runtime_error::runtime_error;
@@ -267,6 +273,10 @@ struct Batch {
   DeviceArray<double> d_coef;  // Teukolsky row coefficients per solve row
   DeviceArray<double> d_nodes;  // 1 / C_T on the nodes per solve row
   int withhold_chunk_ = -1;    // failure-detection test hook
+  teuk_b200_batch_options options{TEUK_B200_ABI_VERSION, TEUK_B200_KERNEL_AUTO,
+                                  TEUK_B200_PRECISION_FP64, 0, 0};
+  std::vector<int> group_strip_rows;  // strip length per group (0: tile)
+  int last_strip_rows_ = 0;           // target of the last plan_strips
   int coef_rows = 0;
   DeviceArray<double> d_mat, d_trig;
   DeviceArray<double2> d_nodal;     // one instance's nodal state (lazy)
@@ -410,11 +420,8 @@ struct Batch {
     // n_ell <= 16 of solves with at most 32 nodes run the streaming kernel
     // (radial strips), the others the tile kernel (radial tiles).  Segments
     // do not couple, so a solve may have segments in both.
-    const char* forced = std::getenv("TEUK_B200_STAGE_KERNEL");
-    const bool tile_only = forced != nullptr && std::string(forced) == "tile";
-    // failure-detection test hook (StageLaunch::withhold_chunk)
-    const char* withhold = std::getenv("TEUK_B200_WITHHOLD_CHUNK");
-    withhold_chunk_ = withhold != nullptr ? std::atoi(withhold) : -1;
+    const bool tile_only = options.stage_kernel == TEUK_B200_KERNEL_TILE;
+    withhold_chunk_ = g_test_withhold_chunk.load();
     const auto streamable = [&](const size_t s) {
       const InstanceDesc& in = h_inst[static_cast<size_t>(h_seg[s].instance)];
       return !tile_only && h_seg[s].n_ell <= kStreamMaxEll &&
@@ -469,6 +476,7 @@ struct Batch {
           g.strip_count = 0;
           group_first_strip.push_back(kind == 0 ? plan_strips(g, group_segments)
                                                 : -1);
+          group_strip_rows.push_back(kind == 0 ? last_strip_rows_ : 0);
           groups.push_back(g);
           group_first_tile.push_back(first_tile);
         }
@@ -605,8 +613,12 @@ struct Batch {
       rows += h_inst[static_cast<size_t>(h_seg[static_cast<size_t>(s)].instance)].nr;
     }
     const long long want = static_cast<long long>(std::max(sms, 1)) * kStripsPerCta;
-    const int target = static_cast<int>(std::min<long long>(
-        1024, std::max<long long>(kStripMinRows, rows / want)));
+    const int target =
+        options.strip_rows > 0
+            ? options.strip_rows
+            : static_cast<int>(std::min<long long>(
+                  1024, std::max<long long>(kStripMinRows, rows / want)));
+    last_strip_rows_ = target;
     std::stable_sort(segs.begin(), segs.end(), [&](const int a, const int b) {
       return h_seg[static_cast<size_t>(a)].n_ell > h_seg[static_cast<size_t>(b)].n_ell;
     });
@@ -1590,10 +1602,37 @@ const char* teuk_b200_last_error(void) {
 
 int teuk_b200_abi_version(void) { return TEUK_B200_ABI_VERSION; }
 
-int teuk_b200_create(const teuk_b200_config* config,
-                     teuk_b200_pipeline** out) {
+namespace {
+teuk_b200_batch_options checked_options(const teuk_b200_batch_options* o) {
+  teuk_b200_batch_options out{TEUK_B200_ABI_VERSION, TEUK_B200_KERNEL_AUTO,
+                              TEUK_B200_PRECISION_FP64, 0, 0};
+  if (o == nullptr) return out;
+  if (o->abi_version != TEUK_B200_ABI_VERSION) {
+    throw std::invalid_argument("teuk_b200_batch_options.abi_version mismatch");
+  }
+  if (o->stage_kernel != TEUK_B200_KERNEL_AUTO &&
+      o->stage_kernel != TEUK_B200_KERNEL_TILE) {
+    throw std::invalid_argument("unknown stage kernel choice");
+  }
+  if (o->precision != TEUK_B200_PRECISION_FP64 &&
+      o->precision != TEUK_B200_PRECISION_SPLIT) {
+    throw std::invalid_argument("unknown transform precision");
+  }
+  if (o->strip_rows != 0 && o->strip_rows < teuk_b200::kStripMinRows) {
+    throw std::invalid_argument("strip_rows must be 0 or at least 64");
+  }
+  if (o->autotune != 0 && o->autotune != 1) {
+    throw std::invalid_argument("autotune must be 0 or 1");
+  }
+  return *o;
+}
+
+int create_pipeline(const teuk_b200_config* config,
+                    const teuk_b200_batch_options* options,
+                    teuk_b200_pipeline** out) {
   return guarded([&] {
     require(config != nullptr && out != nullptr, "null argument");
+    const teuk_b200_batch_options opts = checked_options(options);
     auto p = std::make_unique<teuk_b200_pipeline>();
     const teuk_b200::Config c = teuk_b200::to_config(*config);
     if (c.source_mode != TEUK_B200_SOURCE_DISABLED) {
@@ -1602,9 +1641,29 @@ int teuk_b200_create(const teuk_b200_config* config,
       p->nodal = std::make_unique<teuk_b200::NodalPipeline>(plan);
     } else {
       p->batch = std::make_unique<Batch>();
+      p->batch->options = opts;
       p->batch->build({c});
     }
     *out = p.release();
+  });
+}
+}  // namespace
+
+int teuk_b200_create(const teuk_b200_config* config,
+                     teuk_b200_pipeline** out) {
+  return create_pipeline(config, nullptr, out);
+}
+
+int teuk_b200_create_with_options(const teuk_b200_config* config,
+                                  const teuk_b200_batch_options* options,
+                                  teuk_b200_pipeline** out) {
+  return create_pipeline(config, options, out);
+}
+
+int teuk_b200_test_withhold_chunk(int chunk) {
+  return guarded([&] {
+    require(chunk >= -1, "chunk must be -1 (off) or a chunk index");
+    teuk_b200::g_test_withhold_chunk.store(chunk);
   });
 }
 
@@ -2128,19 +2187,41 @@ int teuk_b200_footprint_bytes(const teuk_b200_config* config, size_t* bytes) {
   });
 }
 
-int teuk_b200_batch_create(const teuk_b200_config* configs, int count,
-                           teuk_b200_batch** out) {
+int teuk_b200_batch_create_with_options(const teuk_b200_config* configs,
+                                        int count,
+                                        const teuk_b200_batch_options* options,
+                                        teuk_b200_batch** out) {
   return guarded([&] {
     require(configs != nullptr && out != nullptr && count > 0,
             "null argument or empty batch");
+    const teuk_b200_batch_options opts = checked_options(options);
     std::vector<teuk_b200::Config> list;
     for (int i = 0; i < count; ++i) {
       list.push_back(teuk_b200::to_config(configs[i]));
     }
     auto b = std::make_unique<teuk_b200_batch>();
     b->batch = std::make_unique<Batch>();
+    b->batch->options = opts;
     b->batch->build(list);
     *out = b.release();
+  });
+}
+
+int teuk_b200_batch_create(const teuk_b200_config* configs, int count,
+                           teuk_b200_batch** out) {
+  return teuk_b200_batch_create_with_options(configs, count, nullptr, out);
+}
+
+int teuk_b200_batch_strip_rows(const teuk_b200_batch* b, int* rows,
+                               int capacity, int* count) {
+  return guarded([&] {
+    require(b != nullptr && count != nullptr && capacity >= 0 &&
+                (rows != nullptr || capacity == 0),
+            "null argument");
+    const auto& v = b->batch->group_strip_rows;
+    const int n = std::min(capacity, static_cast<int>(v.size()));
+    for (int i = 0; i < n; ++i) rows[i] = v[static_cast<size_t>(i)];
+    *count = static_cast<int>(v.size());
   });
 }
 

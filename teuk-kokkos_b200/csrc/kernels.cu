@@ -16,6 +16,8 @@
 //      84-128) in the same pass.
 // All arithmetic is binary64.
 #include <cstdio>
+#include <mutex>
+#include <unordered_map>
 
 #include "kernels.h"
 
@@ -963,41 +965,72 @@ __global__ void __launch_bounds__(kThreads, 2)
 
 #include "stream_kernel.cuh"
 
+// Launch set-up of one kernel on one device: the dynamic shared-memory
+// opt-in (an attribute of the function on each device), the SM count, the
+// registers the compiled kernel is launched with and the resident CTAs for
+// a shared-memory size.  Kept per device, because one process may run
+// pipelines on several devices, and behind a mutex, because several host
+// threads may launch at once.
+struct KernelSetup {
+  int configured_bytes = 0;
+  int sms = 0;
+  int launch_regs = -1;
+  size_t resident_bytes = 0;
+  int resident = 0;
+};
+
+class KernelSetups {
+ public:
+  // Runs `body(setup)` on the calling device's record under the lock.
+  template <class Body>
+  cudaError_t with(Body&& body) {
+    int device = 0;
+    const cudaError_t err = cudaGetDevice(&device);
+    if (err != cudaSuccess) return err;
+    std::lock_guard<std::mutex> lock(mutex_);
+    return body(per_device_[device], device);
+  }
+
+ private:
+  std::mutex mutex_;
+  std::unordered_map<int, KernelSetup> per_device_;
+};
+
 template <int DISC, int SC>
 cudaError_t launch_stream_typed(const StageLaunch& p, cudaStream_t stream) {
   const size_t bytes = StreamLayout(SC).total;
   auto kernel = stream_stage_kernel<DISC, SC>;
-  static int configured_bytes = 0;
-  static int sms = 0;
-  if (configured_bytes != static_cast<int>(bytes)) {
-    cudaError_t err = cudaFuncSetAttribute(
-        kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-        static_cast<int>(bytes));
-    if (err != cudaSuccess) return err;
-    configured_bytes = static_cast<int>(bytes);
-  }
-  if (sms == 0) {
-    int device = 0;
-    cudaError_t err = cudaGetDevice(&device);
-    if (err == cudaSuccess) {
-      err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount,
-                                   device);
+  static KernelSetups setups;
+  int sms = 0;
+  const cudaError_t setup_err = setups.with([&](KernelSetup& k, const int device) {
+    if (k.configured_bytes != static_cast<int>(bytes)) {
+      const cudaError_t err = cudaFuncSetAttribute(
+          kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+          static_cast<int>(bytes));
+      if (err != cudaSuccess) return err;
+      k.configured_bytes = static_cast<int>(bytes);
     }
-    if (err != cudaSuccess) return err;
-  }
-  // The warpgroups' setmaxnreg requests must fit the registers the CTA is
-  // launched with; a larger request would never be granted.
-  static int launch_regs = -1;
-  if (launch_regs < 0) {
-    cudaFuncAttributes attributes{};
-    const cudaError_t err = cudaFuncGetAttributes(&attributes, kernel);
-    if (err != cudaSuccess) return err;
-    launch_regs = attributes.numRegs;
-  }
-  if (launch_regs != kStreamLaunchRegs ||
-      launch_regs * kStreamThreads < kStreamRegisterDemand) {
-    return cudaErrorInvalidConfiguration;
-  }
+    if (k.sms == 0) {
+      const cudaError_t err = cudaDeviceGetAttribute(
+          &k.sms, cudaDevAttrMultiProcessorCount, device);
+      if (err != cudaSuccess) return err;
+    }
+    // The warpgroups' setmaxnreg requests must fit the registers the CTA
+    // is launched with; a larger request would never be granted.
+    if (k.launch_regs < 0) {
+      cudaFuncAttributes attributes{};
+      const cudaError_t err = cudaFuncGetAttributes(&attributes, kernel);
+      if (err != cudaSuccess) return err;
+      k.launch_regs = attributes.numRegs;
+    }
+    if (k.launch_regs != kStreamLaunchRegs ||
+        k.launch_regs * kStreamThreads < kStreamRegisterDemand) {
+      return cudaErrorInvalidConfiguration;
+    }
+    sms = k.sms;
+    return cudaSuccess;
+  });
+  if (setup_err != cudaSuccess) return setup_err;
   const int grid = p.strip_count < sms ? p.strip_count : sms;
   kernel<<<grid, kStreamThreads, bytes, stream>>>(p);
   return cudaGetLastError();
@@ -1010,34 +1043,35 @@ cudaError_t launch_typed(const StageLaunch& p, cudaStream_t stream) {
   }
   const size_t bytes = stage_smem_bytes(p);
   auto kernel = stage_kernel<DISC, SC>;
-  // The opt-in limit is raised once per instantiation to the largest size
-  // requested so far (never inside a launch sequence that needs less).
-  static int configured_bytes = 0;
-  if (static_cast<int>(bytes) > configured_bytes) {
-    cudaError_t err = cudaFuncSetAttribute(
-        kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-        static_cast<int>(bytes));
-    if (err != cudaSuccess) return err;
-    configured_bytes = static_cast<int>(bytes);
-  }
-  // resident CTAs for this shared-memory size, cached per size
-  static size_t resident_bytes = 0;
-  static int resident = 0;
-  if (bytes != resident_bytes) {
-    int device = 0, sms = 0, per_sm = 0;
-    cudaError_t err = cudaGetDevice(&device);
-    if (err == cudaSuccess) {
-      err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount,
-                                   device);
+  static KernelSetups setups;
+  int resident = 0;
+  const cudaError_t setup_err = setups.with([&](KernelSetup& k, const int device) {
+    // The opt-in limit is raised to the largest size requested so far on
+    // this device (never inside a launch sequence that needs less).
+    if (static_cast<int>(bytes) > k.configured_bytes) {
+      const cudaError_t err = cudaFuncSetAttribute(
+          kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+          static_cast<int>(bytes));
+      if (err != cudaSuccess) return err;
+      k.configured_bytes = static_cast<int>(bytes);
     }
-    if (err == cudaSuccess) {
-      err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel,
-                                                          kThreads, bytes);
+    // resident CTAs for this shared-memory size, cached per size
+    if (bytes != k.resident_bytes) {
+      int sms = 0, per_sm = 0;
+      cudaError_t err =
+          cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+      if (err == cudaSuccess) {
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel,
+                                                            kThreads, bytes);
+      }
+      if (err != cudaSuccess) return err;
+      k.resident = sms * per_sm;
+      k.resident_bytes = bytes;
     }
-    if (err != cudaSuccess) return err;
-    resident = sms * per_sm;
-    resident_bytes = bytes;
-  }
+    resident = k.resident;
+    return cudaSuccess;
+  });
+  if (setup_err != cudaSuccess) return setup_err;
   StageLaunch q = p;
   q.prefetch_stride = resident;
   kernel<<<p.tile_count, kThreads, bytes, stream>>>(q);
@@ -1435,14 +1469,18 @@ size_t gaussian_smem_bytes(const int max_ell, const int ntheta,
 cudaError_t launch_gaussian_band(const GaussianLaunch& p, cudaStream_t stream) {
   int warps = 1;
   const size_t bytes = gaussian_smem_bytes(p.max_ell, p.instance.ntheta, &warps);
-  static size_t configured = 0;
-  if (bytes > configured) {
-    const cudaError_t err = cudaFuncSetAttribute(
-        gaussian_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-        static_cast<int>(bytes));
-    if (err != cudaSuccess) return err;
-    configured = bytes;
-  }
+  static KernelSetups setups;
+  const cudaError_t setup_err = setups.with([&](KernelSetup& k, int) {
+    if (static_cast<int>(bytes) > k.configured_bytes) {
+      const cudaError_t err = cudaFuncSetAttribute(
+          gaussian_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+          static_cast<int>(bytes));
+      if (err != cudaSuccess) return err;
+      k.configured_bytes = static_cast<int>(bytes);
+    }
+    return cudaSuccess;
+  });
+  if (setup_err != cudaSuccess) return setup_err;
   const long long rows = static_cast<long long>(p.segment_count) * p.instance.nr;
   if (rows == 0) return cudaSuccess;
   long long blocks = (rows + warps - 1) / warps;

@@ -25,7 +25,9 @@ inline constexpr std::size_t kStaticSlopeCapacity = std::size_t{1} << 19;
 // (3 * kStaticSlopeCapacity complex values, 256-byte aligned).  The first
 // call on each device resolves the symbol, which loads the module that owns
 // the array; later calls return the cached address without any CUDA call
-// other than cudaGetDevice.
+// other than cudaGetDevice.  The cached address outlives a cudaDeviceReset
+// of that device, which frees the array: the entry point must not run on a
+// device after the host process reset it.
 cudaError_t static_slope_buffers(double2** base);
 
 }  // namespace teuk_b200

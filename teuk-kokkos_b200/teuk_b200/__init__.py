@@ -6,7 +6,10 @@ The classes mirror the reference's C++ interface: ``Pipeline`` is
 solve and ``Batch`` packs many solves into one set of stage launches.  State
 arrays are complex128 in the reference's (mode, field, radial, theta) order.
 Arrays may be numpy (host) or torch CUDA tensors (device).  There is no CPU
-fallback: importing this module fails when libteuk_b200.so is missing.
+fallback: the first call into the engine (``library()``, creating a
+``Pipeline``, ``Batch`` or ``Server``) fails when libteuk_b200.so is missing.
+The structures and configuration classes load nothing, so host-only code can
+describe solves without mapping the engine.
 """
 from __future__ import annotations
 
@@ -16,15 +19,12 @@ from dataclasses import dataclass, field
 from pathlib import Path
 from typing import Iterable, Sequence
 
+import threading
+
 import numpy as np
 
-import os
-
 _PACKAGE = Path(__file__).resolve().parent.parent
-# TEUK_B200_LIBRARY selects another build of the same C ABI (for A/B timing
-# of build variants); the default is the in-tree library.
-LIBRARY_PATH = Path(os.environ.get("TEUK_B200_LIBRARY",
-                                   _PACKAGE / "lib" / "libteuk_b200.so"))
+LIBRARY_PATH = _PACKAGE / "lib" / "libteuk_b200.so"
 
 OK = 0
 ERR_INVALID_ARGUMENT = -1
@@ -267,6 +267,34 @@ class WaveformRecord(ctypes.Structure):
 
 ABI_VERSION = 1
 
+KERNEL_AUTO, KERNEL_TILE = 0, 1
+PRECISION_FP64, PRECISION_SPLIT = 0, 1
+
+
+class _BatchOptions(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_int),
+        ("stage_kernel", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("strip_rows", ctypes.c_int),
+        ("autotune", ctypes.c_int),
+    ]
+
+
+@dataclass
+class LaunchOptions:
+    """teuk_b200_batch_options: stage kernel choice, transform precision,
+    streaming strip length (0: built-in or tuned), autotuning."""
+
+    stage_kernel: int = KERNEL_AUTO
+    precision: int = PRECISION_FP64
+    strip_rows: int = 0
+    autotune: bool = False
+
+    def to_struct(self):
+        return _BatchOptions(ABI_VERSION, self.stage_kernel, self.precision,
+                             self.strip_rows, int(self.autotune))
+
 
 @dataclass
 class SolveConfig:
@@ -365,6 +393,15 @@ def _load() -> ctypes.CDLL:
         "teuk_b200_last_error": ([], ctypes.c_char_p),
         "teuk_b200_abi_version": ([], I),
         "teuk_b200_create": ([ctypes.POINTER(_Config), ctypes.POINTER(P)], I),
+        "teuk_b200_create_with_options": ([ctypes.POINTER(_Config),
+                                           ctypes.POINTER(_BatchOptions),
+                                           ctypes.POINTER(P)], I),
+        "teuk_b200_test_withhold_chunk": ([I], I),
+        "teuk_b200_batch_create_with_options": ([ctypes.POINTER(_Config), I,
+                                                 ctypes.POINTER(_BatchOptions),
+                                                 ctypes.POINTER(P)], I),
+        "teuk_b200_batch_strip_rows": ([P, ctypes.POINTER(I), I,
+                                        ctypes.POINTER(I)], I),
         "teuk_b200_destroy": ([P], I),
         "teuk_b200_shape": ([P, ctypes.POINTER(SZ)], I),
         "teuk_b200_set_state": ([P, P, SZ, I], I),
@@ -432,12 +469,44 @@ def _load() -> ctypes.CDLL:
     return lib
 
 
-_lib = _load()
-EXPORTED_SYMBOLS = [n for n in dir(_lib) if n.startswith("teuk_b200_")]
+class _Library:
+    """The engine library, mapped on first use.  The structures, constants
+    and configuration classes above need no library, so host-only code (the
+    oracle bindings, workload descriptions) can use them without mapping the
+    engine into its process.  Any call into the engine loads it, and fails
+    loudly when it is missing: there is no CPU fallback."""
+
+    def __init__(self):
+        self._cdll = None
+        self._lock = threading.Lock()
+
+    def load(self) -> ctypes.CDLL:
+        if self._cdll is None:
+            with self._lock:
+                if self._cdll is None:
+                    self._cdll = _load()
+        return self._cdll
+
+    def loaded(self) -> bool:
+        return self._cdll is not None
+
+    def __getattr__(self, name):
+        return getattr(self.load(), name)
+
+
+_lib = _Library()
 
 
 def library() -> ctypes.CDLL:
-    return _lib
+    """The mapped engine library (loads it on first use)."""
+    return _lib.load()
+
+
+def test_withhold_chunk(chunk: int):
+    """Failure-detection test hook (teuk_b200_test_withhold_chunk): batches
+    built while chunk >= 0 withhold that chunk from CTA 0 of their stage-1
+    streaming launches; -1 switches it off."""
+    _check(_lib.teuk_b200_test_withhold_chunk(chunk))
 
 
 def _check(status: int):
@@ -519,11 +588,16 @@ def footprint_bytes(config: SolveConfig) -> int:
 class Pipeline:
     """One solve (teuk::SpatialPipeline)."""
 
-    def __init__(self, config: SolveConfig):
+    def __init__(self, config: SolveConfig, options: LaunchOptions | None = None):
         self.config = config
         s, keep = config.to_struct()
         handle = ctypes.c_void_p()
-        _check(_lib.teuk_b200_create(ctypes.byref(s), ctypes.byref(handle)))
+        if options is None:
+            _check(_lib.teuk_b200_create(ctypes.byref(s), ctypes.byref(handle)))
+        else:
+            o = options.to_struct()
+            _check(_lib.teuk_b200_create_with_options(
+                ctypes.byref(s), ctypes.byref(o), ctypes.byref(handle)))
         self._handle = handle
 
     def close(self):
@@ -636,7 +710,8 @@ class Pipeline:
 class Batch:
     """Many independent solves advanced by the same stage launches."""
 
-    def __init__(self, configs: Iterable[SolveConfig]):
+    def __init__(self, configs: Iterable[SolveConfig],
+                 options: LaunchOptions | None = None):
         self.configs = list(configs)
         structs = (_Config * len(self.configs))()
         keep = []
@@ -645,9 +720,25 @@ class Batch:
             structs[i] = s
             keep.append(k)
         handle = ctypes.c_void_p()
-        _check(_lib.teuk_b200_batch_create(structs, len(self.configs),
-                                           ctypes.byref(handle)))
+        if options is None:
+            _check(_lib.teuk_b200_batch_create(structs, len(self.configs),
+                                               ctypes.byref(handle)))
+        else:
+            o = options.to_struct()
+            _check(_lib.teuk_b200_batch_create_with_options(
+                structs, len(self.configs), ctypes.byref(o),
+                ctypes.byref(handle)))
         self._handle = handle
+
+    def strip_rows(self) -> list[int]:
+        """Streaming strip length per launch group (0: tile-kernel group)."""
+        n = ctypes.c_int()
+        _check(_lib.teuk_b200_batch_strip_rows(self._handle, None, 0,
+                                               ctypes.byref(n)))
+        out = (ctypes.c_int * max(n.value, 1))()
+        _check(_lib.teuk_b200_batch_strip_rows(self._handle, out, n.value,
+                                               ctypes.byref(n)))
+        return list(out[:n.value])
 
     def close(self):
         if getattr(self, "_handle", None):
