@@ -42,6 +42,7 @@ METRIC = ("grid-point updates/s, p99 latency: batched split-prec vs plain "
 UNIT = "grid-point updates/s"
 FALLBACK_HBM_GBS = 6650.0
 PASSES_PER_STEP = 14  # compulsory modal passes of the fused stage schedule
+SECOND_ORDER_BYTES_PER_POINT = 17 * 16 * 13  # 3,536 B per nodal point and step
 L2_BYTES = 126 * 1024 * 1024
 
 
@@ -60,10 +61,13 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-serving", action="store_true")
     p.add_argument("--no-second-order", action="store_true")
-    p.add_argument("--serve-requests", type=int, default=48,
+    p.add_argument("--serve-requests", type=int, default=64,
                    help="requests of the continuous-batching measurement")
-    p.add_argument("--serve-steps", type=int, default=200,
+    p.add_argument("--serve-steps", type=int, default=100,
                    help="RK4 steps per serving request")
+    p.add_argument("--no-uneven", action="store_true")
+    p.add_argument("--uneven-steps", type=int, default=20,
+                   help="timed RK4 steps of the 256-solve uneven batch")
     return p.parse_args()
 
 
@@ -85,55 +89,111 @@ def workload_config(batch: int):
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
+    """SM clock and clock-event reasons of one GPU during a timed region:
+    read-only NVML queries every `period_s` from a thread, plus one sample
+    when the sampler starts and one when it stops, so even a region of a
+    few tens of milliseconds carries its own record.  Falls back to
+    `nvidia-smi -lms 200` when NVML cannot be opened."""
+
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,"
               "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device_id: str | None):
-        self.samples = []
+    def __init__(self, device_uuid: str | None, period_s: float = 0.01):
+        self.samples = []  # (sm_mhz, sm_max_mhz, set of reason names)
+        self.period = period_s
         self.proc = None
+        self.nvml = None
+        self.handle = None
+        self._stop = threading.Event()
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            if device_uuid:
+                self.handle = pynvml.nvmlDeviceGetHandleByUUID(device_uuid)
+            else:
+                self.handle = pynvml.nvmlDeviceGetHandleByIndex(0)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(
+                self.handle, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nvml = None
+        if self.nvml is not None:
+            self._sample()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
         cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}",
                "--format=csv,noheader,nounits", "-lms", "200"]
-        if device_id:
-            cmd += ["-i", device_id]
+        if device_uuid:
+            cmd += ["-i", device_uuid]
         try:
             self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
             return
-        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread = threading.Thread(target=self._read_smi, daemon=True)
         self.thread.start()
 
-    def _read(self):
+    def _sample(self):
+        nv = self.nvml
+        try:
+            sm = nv.nvmlDeviceGetClockInfo(self.handle, nv.NVML_CLOCK_SM)
+            bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+        except Exception:
+            return
+        names = {name for name, const in self.REASONS
+                 if bits & getattr(nv, const, 0)}
+        self.samples.append((float(sm), float(self.max_mhz), names))
+
+    def _poll(self):
+        while not self._stop.wait(self.period):
+            self._sample()
+
+    def _read_smi(self):
         for line in self.proc.stdout:
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) >= 9:
-                self.samples.append(parts)
+            if len(parts) < 9 or not parts[1].replace(".", "").isdigit():
+                continue
+            names = {n for n, flag in zip(("hw_slowdown", "hw_thermal_slowdown",
+                                            "sw_thermal_slowdown", "sw_power_cap"),
+                                           parts[5:9])
+                     if flag.lower() == "active"}
+            self.samples.append((float(parts[1]), float(parts[2]), names))
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.thread.join(timeout=2)
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        sm_max = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
-                 "sw_power_cap"]
+        if self.nvml is not None:
+            self._stop.set()
+            self.thread.join(timeout=2)
+            self._sample()
+            source = "nvml"
+        elif self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+            source = "nvidia-smi"
+        else:
+            return {"sm_mhz": None, "sm_max_mhz": None,
+                    "reasons": ["unsampled"], "samples": 0}
+        sm = [x[0] for x in self.samples]
         reasons = set()
-        for s in self.samples:
-            for name, flag in zip(names, s[5:9]):
-                if flag.strip().lower() == "active":
-                    reasons.add(name)
+        for x in self.samples:
+            reasons |= x[2]
         return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(sm_max) if sm_max else None,
-                "reasons": sorted(reasons), "samples": len(self.samples)}
+                "sm_max_mhz": max(x[1] for x in self.samples) if sm else None,
+                "reasons": sorted(reasons), "samples": len(self.samples),
+                "source": source}
 
 
 def device_uuid(torch, device: int):
@@ -172,38 +232,57 @@ def recorded_traffic(kernel: str, algorithmic_bytes_per_launch: float):
 
 
 # ---------------------------------------------------------------- serving
+def solve_alone_seconds(tb, config, pulse, dt, steps: int, stream):
+    """Device seconds of `steps` RK4 steps of one solve alone (the plain
+    FP64 one-solve-at-a-time path), CUDA events on its stream, after two
+    untimed steps."""
+    import torch
+
+    p = tb.Pipeline(config)
+    p.set_stream(stream.cuda_stream)
+    p.initialize_gaussian(pulse)
+    p.step(0.0, dt, 2)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    p.step(2 * dt, dt, steps)
+    b.record(stream)
+    b.synchronize()
+    p.close()
+    return a.elapsed_time(b) / 1e3
+
+
 def one_at_a_time_rate(tb, wl, kinds, steps: int):
     """Plain FP64 path, one solve at a time: device grid-point updates/s of
     a representative solve of each request kind (CUDA events)."""
     import torch
 
-    rates = {}
     stream = torch.cuda.Stream()
+    rates = {}
     for kind, (config, pulse, dt) in kinds.items():
-        p = tb.Pipeline(config)
-        p.set_stream(stream.cuda_stream)
-        p.initialize_gaussian(pulse)
-        p.step(0.0, dt, 3)
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        p.step(3 * dt, dt, steps)
-        b.record(stream)
-        b.synchronize()
-        rates[kind] = steps * wl.grid_points(config) / (a.elapsed_time(b) / 1e3)
-        p.close()
+        seconds = solve_alone_seconds(tb, config, pulse, dt, steps, stream)
+        rates[kind] = steps * wl.grid_points(config) / seconds
     return rates
 
 
 def serving_run(tb, wl, capacity: float, requests: int, steps: int,
                 seed: int = 20260101):
-    """Poisson stream of mixed requests through the continuous-batching
-    server at ~80 % of the batched capacity; returns the 'serving' record."""
+    """Poisson stream of the serving mix through the continuous-batching
+    server at ~80 % of its capacity; returns the 'serving' record."""
     import torch
 
     mix = wl.serving_mix(requests, seed)
+    kinds = {}
+    for kind, c, pulse, dt in mix:
+        kinds.setdefault(kind, (c, pulse, dt))
+    alone = one_at_a_time_rate(tb, wl, kinds, min(steps, 20))
     work = [steps * wl.grid_points(c) for _, c, _, _ in mix]
-    rate = 0.8 * capacity / (sum(work) / len(work))
+    # offered load: 80 % of the rate at which the batched server would
+    # finish the mix, estimated from the batched linear rate and the
+    # second-order solves' own rate
+    seconds_needed = sum(w / (alone[k] if k == "second_order" else capacity)
+                         for w, (k, *_r) in zip(work, mix))
+    rate = 0.8 * len(mix) / seconds_needed
     rng = np.random.Generator(np.random.PCG64(seed + 1))
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=requests))
     arrivals -= arrivals[0]
@@ -226,32 +305,88 @@ def serving_run(tb, wl, capacity: float, requests: int, steps: int,
         server.advance(4)
     makespan = time.perf_counter() - t0
     latencies = np.array([server.result(i)[1] for i in ids])
+    by_kind = {}
+    for (kind, *_r), lat in zip(mix, latencies):
+        by_kind.setdefault(kind, []).append(lat)
     st = server.stats()
-    kinds = {}
-    for kind, c, pulse, dt in mix:
-        kinds.setdefault(kind, (c, pulse, dt))
-    alone = one_at_a_time_rate(tb, wl, kinds, min(steps, 50))
-    alone_seconds = sum(w / alone[k] for w, (k, *_rest) in zip(work, mix))
+    alone_seconds = sum(w / alone[k] for w, (k, *_r) in zip(work, mix))
     server.close()
     device_rate = st.grid_point_updates / st.device_seconds
+    counts = {k: len(v) for k, v in by_kind.items()}
     return {
         "requests": requests,
-        "mix": "40% schwarzschild nr=257 d8-4 ell<=8, 30% kerr_ringdown "
-               "nr=1025 d10-5 ell<=16, 30% uneven (a U[0,.95], nr in "
-               "{257,513,1025,2049}, ell U{8..20}, m=-2..2, d10-5)",
+        "mix": "40% schwarzschild a=0 nr=257 d8-4 ell<=8; 30% kerr_ringdown "
+               "a=0.7 nr=1025 d10-5 ell<=16; 20% second_order a=0.9 nr=1025 "
+               "ntheta=48 ell<=10/20 source on from t=0; 10% extremal a=0.99 "
+               "nr=4097 ell<=24 ntheta=37 m=-4..4",
+        "drawn": counts,
+        "reduced_from": "4096 requests at each configuration's own step "
+                        f"count; here {requests} requests x {steps} RK4 steps "
+                        "so the run fits the benchmark's time budget",
         "steps_per_request": steps,
-        "arrivals": f"Poisson, {rate:.2f}/s (80% of batched capacity)",
+        "arrivals": f"Poisson, {rate:.2f}/s (80% of the estimated capacity)",
         "p50_time_to_waveform_s": float(np.percentile(latencies, 50)),
         "p99_time_to_waveform_s": float(np.percentile(latencies, 99)),
+        "p50_p99_by_kind_s": {k: [float(np.percentile(v, 50)),
+                                  float(np.percentile(v, 99))]
+                              for k, v in by_kind.items()},
         "throughput": float(sum(work) / makespan),
         "device_throughput": float(device_rate),
         "one_at_a_time_device_throughput": float(sum(work) / alone_seconds),
+        "one_at_a_time_by_kind": alone,
         "batched_vs_one_at_a_time": float(device_rate / (sum(work) / alone_seconds)),
         "unit": UNIT,
         "batched_steps": int(st.steps),
         "makespan_s": makespan,
         "rebuilds": int(st.rebuilds),
         "rebuild_host_s": float(st.rebuild_seconds),
+    }
+
+
+# ---------------------------------------------------------------- uneven batch
+def uneven_batch_run(tb, wl, steps: int, options=None, label="fp64"):
+    """The batched uneven-instance configuration: 256 first-order solves of
+    uneven shape in one set of stage launches per RK4 step (graph replay),
+    against the same solves one at a time."""
+    import torch
+
+    solves = wl.uneven_batch()
+    configs = [c for c, _, _ in solves]
+    batch = tb.Batch(configs, options)
+    stream = torch.cuda.Stream()
+    batch.set_stream(stream.cuda_stream)
+    for i, (_, pulse, _) in enumerate(solves):
+        batch.initialize_gaussian(i, pulse)
+    dts = [dt for _, _, dt in solves]
+    batch.step(dts, steps=3, graph=True)
+    batch.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    batch.step(dts, steps=steps, graph=True)
+    b.record(stream)
+    b.synchronize()
+    seconds = a.elapsed_time(b) / 1e3
+    gp = sum(wl.grid_points(c) for c in configs)
+    kernels = batch.stage_kernels()
+    strips = batch.strip_rows()
+    batch.close()
+    alone = 0.0
+    for c, pulse, dt in solves:
+        alone += solve_alone_seconds(tb, c, pulse, dt, 3, stream) / 3
+    return {
+        "workload": "256 first-order solves: a U[0,0.95], nr from "
+                    "{257,513,1025,2049}, ell_max U{8..20}, m=-2..2, d10-5, "
+                    "Gaussian in ell=2 m=+-2 (centre U[6,14]M, width "
+                    "U[0.5,1.5]M), CFL 0.25; one seeded draw",
+        "precision": label,
+        "steps": steps, "reduced_from": "5000 RK4 steps per solve",
+        "value": gp * steps / seconds, "unit": UNIT,
+        "ms_per_step": 1e3 * seconds / steps,
+        "one_at_a_time": gp / alone,
+        "batched_vs_one_at_a_time": (gp * steps / seconds) / (gp / alone),
+        "stage_kernel_groups": {"streaming": kernels[0], "tile": kernels[1]},
+        "strip_rows": strips,
     }
 
 
@@ -277,6 +412,10 @@ def second_order_run(tb, wl, steps: int, cpu_steps: int):
     gp = wl.grid_points(config)
     gpu_rate = steps * gp / (a.elapsed_time(b) / 1e3)
     p.close()
+    peak, peak_kind = measured_hbm_peak()
+    # state-streaming floor: 17 passes x 16 B x 13 fields per nodal point
+    # and RK4 step
+    achieved = gpu_rate * SECOND_ORDER_BYTES_PER_POINT / 1e9
     sys.path.insert(0, str(REPO / "tests"))
     import oracle_bindings as ob
 
@@ -296,14 +435,36 @@ def second_order_run(tb, wl, steps: int, cpu_steps: int):
         "reference_cpu": ref_rate, "reference_cores": cores,
         "reference_steps": cpu_steps,
         "dtype": "f64", "storage": "nodal (m, 13 fields, r, theta)",
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak,
+                     "algorithmic_bytes_per_point_step": SECOND_ORDER_BYTES_PER_POINT,
+                     "peak_source": f"{peak_kind} hbm_gbs", "scope": "whole step"},
     }
 
 
 # ---------------------------------------------------------------- CPU side
-def cpu_reference_run(config, pulse, dt, seconds: float, warmup: int = 1,
-                      steps: int | None = None):
-    """Reference implementation on the host (oracle/_ref, all threads), else
-    the C restatement (port).  Returns (grid-point updates/s, description)."""
+def mapped_repo_libraries():
+    """Shared libraries of this repository mapped into this process."""
+    try:
+        maps = Path("/proc/self/maps").read_text()
+    except OSError:
+        return []
+    found = set()
+    for line in maps.splitlines():
+        path = line.split()[-1] if line.split() else ""
+        if path.endswith(".so") and path.startswith(str(REPO)):
+            found.add(str(Path(path).relative_to(REPO)))
+    return sorted(found)
+
+
+def cpu_reference_samples(config, pulse, dt, warmup: int, samples: int | None,
+                          seconds: float = 15.0):
+    """The reference implementation on the host cores (oracle/_ref, thread
+    pool over every core), else the C restatement (port, one core).  One
+    sample = one RK4 step of one solve of the workload.  `warmup` samples run
+    untimed; then `samples` samples (or as many as fit in about `seconds`)
+    are timed one by one.  Returns (grid-point updates/s over the timed
+    samples, description)."""
     sys.path.insert(0, str(REPO / "tests"))
     import oracle_bindings as ob
     from teuk_b200 import workloads as wl
@@ -315,25 +476,36 @@ def cpu_reference_run(config, pulse, dt, seconds: float, warmup: int = 1,
         pipe.initialize_gaussian(pulse)
         kind, cores = "reference", int(os.environ["TEUK_SHIM_NUM_THREADS"])
     else:
-        import teuk_b200 as tb
         pipe = ob.OraclePipeline(config)
         state = np.zeros(config.shape(), dtype=np.complex128)
         pipe.set_state(state + wl.band_noise(config, 1, 1e-3))
         kind, cores = "port", 1
-    pipe.step(0.0, dt, warmup)
-    if steps is None:
+    t = 0.0
+    for _ in range(max(warmup, 1)):
         t0 = time.perf_counter()
-        pipe.step(0.0, dt, 1)
-        one = time.perf_counter() - t0
-        steps = max(1, min(1000, int(seconds / max(one, 1e-6))))
-    t0 = time.perf_counter()
-    pipe.step(0.0, dt, steps)
-    elapsed = time.perf_counter() - t0
-    value = wl.grid_points(config) * steps / elapsed
-    return value, {"kind": kind, "cores": cores,
-                   "sample": f"{steps} RK4 steps of one solve of the same "
-                             f"workload ({wl.grid_points(config)} grid points)",
-                   "seconds": elapsed, "steps": steps}
+        pipe.step(t, dt, 1)
+        last = time.perf_counter() - t0
+        t += dt
+    if samples is None:
+        samples = max(3, min(2000, int(seconds / max(last, 1e-6))))
+    times = []
+    for _ in range(samples):
+        t0 = time.perf_counter()
+        pipe.step(t, dt, 1)
+        times.append(time.perf_counter() - t0)
+        t += dt
+    pipe.close()
+    gp = wl.grid_points(config)
+    total = sum(times)
+    rates = sorted(gp / x for x in times)
+    return gp * samples / total, {
+        "kind": kind, "cores": cores,
+        "sample": f"{samples} timed RK4 steps (after {max(warmup, 1)} untimed) "
+                  f"of one solve of the workload ({gp} grid points per step)",
+        "seconds": total, "steps": samples,
+        "per_step_rate": {"min": rates[0], "median": statistics.median(rates),
+                          "max": rates[-1]},
+    }
 
 
 def reference_arm(args):
@@ -341,12 +513,13 @@ def reference_arm(args):
     if rank != 0:
         return
     meta, config, pulse, dt = workload_config(args.batch)
-    # Each reference "step" is one RK4 step of one solve (bounded sample).
-    value, info = cpu_reference_run(config, pulse, dt, 0.0,
-                                    warmup=args.warmup, steps=args.steps)
-    meta = dict(meta)
-    meta["solves_per_gpu"] = 1
-    meta["l2"] = "host run: one solve's band state, 6.3 MB per buffer"
+    # Each reference step is a bounded sample of the workload: one RK4 step
+    # of one of its solves, on every host core.
+    value, info = cpu_reference_samples(config, pulse, dt, args.warmup,
+                                        args.steps)
+    native = mapped_repo_libraries()
+    if any("libteuk_b200" in n for n in native):
+        raise RuntimeError("the reference arm mapped the B200 engine library")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup,
@@ -355,10 +528,12 @@ def reference_arm(args):
         "dtype": "f64", "data": "synthetic (seeded Gaussian pulses)",
         "config": meta, "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["cores"],
-                         "kind": info["kind"], "sample": info["sample"]},
+                         "kind": info["kind"], "sample": info["sample"],
+                         "per_step_rate": info["per_step_rate"]},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "gpu_launches": 0,
+        "native_libraries": native,
     }
     print(json.dumps(line), flush=True)
 
@@ -479,6 +654,10 @@ def b200_arm(args):
     if rank == 0 and world == 1 and not args.no_second_order:
         second_order = second_order_run(tb, wl, 20, 2)
 
+    uneven = None
+    if rank == 0 and world == 1 and not args.no_uneven:
+        uneven = uneven_batch_run(tb, wl, args.uneven_steps)
+
     serving = None
     if rank == 0 and world == 1 and not args.no_serving:
         serving = serving_run(tb, wl, value, args.serve_requests,
@@ -486,9 +665,11 @@ def b200_arm(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        value_cpu, info = cpu_reference_run(config, pulse, dt, args.cpu_seconds)
+        value_cpu, info = cpu_reference_samples(config, pulse, dt, 3, None,
+                                                args.cpu_seconds)
         cpu = {"value": value_cpu, "unit": UNIT, "cores": info["cores"],
-               "kind": info["kind"], "sample": info["sample"]}
+               "kind": info["kind"], "sample": info["sample"],
+               "per_step_rate": info["per_step_rate"]}
 
     if rank == 0:
         meta = dict(meta)
@@ -509,6 +690,7 @@ def b200_arm(args):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "serving": serving,
+            "uneven_batch": uneven,
             "second_order": second_order,
             "gpu_launches": launches,
             "clocks": clocks,

@@ -5,9 +5,11 @@ each result is compared with the same solve run alone through the
 single-pipeline calls (1e-12 relative: mixing solves of other shapes changes
 the zero padding of the transform tiles, which may reorder a few FP64 sums),
 while requests arrive during the run, wait for memory, and leave at
-different times.
+different times.  Second-order (quadratic-source) requests run their own
+nodal pipelines beside the batch in every server step; their records must
+equal the same solve alone bit for bit (nothing they compute depends on the
+mix).
 """
-import dataclasses
 
 import numpy as np
 import pytest
@@ -19,6 +21,23 @@ pytestmark = pytest.mark.gpu
 
 TOL = 1e-12
 
+SECOND_ORDER = {
+    "so_unrestricted_d84": tb.SolveConfig(
+        mass=1.0, spin=0.7, compactification_length=1.2, radial_points=48,
+        theta_nodes=9, ell_max_first=4, ell_max_second=8,
+        modes=(-4, -2, 0, 2, 4), parents=(-2, 2), targets=(-4, 0, 4),
+        dissipation=0.003, discretization=tb.D84,
+        source_mode=tb.SOURCE_UNRESTRICTED, source_start_time=0.0),
+    "so_constraint_d42": tb.SolveConfig(
+        mass=1.0, spin=0.5, compactification_length=1.5, radial_points=40,
+        theta_nodes=10, ell_max_first=4, ell_max_second=6,
+        modes=(-4, -3, -2, -1, 0, 1, 2, 3, 4), parents=(-2, -1, 1, 2),
+        targets=(-3, -2, -1, 0, 1, 2, 3), dissipation=0.01,
+        discretization=tb.D42, reduction=tb.STAGE_CONSTRAINED,
+        source_mode=tb.SOURCE_CONSTRAINT_AWARE,
+        normalized_constraint_tolerance=1e30, required_consecutive_passes=2),
+}
+
 # linear solves of different shapes, discretizations and reductions
 MIX = [
     ("kerr_d105", 7, 12),
@@ -26,7 +45,34 @@ MIX = [
     ("kerr_d42_sc", 9, 9),
     ("nonparent", 10, 15),
     ("kerr_d105", 11, 5),
+    ("so_unrestricted_d84", 12, 6),
+    ("so_constraint_d42", 13, 4),
 ]
+
+
+def test_second_order_requests_match_alone_exactly(require_gpu):
+    """Only second-order requests: every record bit-identical to the solve
+    run alone (the nodal pipelines do not share buffers or launches)."""
+    server = tb.Server(hbm_budget_bytes=8 << 30)
+    jobs = []
+    for name, seed, steps in (("so_unrestricted_d84", 3, 5),
+                              ("so_constraint_d42", 4, 3)):
+        config = SECOND_ORDER[name]
+        pulse = pulse_for(config, seed)
+        dt = step_size(config)
+        jobs.append((server.submit(config, pulse, dt, steps), config, pulse,
+                     dt, steps))
+    while server.advance(2) > 0:
+        pass
+    for rid, config, pulse, dt, steps in jobs:
+        records, _ = server.result(rid)
+        alone = _alone(config, pulse, dt, steps)
+        assert _keys(records) == _keys(alone)
+        assert np.array_equal(_values(records), _values(alone))
+
+
+def _config(name):
+    return CASES[name] if name in CASES else SECOND_ORDER[name]
 
 
 def _alone(config, pulse, dt, steps):
@@ -54,7 +100,7 @@ def test_results_in_the_mix_match_results_alone(require_gpu):
     jobs = []
     # two requests up front, the rest arrive while the batch is running
     for i, (name, seed, steps) in enumerate(MIX):
-        config = CASES[name]
+        config = _config(name)
         pulse = pulse_for(config, seed)
         dt = step_size(config)
         rid = server.submit(config, pulse, dt, steps)
@@ -98,9 +144,7 @@ def test_server_rejects_what_it_cannot_run(require_gpu):
     with pytest.raises(tb.InvalidArgument, match="exceeds the server HBM budget"):
         server.submit(config, pulse_for(config, 1), step_size(config), 2)
     big = tb.Server(hbm_budget_bytes=8 << 30)
-    second = dataclasses.replace(CASES["nonparent"],
-                                 source_mode=tb.SOURCE_UNRESTRICTED)
-    with pytest.raises(tb.Unsupported):
-        big.submit(second, pulse_for(second, 1), step_size(second), 2)
+    with pytest.raises(tb.InvalidArgument, match="finite positive"):
+        big.submit(config, pulse_for(config, 1), 0.0, 2)
     with pytest.raises(tb.InvalidArgument, match="unknown request id"):
         big.result(12345)

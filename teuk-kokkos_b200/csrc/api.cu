@@ -1316,6 +1316,16 @@ struct ServerRequest {
   double submit_time = 0.0;
   double finish_time = -1.0;
   std::vector<teuk_b200_waveform_record> records;
+  // Second-order (ConstraintAware / Unrestricted) requests: their own nodal
+  // pipeline on its own stream, stepped beside the batch in every server
+  // step; `time` advances by dt per step as in teuk_b200_step.
+  bool second_order = false;
+  double time = 0.0;
+  std::unique_ptr<teuk_b200::NodalPipeline> nodal;
+  cudaEvent_t joined = nullptr;  // end of this request's work of a step
+  ~ServerRequest() {
+    if (joined != nullptr) cudaEventDestroy(joined);
+  }
 };
 
 // Continuous batching over Batch: admitted solves share one batched RK4
@@ -1378,10 +1388,7 @@ class Server {
     r->config = teuk_b200::to_config(raw);
     r->plan = teuk_b200::build_instance_plan(r->config);
     const teuk_b200::InstancePlan& plan = r->plan;
-    if (r->config.source_mode != TEUK_B200_SOURCE_DISABLED) {
-      throw teuk_b200::Unsupported(
-          "the server batches linear (disabled-source) solves only");
-    }
+    r->second_order = r->config.source_mode != TEUK_B200_SOURCE_DISABLED;
     if (!std::isfinite(dt) || !(dt > 0.0)) {
       throw std::invalid_argument("pipeline step requires finite positive time data");
     }
@@ -1389,7 +1396,8 @@ class Server {
     if (pulse.mode_count < 0 || (pulse.mode_count > 0 && pulse.modes == nullptr)) {
       throw std::invalid_argument("Gaussian mode list pointer/count mismatch");
     }
-    r->footprint = linear_footprint(plan);
+    r->footprint = r->second_order ? teuk_b200::nodal_footprint_bytes(plan)
+                                   : linear_footprint(plan);
     if (r->footprint > options_.hbm_budget_bytes) {
       throw std::invalid_argument("solve footprint exceeds the server HBM budget");
     }
@@ -1438,6 +1446,9 @@ class Server {
     st.grid_point_updates = grid_point_updates_;
     st.device_seconds = device_seconds_;
     st.resident_bytes = batch_ ? batch_->device_bytes() : 0;
+    for (const auto& r : active_) {
+      if (r->second_order) st.resident_bytes += r->footprint;
+    }
     st.rebuilds = rebuilds_;
     st.rebuild_seconds = rebuild_seconds_;
     return st;
@@ -1454,33 +1465,59 @@ class Server {
       }
       if (active_bytes_ + r->footprint > options_.hbm_budget_bytes) break;
       active_bytes_ += r->footprint;
+      if (r->second_order) {
+        start_nodal(*r);
+      } else {
+        changed = true;
+      }
       active_.push_back(r);
       queue_.pop_front();
-      changed = true;
     }
     if (changed) rebuild();
     membership_changed_ = false;
   }
 
+  // A second-order request gets its nodal pipeline, on its own stream, and
+  // its Gaussian initial data when it is admitted.
+  void start_nodal(ServerRequest& r) {
+    r.nodal = std::make_unique<teuk_b200::NodalPipeline>(r.plan);
+    teuk_b200_gaussian pulse = r.pulse;
+    pulse.modes = r.modes.data();
+    initialize_nodal_gaussian(*r.nodal, &pulse);
+    teuk_b200::check(cudaEventCreateWithFlags(&r.joined, cudaEventDisableTiming),
+                     "cudaEventCreate");
+    r.time = 0.0;
+  }
+
+  std::vector<std::shared_ptr<ServerRequest>> linear_active() const {
+    std::vector<std::shared_ptr<ServerRequest>> out;
+    for (const auto& r : active_) {
+      if (!r->second_order) out.push_back(r);
+    }
+    return out;
+  }
+
   // New batch layout for the admitted set; continuing solves keep their
   // band state (device-to-device), new ones get their Gaussian data.
   void rebuild() {
-    if (active_.empty()) {
+    const auto linear = linear_active();
+    if (linear.empty()) {
+      collect_step_times();
       batch_.reset();
       return;
     }
     collect_step_times();
     const double t0 = wall_seconds();
     std::vector<teuk_b200::InstancePlan> plans;
-    for (const auto& r : active_) plans.push_back(r->plan);
+    for (const auto& r : linear) plans.push_back(r->plan);
     auto next = std::make_unique<Batch>();
     next->build_planned(std::move(plans), &arena_);
     // the coefficient tables were computed on the batch's build stream:
     // finish them before the server's stream takes over
     teuk_b200::check(cudaStreamSynchronize(next->stream), "batch build");
     next->stream = stream_;
-    for (size_t i = 0; i < active_.size(); ++i) {
-      ServerRequest& r = *active_[i];
+    for (size_t i = 0; i < linear.size(); ++i) {
+      ServerRequest& r = *linear[i];
       const int slot = static_cast<int>(i);
       if (r.slot >= 0 && batch_) {
         const auto& from = batch_->instance_segments[static_cast<size_t>(r.slot)];
@@ -1514,16 +1551,33 @@ class Server {
 
   // One batched step, bracketed by a pair of events; the host does not
   // wait for it (a retirement's endpoint read is the next synchronisation).
+  //
+  // Second-order requests step on their own streams between the same pair
+  // of events: they wait for the step's start event and the server stream
+  // waits for each of them before the stop event, so the device time of a
+  // step covers the batch and every nodal pipeline running beside it.
   void step_once() {
     std::vector<double> dts;
-    for (const auto& r : active_) dts.push_back(r->dt);
+    for (const auto& r : active_) {
+      if (!r->second_order) dts.push_back(r->dt);
+    }
     while (events_.size() < 2 * static_cast<size_t>(pending_ + 1)) {
       cudaEvent_t e = nullptr;
       teuk_b200::check(cudaEventCreate(&e), "cudaEventCreate");
       events_.push_back(e);
     }
-    teuk_b200::check(cudaEventRecord(events_[2 * pending_], stream_), "event");
-    batch_->step(dts, 1, options_.graph != 0);
+    cudaEvent_t start = events_[2 * pending_];
+    teuk_b200::check(cudaEventRecord(start, stream_), "event");
+    if (batch_ && !dts.empty()) batch_->step(dts, 1, options_.graph != 0);
+    for (const auto& r : active_) {
+      if (!r->second_order) continue;
+      teuk_b200::check(cudaStreamWaitEvent(r->nodal->stream(), start, 0),
+                       "nodal fork");
+      r->nodal->step(r->time, r->dt);
+      r->time += r->dt;
+      teuk_b200::check(cudaEventRecord(r->joined, r->nodal->stream()), "event");
+      teuk_b200::check(cudaStreamWaitEvent(stream_, r->joined, 0), "nodal join");
+    }
     teuk_b200::check(cudaEventRecord(events_[2 * pending_ + 1], stream_),
                      "event");
     ++pending_;
@@ -1559,14 +1613,21 @@ class Server {
       size_t count = 0;
       r->records.resize(2 * c.modes.size() *
                         static_cast<size_t>(c.ell_max_first + c.ell_max_second + 2));
-      batch_->sample_endpoint(r->slot, r->records.data(), r->records.size(),
+      if (r->second_order) {
+        collect_step_times();
+        sample_nodal_endpoint(*r->nodal, r->records.data(), r->records.size(),
                               &count);
+        r->nodal.reset();
+      } else {
+        batch_->sample_endpoint(r->slot, r->records.data(), r->records.size(),
+                                &count);
+        membership_changed_ = true;
+      }
       r->records.resize(count);
       r->finish_time = wall_seconds();
       r->slot = -1;
       active_bytes_ -= r->footprint;
       ++finished_;
-      membership_changed_ = true;
     }
     active_.swap(keep);
   }

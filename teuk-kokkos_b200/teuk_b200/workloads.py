@@ -152,10 +152,35 @@ def uneven_instance(rng: np.random.Generator, cfl: float = 0.25):
     return config, GaussianPulse(center=center, width=width, modes=modes), dt
 
 
+def extremal_kerr(seed: int = 20260101, cfl: float = 0.25):
+    """Near-extremal linear Kerr solve of the serving mix: a = 0.99, M = 1,
+    nr = 4097, D10-5, m = -4..4, ell <= 24 (ntheta 37 by the exact-product
+    rule), Gaussian pulses (centre 8M, width 0.8M, amplitude 1e-3) in
+    ell = 2, m = +-2; CFL 0.25."""
+    base = SolveConfig(mass=1.0, spin=0.99, compactification_length=1.0,
+                       radial_points=4097, theta_nodes=37, ell_max_first=24,
+                       ell_max_second=24, modes=tuple(range(-4, 5)),
+                       reduction_damping=0.1, dissipation=0.0,
+                       discretization=D105)
+    dt = cfl_time_step(base, cfl)
+    sigma = min(0.005, 0.9 * dissipation_bound(D105, dt / base.spacing))
+    config = replace(base, dissipation=sigma)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    center, width = compactified(config, 8.0, 0.8)
+    modes = [(2, m, 1e-3 * complex(rng.standard_normal(), rng.standard_normal()))
+             for m in (-2, 2)]
+    return config, GaussianPulse(center=center, width=width, modes=modes), dt
+
+
+SERVING_KINDS = ("schwarzschild", "kerr_ringdown", "second_order", "extremal")
+
+
 def serving_mix(count: int, seed: int = 20260101):
-    """Request stream for the continuous-batching measurement: 40 %
-    Schwarzschild quadrupoles (nr 257), 30 % Kerr ringdowns (nr 1025),
-    30 % uneven instances; each entry (kind, config, pulse, dt)."""
+    """Request stream of the serving configuration: 40 % Schwarzschild
+    quadrupoles (nr 257, D8-4), 30 % Kerr ringdowns (a 0.7, nr 1025), 20 %
+    quadratic-source solves (a 0.9, nr 1025, ntheta 48, ell <= 10 / 20, the
+    source active from t = 0) and 10 % near-extremal Kerr solves (a 0.99,
+    nr 4097, ell <= 24); each entry (kind, config, pulse, dt)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     out = []
     for i in range(count):
@@ -166,10 +191,20 @@ def serving_mix(count: int, seed: int = 20260101):
         elif u < 0.7:
             config, pulse, dt = kerr_ringdown(seed + i)
             out.append(("kerr_ringdown", config, pulse, dt))
+        elif u < 0.9:
+            config, pulse, dt = second_order_self_coupling(seed + i)
+            out.append(("second_order", config, pulse, dt))
         else:
-            config, pulse, dt = uneven_instance(rng)
-            out.append(("uneven", config, pulse, dt))
+            config, pulse, dt = extremal_kerr(seed + i)
+            out.append(("extremal", config, pulse, dt))
     return out
+
+
+def uneven_batch(count: int = 256, seed: int = 20260101):
+    """The batched uneven-instance configuration: `count` solves drawn by
+    ``uneven_instance`` from one seeded stream; each (config, pulse, dt)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return [uneven_instance(rng) for _ in range(count)]
 
 
 def band_noise(config: SolveConfig, seed: int, scale: float = 1e-6):
