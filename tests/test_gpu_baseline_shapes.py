@@ -1,0 +1,355 @@
+"""Parity at the benchmark configurations' own shapes (GPU).
+
+The other parity tests use reduced radial sizes and a few dozen steps; these
+run the engine at the shapes the benchmark quotes and against the reference
+build (oracle/_ref) on the same seeded inputs:
+
+* the 2000-step Schwarzschild quadrupole (nr 257, D8-4) with its endpoint
+  waveform compared every 50 steps as a time series, against the serial
+  reference;
+* the Kerr ringdown at nr 1025 (D10-5, m = -4..4, ell <= 16) over 100 steps
+  with band-projected seeded noise, against the thread-pool reference;
+* the quadratic-source run at its full shape (a 0.9, nr 1025, ntheta 48,
+  ell <= 10 / 20) with the Unrestricted source switched on inside the run,
+  all 13 fields and the activation record;
+* the near-extremal linear shape class of the serving mix (a 0.99, ell <= 24,
+  ntheta 37) at a reduced nr;
+* a ConstraintAware latch whose tolerance lies between two measured
+  normalized-constraint maxima, so that it flips in the middle of the run.
+
+Tolerance: 1e-10 relative to each compared quantity's maximum modulus (the
+plain FP64 path); activation records and record keys exactly.
+
+The last test reproduces the reference's production-pipeline quasinormal
+mode anchors (tests/test_qnm.cpp:142-214, 321-403) on the engine alone:
+ringdown fits of the ell = m = 2 mode against the tabulated Schwarzschild
+frequency and the Leaver value for a = 0.7, with the reference's own
+thresholds.
+"""
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+import teuk_b200 as tb
+from teuk_b200 import workloads as wl
+from cases import relative_error
+from oracle_bindings import RefPipeline, ref_transform_matrices
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def _keys(records):
+    return [(r["boundary"], r["order"], r["m"], r["ell"]) for r in records]
+
+
+def _values(records):
+    return np.array([r["endpoint"] for r in records])
+
+
+def _compare_fields(gpu_state, ref_state, fields):
+    for f in fields:
+        err = relative_error(gpu_state[:, f], ref_state[:, f])
+        assert err < TOL, f"field {f}: relative error {err:.3e}"
+
+
+def test_schwarzschild_quadrupole_2000_step_waveform_series(require_gpu):
+    config, pulse, dt = wl.schwarzschild_quadrupole()
+    assert config.radial_points == 257 and config.discretization == tb.D84
+    gpu = tb.Pipeline(config)
+    ref = RefPipeline(config)
+    gpu.initialize_gaussian(pulse)
+    ref.initialize_gaussian(pulse)
+    series_gpu, series_ref = [], []
+    t = 0.0
+    for _ in range(2000 // 50):
+        gpu.step(t, dt, 50)
+        ref.step(t, dt, 50)
+        t += 50 * dt
+        g, r = gpu.sample_endpoint(), ref.sample_endpoint()
+        assert _keys(g) == _keys(r)
+        series_gpu.append(_values(g))
+        series_ref.append(_values(r))
+    series_gpu = np.array(series_gpu)  # (sample, record)
+    series_ref = np.array(series_ref)
+    for k in range(series_ref.shape[1]):
+        err = relative_error(series_gpu[:, k], series_ref[:, k])
+        assert err < TOL, f"record {k}: relative error {err:.3e}"
+    _compare_fields(gpu.get_state(), ref.get_state(), range(3))
+
+
+def test_kerr_ringdown_nr1025_100_steps(require_gpu):
+    config, pulse, dt = wl.kerr_ringdown()
+    assert config.radial_points == 1025 and len(config.modes) == 9
+    ref = RefPipeline(config, threads=True)
+    ref.initialize_gaussian(pulse)
+    noise = ref.project_to_bands(wl.band_noise(config, 7))
+    state = ref.get_state() + noise
+    ref.set_state(state)
+    gpu = tb.Pipeline(config)
+    gpu.set_state(state)
+    gpu.step(0.0, dt, 100)
+    ref.step(0.0, dt, 100)
+    _compare_fields(gpu.get_state(), ref.get_state(), range(3))
+    g, r = gpu.sample_endpoint(), ref.sample_endpoint()
+    assert _keys(g) == _keys(r)
+    assert relative_error(_values(g), _values(r)) < TOL
+
+
+def _activation(a):
+    return (a.active, a.activation_time, a.consecutive_passes,
+            a.last_eligibility_time)
+
+
+def test_quadratic_source_full_shape_source_starts_inside_run(require_gpu):
+    base, pulse, dt = wl.second_order_self_coupling()
+    config = replace(base, source_start_time=5.5 * dt)
+    assert (config.radial_points, config.theta_nodes) == (1025, 48)
+    assert (config.ell_max_first, config.ell_max_second) == (10, 20)
+    gpu = tb.Pipeline(config)
+    ref = RefPipeline(config, threads=True)
+    gpu.initialize_gaussian(pulse)
+    ref.initialize_gaussian(pulse)
+    _compare_fields(gpu.get_state(), ref.get_state(), range(13))
+    t = 0.0
+    for block in (4, 4, 4):  # the source switches on in the second block
+        gpu.step(t, dt, block)
+        ref.step(t, dt, block)
+        t += block * dt
+        assert _activation(gpu.activation()) == _activation(ref.activation())
+    assert gpu.activation().active
+    _compare_fields(gpu.get_state(), ref.get_state(), range(13))
+    g, r = gpu.sample_endpoint(), ref.sample_endpoint()
+    assert _keys(g) == _keys(r)
+    assert relative_error(_values(g), _values(r)) < TOL
+
+
+def test_near_extremal_ell24_ntheta37_linear(require_gpu):
+    base, pulse, _ = wl.extremal_kerr()
+    config = replace(base, radial_points=257)
+    dt = wl.time_step(config, 0.25)
+    config = replace(config, dissipation=min(
+        0.005, 0.9 * wl.dissipation_bound(tb.D105, dt / config.spacing)))
+    assert (config.ell_max_first, config.theta_nodes, config.spin) == (24, 37, 0.99)
+    ref = RefPipeline(config, threads=True)
+    ref.initialize_gaussian(pulse)
+    noise = ref.project_to_bands(wl.band_noise(config, 9))
+    state = ref.get_state() + noise
+    ref.set_state(state)
+    gpu = tb.Pipeline(config)
+    gpu.set_state(state)
+    gpu.step(0.0, dt, 20)
+    ref.step(0.0, dt, 20)
+    _compare_fields(gpu.get_state(), ref.get_state(), range(3))
+
+
+LATCH_BASE = tb.SolveConfig(
+    mass=1.0, spin=0.5, compactification_length=1.5, radial_points=40,
+    theta_nodes=10, ell_max_first=4, ell_max_second=6,
+    modes=(-4, -3, -2, -1, 0, 1, 2, 3, 4), parents=(-2, -1, 1, 2),
+    targets=(-3, -2, -1, 0, 1, 2, 3), dissipation=0.01,
+    discretization=tb.D42, reduction=tb.STAGE_CONSTRAINED,
+    source_mode=tb.SOURCE_CONSTRAINT_AWARE,
+    normalized_constraint_tolerance=0.0, required_consecutive_passes=1)
+LATCH_STEPS = 12
+
+
+def _ref_run(config, pulse, dt, steps, record=False):
+    ref = RefPipeline(config)
+    ref.initialize_gaussian(pulse)
+    values = []
+    t = 0.0
+    for _ in range(steps):
+        ref.step(t, dt, 1)
+        t += dt
+        if record:
+            values.append(ref.diagnostics().constraint_controlling_normalized)
+    return ref, values
+
+
+def _near_threshold_policy(pulse, dt):
+    """A (tolerance, required passes) policy whose latch activates in the
+    middle of the run: checks start at t = 4 dt (source_start_time 3.5 dt),
+    and the tolerance lies halfway between two consecutive measured
+    controlling normalized constraints (every measured value at least 1e-12
+    away from it), found by running the reference."""
+    base = replace(LATCH_BASE, source_start_time=3.5 * dt)
+    _, values = _ref_run(base, pulse, dt, LATCH_STEPS, record=True)
+    values = values[3:]  # the accepted states at t = 4 dt, 5 dt, ...
+    levels = sorted(set(values))
+    for passes in (1, 2, 3):
+        for lo, hi in zip(levels, levels[1:]):
+            tol = 0.5 * (lo + hi)
+            if min(abs(v - tol) for v in values) < 1e-12:
+                continue
+            config = replace(base, normalized_constraint_tolerance=tol,
+                             required_consecutive_passes=passes)
+            ref, _ = _ref_run(config, pulse, dt, LATCH_STEPS)
+            a = ref.activation()
+            if a.active and 4.5 * dt < a.activation_time < (LATCH_STEPS - 1.5) * dt:
+                return config, values
+    pytest.fail(f"no near-threshold tolerance found among {values}")
+
+
+def test_constraint_aware_latch_flips_between_measured_maxima(require_gpu):
+    """The latch decision compares a device reduction with the tolerance;
+    here the tolerance separates measured values that differ in their 9th
+    digit, so the activation record (active, time, passes, last eligibility
+    time) must match the reference exactly after every step."""
+    from cases import pulse_for, step_size
+
+    pulse = pulse_for(LATCH_BASE, 11)
+    dt = step_size(LATCH_BASE)
+    config, values = _near_threshold_policy(pulse, dt)
+    gpu = tb.Pipeline(config)
+    ref = RefPipeline(config)
+    gpu.initialize_gaussian(pulse)
+    ref.initialize_gaussian(pulse)
+    t = 0.0
+    for _ in range(LATCH_STEPS):
+        gpu.step(t, dt, 1)
+        ref.step(t, dt, 1)
+        t += dt
+        assert _activation(gpu.activation()) == _activation(ref.activation())
+    assert gpu.activation().active
+    _compare_fields(gpu.get_state(), ref.get_state(), range(13))
+
+
+# ------------------------------------------------------------ QNM anchors
+def _fit_real_damped(times, signal, step, start, end):
+    """Two-term real recurrence fit y2 = c1 y1 + c2 y0 (tests/test_qnm.cpp:
+    36-74): frequency and damping of the root pair, recurrence residual."""
+    s11 = s12 = s22 = b1 = b2 = sq = 0.0
+    n = len(signal)
+    for i in range(n - 2):
+        if times[i] < start or times[i + 2] > end:
+            continue
+        y0, y1, y2 = signal[i], signal[i + 1], signal[i + 2]
+        s11 += y1 * y1
+        s12 += y1 * y0
+        s22 += y0 * y0
+        b1 += y1 * y2
+        b2 += y0 * y2
+        sq += y2 * y2
+    det = s11 * s22 - s12 * s12
+    c1 = (b1 * s22 - b2 * s12) / det
+    c2 = (s11 * b2 - s12 * b1) / det
+    radius = np.sqrt(-c2)
+    phase = np.arccos(np.clip(c1 / (2.0 * radius), -1.0, 1.0))
+    res = 0.0
+    for i in range(n - 2):
+        if times[i] < start or times[i + 2] > end:
+            continue
+        r = signal[i + 2] - c1 * signal[i + 1] - c2 * signal[i]
+        res += r * r
+    return phase / step, -np.log(radius) / step, np.sqrt(res / sq)
+
+
+def _fit_complex_two_pole(times, signal, step, start, end):
+    """Complex two-pole recurrence fit (tests/test_qnm.cpp:76-140): the
+    positive-frequency root with the smaller damping."""
+    h11 = h12 = h22 = g1 = g2 = 0j
+    sq = 0.0
+    n = len(signal)
+    for i in range(n - 2):
+        if times[i] < start or times[i + 2] > end:
+            continue
+        y0, y1, y2 = signal[i], signal[i + 1], signal[i + 2]
+        h11 += np.conj(y1) * y1
+        h12 += np.conj(y1) * y0
+        h22 += np.conj(y0) * y0
+        g1 += np.conj(y1) * y2
+        g2 += np.conj(y0) * y2
+        sq += abs(y2) ** 2
+    det = h11 * h22 - h12 * np.conj(h12)
+    c1 = (g1 * h22 - h12 * g2) / det
+    c2 = (h11 * g2 - np.conj(h12) * g1) / det
+    disc = np.sqrt(c1 * c1 + 4.0 * c2)
+    roots = [0.5 * (c1 + disc), 0.5 * (c1 - disc)]
+    sel = 0
+    f0 = -np.angle(roots[0]) / step
+    f1 = -np.angle(roots[1]) / step
+    if f0 <= 0.0 and f1 > 0.0:
+        sel = 1
+    elif f0 > 0.0 and f1 > 0.0:
+        if -np.log(abs(roots[1])) / step < -np.log(abs(roots[0])) / step:
+            sel = 1
+    freq = -np.angle(roots[sel]) / step
+    damping = -np.log(abs(roots[sel])) / step
+    res = 0.0
+    for i in range(n - 2):
+        if times[i] < start or times[i + 2] > end:
+            continue
+        res += abs(signal[i + 2] - c1 * signal[i + 1] - c2 * signal[i]) ** 2
+    return freq, damping, np.sqrt(res / sq)
+
+
+def _production_ringdown(nr, ell_max, ntheta, spin, fit_start, fit_end):
+    """The reference's production-pipeline ringdown (tests/test_qnm.cpp:
+    142-214): M = 1, L = 2, D4-2, damping 0.1, dissipation 0.005, stored
+    modes m = +-2, a unit ell = m = 2 Gaussian at 0.675 R_H (width
+    0.08 R_H), dt 0.01, psi's ell = 2 coefficient of m = 2 sampled every
+    five steps at the radial index of R = 1."""
+    config = tb.SolveConfig(mass=1.0, spin=spin, compactification_length=2.0,
+                            radial_points=nr, theta_nodes=ntheta,
+                            ell_max_first=ell_max, ell_max_second=ell_max,
+                            modes=(-2, 2), reduction_damping=0.1,
+                            dissipation=0.005, discretization=tb.D42)
+    R_H = config.horizon_radius
+    gpu = tb.Pipeline(config)
+    gpu.initialize_gaussian(tb.GaussianPulse(center=0.675 * R_H,
+                                             width=0.08 * R_H,
+                                             modes=[(2, 2, 1.0)]))
+    dt, every, sample = 0.01, 5, 0.05
+    steps = int(round(fit_end / dt))
+    observe = int(round((1.0 / R_H) * (nr - 1)))
+    _, A = ref_transform_matrices(-2, 2, ell_max, ntheta)
+    mode = list(config.modes).index(2)
+    times, signal = [], []
+    for step in range(0, steps + 1, every):
+        line = gpu.get_state()[mode, 2, observe, :]
+        times.append(step * dt)
+        signal.append((A @ line)[0])
+        if step != steps:
+            gpu.step(step * dt, dt, every)
+    gpu.close()
+    if spin == 0.0:
+        return _fit_real_damped(times, np.real(signal), sample, fit_start,
+                                fit_end)
+    return _fit_complex_two_pole(times, np.array(signal), sample, fit_start,
+                                 fit_end)
+
+
+def test_production_quasinormal_modes_converge(require_gpu):
+    """The reference's convergence checks and thresholds
+    (tests/test_qnm.cpp:321-403) on ringdowns evolved by the engine."""
+    schw = (0.37367168, 0.08896232)
+    kerr = (0.5326002435510186, 0.08079287315500745)
+    setups = [(17, 3, 5, 0.0, 45.0, 65.0), (25, 3, 5, 0.0, 45.0, 65.0),
+              (33, 3, 5, 0.0, 45.0, 65.0), (33, 4, 7, 0.0, 45.0, 65.0),
+              (65, 3, 5, 0.7, 55.0, 80.0), (65, 4, 7, 0.7, 55.0, 80.0),
+              (65, 5, 8, 0.7, 55.0, 80.0)]
+    fits = [_production_ringdown(*s) for s in setups]
+    for f in fits:
+        assert all(np.isfinite(f))
+
+    def err(f, trusted):
+        return np.hypot(f[0] - trusted[0], f[1] - trusted[1])
+
+    coarse, medium, fine = (err(fits[i], schw) for i in range(3))
+    assert medium < 0.25 * coarse
+    assert fine < 0.70 * medium
+    assert fine < 3.0e-4
+    assert fits[2][2] < fits[1][2] < fits[0][2]
+    assert abs(fits[3][0] - fits[2][0]) < 1e-8
+    assert abs(fits[3][1] - fits[2][1]) < 1e-8
+    assert err(fits[3], schw) < 3.0e-4
+    coarse_to_medium = np.hypot(fits[5][0] - fits[4][0], fits[5][1] - fits[4][1])
+    medium_to_fine = np.hypot(fits[6][0] - fits[5][0], fits[6][1] - fits[5][1])
+    assert medium_to_fine < 0.05 * coarse_to_medium
+    assert err(fits[6], kerr) < 7.0e-4
+    assert abs(fits[6][0] - kerr[0]) < 5.0e-4
+    assert abs(fits[6][1] - kerr[1]) < 5.0e-4
+    assert fits[6][2] < 3.0e-6
