@@ -17,8 +17,9 @@ build (oracle/_ref) on the same seeded inputs:
 * a ConstraintAware latch whose tolerance lies between two measured
   normalized-constraint maxima, so that it flips in the middle of the run.
 
-Tolerance: 1e-10 relative to each compared quantity's maximum modulus (the
-plain FP64 path); activation records and record keys exactly.
+Tolerance: 1e-10 relative to each field's maximum modulus, endpoint records
+relative to the maximum modulus of the field they sample (the plain FP64
+path); activation records and record keys exactly.
 
 The last test reproduces the reference's production-pipeline quasinormal
 mode anchors (tests/test_qnm.cpp:142-214, 321-403) on the engine alone:
@@ -55,29 +56,40 @@ def _compare_fields(gpu_state, ref_state, fields):
         assert err < TOL, f"field {f}: relative error {err:.3e}"
 
 
+def _compare_records(gpu_records, ref_records, ref_state):
+    """Endpoint records against the reference, relative to the maximum
+    modulus of the psi field they sample (field 2 for first order, 12 for
+    second order) over the whole grid: the scale the field comparisons use.
+    At these step counts the pulse has not reached either boundary, so the
+    endpoint values are Gaussian tails far below the field's scale and a
+    record-by-record relative error would compare rounding noise."""
+    assert _keys(gpu_records) == _keys(ref_records)
+    g, r = _values(gpu_records), _values(ref_records)
+    for order, field in ((1, 2), (2, 12)):
+        idx = [i for i, rec in enumerate(ref_records) if rec["order"] == order]
+        if not idx:
+            continue
+        scale = np.max(np.abs(ref_state[:, field]))
+        err = np.max(np.abs(g[idx] - r[idx])) / scale
+        assert err < TOL, f"order {order} records: error {err:.3e} of the field scale"
+
+
 def test_schwarzschild_quadrupole_2000_step_waveform_series(require_gpu):
+    """Every 50 steps: the endpoint records and the three evolved fields."""
     config, pulse, dt = wl.schwarzschild_quadrupole()
     assert config.radial_points == 257 and config.discretization == tb.D84
     gpu = tb.Pipeline(config)
     ref = RefPipeline(config)
     gpu.initialize_gaussian(pulse)
     ref.initialize_gaussian(pulse)
-    series_gpu, series_ref = [], []
     t = 0.0
     for _ in range(2000 // 50):
         gpu.step(t, dt, 50)
         ref.step(t, dt, 50)
         t += 50 * dt
-        g, r = gpu.sample_endpoint(), ref.sample_endpoint()
-        assert _keys(g) == _keys(r)
-        series_gpu.append(_values(g))
-        series_ref.append(_values(r))
-    series_gpu = np.array(series_gpu)  # (sample, record)
-    series_ref = np.array(series_ref)
-    for k in range(series_ref.shape[1]):
-        err = relative_error(series_gpu[:, k], series_ref[:, k])
-        assert err < TOL, f"record {k}: relative error {err:.3e}"
-    _compare_fields(gpu.get_state(), ref.get_state(), range(3))
+        ref_state = ref.get_state()
+        _compare_records(gpu.sample_endpoint(), ref.sample_endpoint(), ref_state)
+        _compare_fields(gpu.get_state(), ref_state, range(3))
 
 
 def test_kerr_ringdown_nr1025_100_steps(require_gpu):
@@ -92,10 +104,9 @@ def test_kerr_ringdown_nr1025_100_steps(require_gpu):
     gpu.set_state(state)
     gpu.step(0.0, dt, 100)
     ref.step(0.0, dt, 100)
-    _compare_fields(gpu.get_state(), ref.get_state(), range(3))
-    g, r = gpu.sample_endpoint(), ref.sample_endpoint()
-    assert _keys(g) == _keys(r)
-    assert relative_error(_values(g), _values(r)) < TOL
+    ref_state = ref.get_state()
+    _compare_fields(gpu.get_state(), ref_state, range(3))
+    _compare_records(gpu.sample_endpoint(), ref.sample_endpoint(), ref_state)
 
 
 def _activation(a):
@@ -120,10 +131,9 @@ def test_quadratic_source_full_shape_source_starts_inside_run(require_gpu):
         t += block * dt
         assert _activation(gpu.activation()) == _activation(ref.activation())
     assert gpu.activation().active
-    _compare_fields(gpu.get_state(), ref.get_state(), range(13))
-    g, r = gpu.sample_endpoint(), ref.sample_endpoint()
-    assert _keys(g) == _keys(r)
-    assert relative_error(_values(g), _values(r)) < TOL
+    ref_state = ref.get_state()
+    _compare_fields(gpu.get_state(), ref_state, range(13))
+    _compare_records(gpu.sample_endpoint(), ref.sample_endpoint(), ref_state)
 
 
 def test_near_extremal_ell24_ntheta37_linear(require_gpu):
