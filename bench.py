@@ -68,6 +68,8 @@ def parse_args():
     p.add_argument("--serve-steps", type=int, default=100,
                    help="RK4 steps per serving request")
     p.add_argument("--no-uneven", action="store_true")
+    p.add_argument("--so-steps", type=int, default=20,
+                   help="timed RK4 steps of the quadratic-source solve")
     p.add_argument("--uneven-steps", type=int, default=20,
                    help="timed RK4 steps of the 256-solve uneven batch")
     return p.parse_args()
@@ -393,14 +395,12 @@ def uneven_batch_run(tb, wl, steps: int, options=None, label="fp64"):
 
 
 # ---------------------------------------------------------------- second order
-def second_order_run(tb, wl, steps: int, cpu_steps: int):
-    """The quadratic-source configuration (full 13-field stage graph with
-    the source active) on the GPU, beside the reference build on the host
-    cores for a few steps of the same solve."""
+def second_order_rate(tb, wl, config, pulse, dt, steps: int, options=None):
+    """Device grid-point updates/s of the quadratic-source solve (CUDA
+    events on its stream, after two untimed steps)."""
     import torch
 
-    config, pulse, dt = wl.second_order_self_coupling()
-    p = tb.Pipeline(config)
+    p = tb.Pipeline(config, options)
     stream = torch.cuda.Stream()
     p.set_stream(stream.cuda_stream)
     p.initialize_gaussian(pulse)
@@ -411,9 +411,28 @@ def second_order_run(tb, wl, steps: int, cpu_steps: int):
     p.step(2 * dt, dt, steps)
     b.record(stream)
     b.synchronize()
-    gp = wl.grid_points(config)
-    gpu_rate = steps * gp / (a.elapsed_time(b) / 1e3)
+    state = p.get_state()
     p.close()
+    if not np.all(np.isfinite(state)):
+        raise RuntimeError("second-order benchmark state is not finite")
+    return steps * wl.grid_points(config) / (a.elapsed_time(b) / 1e3), state
+
+
+def second_order_run(tb, wl, steps: int, cpu_steps: int):
+    """The quadratic-source configuration (full 13-field stage graph with
+    the source active) on the GPU, FP64 and split-precision transforms,
+    beside the reference build on the host cores for a few steps of the
+    same solve."""
+    config, pulse, dt = wl.second_order_self_coupling()
+    gp = wl.grid_points(config)
+    gpu_rate, state64 = second_order_rate(tb, wl, config, pulse, dt, steps)
+    split_rate, state_split = second_order_rate(
+        tb, wl, config, pulse, dt, steps,
+        tb.LaunchOptions(precision=tb.PRECISION_SPLIT))
+    split_dev = max(
+        float(np.max(np.abs(state_split[:, f] - state64[:, f])) /
+              max(np.max(np.abs(state64[:, f])), 1e-300))
+        for f in range(state64.shape[1]))
     peak, peak_kind = measured_hbm_peak()
     # state-streaming floor: 17 passes x 16 B x 13 fields per nodal point
     # and RK4 step
@@ -434,6 +453,11 @@ def second_order_run(tb, wl, steps: int, cpu_steps: int):
                     "m={-4,0,4} ell<=20, ntheta=48, source unrestricted "
                     "(active), Gaussian parents amp 1e-2",
         "value": gpu_rate, "unit": UNIT, "steps": steps,
+        "split_precision": {
+            "value": split_rate, "unit": UNIT, "vs_fp64": split_rate / gpu_rate,
+            "max_field_deviation_vs_fp64": split_dev,
+            "method": "angular operators through BF16 digit slices (5 per "
+                      "operand), FP32 accumulation, FP64 recombination"},
         "reference_cpu": ref_rate, "reference_cores": cores,
         "reference_steps": cpu_steps,
         "dtype": "f64", "storage": "nodal (m, 13 fields, r, theta)",
@@ -658,7 +682,7 @@ def b200_arm(args):
 
     second_order = None
     if rank == 0 and world == 1 and not args.no_second_order:
-        second_order = second_order_run(tb, wl, 20, 2)
+        second_order = second_order_run(tb, wl, args.so_steps, 2)
 
     uneven = None
     if rank == 0 and world == 1 and not args.no_uneven:

@@ -469,6 +469,7 @@ typedef struct teuk_b200_server_options {
   size_t hbm_budget_bytes;  /* device bytes the admitted solves may hold */
   int max_active;           /* cap on concurrent solves (0 = no cap) */
   int graph;                /* replay each batched step from a CUDA graph */
+  int precision;            /* teuk_b200_precision of every admitted solve */
 } teuk_b200_server_options;
 
 typedef struct teuk_b200_server_stats {

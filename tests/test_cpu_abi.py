@@ -126,3 +126,21 @@ def test_server_has_no_cpu_fallback():
     with pytest.raises(tb.TeukError) as info:
         tb.Server(hbm_budget_bytes=1 << 30)
     assert info.value.status == tb.ERR_CUDA
+
+
+@pytest.mark.parametrize("options,message", [
+    (tb.LaunchOptions(strip_rows=32), "strip_rows must be 0 or at least 64"),
+    (tb.LaunchOptions(stage_kernel=7), "unknown stage kernel choice"),
+    (tb.LaunchOptions(precision=3), "unknown transform precision"),
+])
+def test_launch_options_are_validated_before_device_work(options, message):
+    with pytest.raises(tb.InvalidArgument, match=message):
+        tb.Batch([CASES["schw_d84"]], options)
+    with pytest.raises(tb.InvalidArgument, match=message):
+        tb.Pipeline(CASES["schw_d84"], options)
+
+
+def test_test_hook_rejects_bad_chunk():
+    with pytest.raises(tb.InvalidArgument, match="chunk"):
+        tb.test_withhold_chunk(-2)
+    tb.test_withhold_chunk(-1)

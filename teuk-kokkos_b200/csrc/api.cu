@@ -14,12 +14,14 @@
 #include <cstring>
 #include <exception>
 #include <limits>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <new>
 #include <numbers>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -276,7 +278,11 @@ struct Batch {
   teuk_b200_batch_options options{TEUK_B200_ABI_VERSION, TEUK_B200_KERNEL_AUTO,
                                   TEUK_B200_PRECISION_FP64, 0, 0};
   std::vector<int> group_strip_rows;  // strip length per group (0: tile)
-  int last_strip_rows_ = 0;           // target of the last plan_strips
+  // strips of streaming group g live in h_strips / d_strips at
+  // [group_first_strip[g], + group_strip_capacity[g]): room for the most
+  // strips any strip length gives, so retuning one group moves no other
+  std::vector<int> group_strip_capacity;
+  std::vector<std::vector<int>> group_segments_;  // segments of each group
   int coef_rows = 0;
   DeviceArray<double> d_mat, d_trig;
   DeviceArray<double2> d_nodal;     // one instance's nodal state (lazy)
@@ -344,6 +350,10 @@ struct Batch {
       throw std::invalid_argument("a batch needs at least one solve");
     }
     plans = std::move(planned);
+    if (options.precision == TEUK_B200_PRECISION_SPLIT) {
+      throw Unsupported(
+          "split-precision transforms are not built for linear pipelines");
+    }
     for (const InstancePlan& plan : plans) {
       const Config& c = plan.config;
       if (c.source_mode != 0) {
@@ -474,9 +484,14 @@ struct Batch {
           }
           g.strips = nullptr;
           g.strip_count = 0;
-          group_first_strip.push_back(kind == 0 ? plan_strips(g, group_segments)
-                                                : -1);
-          group_strip_rows.push_back(kind == 0 ? last_strip_rows_ : 0);
+          if (kind == 0) {
+            plan_strip_region(g, group_segments);
+          } else {
+            group_first_strip.push_back(-1);
+            group_strip_capacity.push_back(0);
+            group_strip_rows.push_back(0);
+            group_segments_.push_back({});
+          }
           groups.push_back(g);
           group_first_tile.push_back(first_tile);
         }
@@ -594,35 +609,18 @@ struct Batch {
       g.kB = kB.ptr;
       g.acc = acc.ptr;
     }
+    if (options.autotune != 0 && options.strip_rows == 0) autotune_strips();
   }
 
-  // Radial strips of a streaming launch group (its segments `segs`),
-  // sorted by n_ell (largest first) so that a CTA's consecutive strips
-  // mostly share one ring row stride.  Returns the group's first strip
-  // index.
-  int plan_strips(StageLaunch& g, std::vector<int> segs) {
-    if (g.max_ell > kStreamMaxEll || g.max_theta > kStreamMaxNodes) {
-      throw std::logic_error("segment outside the streaming kernel's shapes");
-    }
-    int device = 0, sms = 0;
-    check(cudaGetDevice(&device), "cudaGetDevice");
-    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device),
-          "SM count");
-    long long rows = 0;
-    for (const int s : segs) {
-      rows += h_inst[static_cast<size_t>(h_seg[static_cast<size_t>(s)].instance)].nr;
-    }
-    const long long want = static_cast<long long>(std::max(sms, 1)) * kStripsPerCta;
-    const int target =
-        options.strip_rows > 0
-            ? options.strip_rows
-            : static_cast<int>(std::min<long long>(
-                  1024, std::max<long long>(kStripMinRows, rows / want)));
-    last_strip_rows_ = target;
+  // Radial strips of a streaming launch group (its segments `segs`) for a
+  // strip length of `target` rows, sorted by n_ell (largest first) so that
+  // a CTA's consecutive strips mostly share one ring row stride.  A segment
+  // of nr rows becomes max(1, min(nr / target, nr / 64)) balanced strips.
+  std::vector<TileDesc> make_strips(std::vector<int> segs, const int target) const {
     std::stable_sort(segs.begin(), segs.end(), [&](const int a, const int b) {
       return h_seg[static_cast<size_t>(a)].n_ell > h_seg[static_cast<size_t>(b)].n_ell;
     });
-    const int first = static_cast<int>(h_strips.size());
+    std::vector<TileDesc> out;
     for (const int s : segs) {
       const int nr = h_inst[static_cast<size_t>(h_seg[static_cast<size_t>(s)].instance)].nr;
       int n = std::max(1, nr / target);
@@ -630,11 +628,137 @@ struct Batch {
       for (int t = 0; t < n; ++t) {
         const int r0 = static_cast<int>(static_cast<long long>(nr) * t / n);
         const int r1 = static_cast<int>(static_cast<long long>(nr) * (t + 1) / n);
-        h_strips.push_back({s, r0, r1, 0});
+        out.push_back({s, r0, r1, 0});
       }
     }
-    g.strip_count = static_cast<int>(h_strips.size()) - first;
-    return g.strip_count > 0 ? first : -1;
+    return out;
+  }
+
+  // Built-in strip length: about kStripsPerCta strips per SM over the
+  // group's rows, between 64 and 1024 rows.
+  static int default_strip_rows(const long long rows, const int sms) {
+    const long long want = static_cast<long long>(std::max(sms, 1)) * kStripsPerCta;
+    return static_cast<int>(std::min<long long>(
+        1024, std::max<long long>(kStripMinRows, rows / want)));
+  }
+
+  long long group_rows(const std::vector<int>& segs) const {
+    long long rows = 0;
+    for (const int s : segs) {
+      rows += h_inst[static_cast<size_t>(h_seg[static_cast<size_t>(s)].instance)].nr;
+    }
+    return rows;
+  }
+
+  int device_sms() const {
+    int device = 0, sms = 0;
+    check(cudaGetDevice(&device), "cudaGetDevice");
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device),
+          "SM count");
+    return sms;
+  }
+
+  // Reserves the strip region of a new streaming group and fills it with
+  // the strips of the requested (or built-in) strip length.
+  void plan_strip_region(StageLaunch& g, const std::vector<int>& segs) {
+    if (g.max_ell > kStreamMaxEll || g.max_theta > kStreamMaxNodes) {
+      throw std::logic_error("segment outside the streaming kernel's shapes");
+    }
+    const int target = options.strip_rows > 0
+                           ? options.strip_rows
+                           : default_strip_rows(group_rows(segs), device_sms());
+    const int first = static_cast<int>(h_strips.size());
+    const int capacity = static_cast<int>(make_strips(segs, kStripMinRows).size());
+    std::vector<TileDesc> strips = make_strips(segs, target);
+    h_strips.insert(h_strips.end(), strips.begin(), strips.end());
+    h_strips.resize(static_cast<size_t>(first + capacity), TileDesc{0, 0, 0, 0});
+    g.strip_count = static_cast<int>(strips.size());
+    group_first_strip.push_back(first);
+    group_strip_capacity.push_back(capacity);
+    group_strip_rows.push_back(target);
+    group_segments_.push_back(segs);
+  }
+
+  // Writes strips into group gi's region of the device strip table.
+  void upload_group_strips(const size_t gi, const std::vector<TileDesc>& strips) {
+    std::copy(strips.begin(), strips.end(),
+              h_strips.begin() + group_first_strip[gi]);
+    check(cudaMemcpyAsync(d_strips.ptr + group_first_strip[gi], strips.data(),
+                          strips.size() * sizeof(TileDesc),
+                          cudaMemcpyHostToDevice, stream),
+          "upload strips");
+    groups[gi].strip_count = static_cast<int>(strips.size());
+  }
+
+  // The strip-length autotuner.  For every streaming launch group it times
+  // one RK4 step (the four stage launches) of the group for each candidate
+  // strip length and keeps the fastest; the choice is cached for the
+  // process by (discretization, reduction, widest band, rows rounded to a
+  // quarter octave, SM count).  Strips only decide which CTA streams which
+  // rows: every row gets the same sums in the same order for any choice,
+  // so results are bit-identical across choices.  Runs at build, on the
+  // zero state (every stage of a zero state is zero, and stages 2-4 read
+  // only what the stages before them wrote).
+  void autotune_strips() {
+    static std::mutex cache_mutex;
+    static std::map<std::tuple<int, int, int, int, int>, int> cache;
+    static const int kCandidates[] = {64, 96, 128, 192, 256, 384, 512, 768, 1024};
+    const int sms = device_sms();
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    for (cudaEvent_t& e : ev) check(cudaEventCreate(&e), "cudaEventCreate");
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+      if (group_first_strip[gi] < 0) continue;
+      const auto& segs = group_segments_[gi];
+      const long long rows = group_rows(segs);
+      int max_nr = 0;
+      for (const int s : segs) {
+        max_nr = std::max(max_nr, h_inst[static_cast<size_t>(h_seg[static_cast<size_t>(s)].instance)].nr);
+      }
+      const auto key = std::make_tuple(
+          groups[gi].disc, groups[gi].reduction, groups[gi].max_ell,
+          static_cast<int>(std::lround(4.0 * std::log2(static_cast<double>(rows)))),
+          sms);
+      int best = -1;
+      {
+        std::lock_guard<std::mutex> lock(cache_mutex);
+        const auto it = cache.find(key);
+        if (it != cache.end()) best = it->second;
+      }
+      if (best < 0) {
+        float best_ms = std::numeric_limits<float>::infinity();
+        for (const int c : kCandidates) {
+          if (c > std::max(max_nr, kStripMinRows)) break;
+          upload_group_strips(gi, make_strips(segs, c));
+          float ms = std::numeric_limits<float>::infinity();
+          for (int rep = 0; rep < 3; ++rep) {
+            check(cudaEventRecord(ev[0], stream), "event");
+            for (int kind = kStage1; kind <= kStage4; ++kind) {
+              StageLaunch g = groups[gi];
+              g.stage = kind;
+              check(launch_stage(g, stream), "stage kernel");
+            }
+            check(cudaEventRecord(ev[1], stream), "event");
+            check(cudaEventSynchronize(ev[1]), "autotune step");
+            float t = 0.0f;
+            check(cudaEventElapsedTime(&t, ev[0], ev[1]), "event time");
+            if (rep > 0) ms = std::min(ms, t);
+          }
+          if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+          }
+        }
+        std::lock_guard<std::mutex> lock(cache_mutex);
+        cache[key] = best;
+      }
+      upload_group_strips(gi, make_strips(segs, best));
+      group_strip_rows[gi] = best;
+    }
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    check(cudaStreamSynchronize(stream), "autotune");
+    check_kernel_error();
+    // the stages ran on the zero state: y is still zero, the slopes are
+    // rewritten by the first step
   }
 
   // Raises the error a streaming-kernel wait recorded (after a stream sync).
@@ -1343,6 +1467,10 @@ class Server {
     if (o.max_active < 0) {
       throw std::invalid_argument("server max_active must be nonnegative");
     }
+    if (o.precision != TEUK_B200_PRECISION_FP64 &&
+        o.precision != TEUK_B200_PRECISION_SPLIT) {
+      throw std::invalid_argument("unknown transform precision");
+    }
     require_device();
     teuk_b200::check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking),
                      "cudaStreamCreate");
@@ -1480,7 +1608,7 @@ class Server {
   // A second-order request gets its nodal pipeline, on its own stream, and
   // its Gaussian initial data when it is admitted.
   void start_nodal(ServerRequest& r) {
-    r.nodal = std::make_unique<teuk_b200::NodalPipeline>(r.plan);
+    r.nodal = std::make_unique<teuk_b200::NodalPipeline>(r.plan, options_.precision);
     teuk_b200_gaussian pulse = r.pulse;
     pulse.modes = r.modes.data();
     initialize_nodal_gaussian(*r.nodal, &pulse);
@@ -1511,6 +1639,7 @@ class Server {
     std::vector<teuk_b200::InstancePlan> plans;
     for (const auto& r : linear) plans.push_back(r->plan);
     auto next = std::make_unique<Batch>();
+    next->options.precision = options_.precision;
     next->build_planned(std::move(plans), &arena_);
     // the coefficient tables were computed on the batch's build stream:
     // finish them before the server's stream takes over
@@ -1699,7 +1828,7 @@ int create_pipeline(const teuk_b200_config* config,
     if (c.source_mode != TEUK_B200_SOURCE_DISABLED) {
       const teuk_b200::InstancePlan plan = teuk_b200::build_instance_plan(c);
       require_device();
-      p->nodal = std::make_unique<teuk_b200::NodalPipeline>(plan);
+      p->nodal = std::make_unique<teuk_b200::NodalPipeline>(plan, opts.precision);
     } else {
       p->batch = std::make_unique<Batch>();
       p->batch->options = opts;

@@ -4,6 +4,7 @@
 // is binary64; complex/complex division scales by |c|+|d|.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <limits>
 #include <numbers>
 #include <stdexcept>
@@ -386,6 +387,297 @@ __global__ void angular_op_kernel(const Geo g, const Trig tr,
     // the next row's staging waits for every lane's reads of this one
     for (int k = 0, j = lane; j < g.nt; j += 32, ++k) out[j] = result[k];
     __syncwarp();
+  }
+}
+
+// ------------------------------------------------------------- tile operator
+// The four operations of angular_op_kernel through one composite nodal
+// matrix per (coordinator, operation, mode), built on the host:
+//   T = S_out diag(d) A   (nt x nt),   out[r][j] = sum_k T[j][k] x[r][k],
+// then the GHP point formula for eth / eth'.  A CTA takes 32 radial rows of
+// one mode (a warp 8), stages them in shared memory and multiplies on the
+// tensor cores: in FP64 (mma.sync m8n8k4), or in split precision.
+//
+// Split precision (Ozaki, Ogita, Oishi & Rump, "Error-free transformations
+// of matrix multiplication by using fast routines of matrix multiplication
+// and its applications", Numer. Algorithms 59, 2012): every real row of x and
+// every column of T is scaled by a power of two to below 1 in modulus and cut
+// into five signed 8-bit digits, d = sum_s t_s 2^(-7-8s), |t_s| <= 128, each
+// exact in BF16.  Digit products are integers below 2^14 and a K <= 64 sum of
+// up to five of them stays below 2^24, so the BF16 tensor-core products
+// accumulated in FP32 (mma.sync m16n8k16) are exact; the 15 digit pairs with
+// s + t <= 4 are summed in five FP32 accumulators (one per s + t) and
+// recombined in FP64 with the two scales.  The dropped pairs and the digit
+// remainders leave an error of about 2^-40 of max|x_row| max|T_col| per term.
+constexpr int kTileRows = 8;     // complex rows of one MMA row tile
+constexpr int kTileWarps = 4;    // two warps per row tile, each half the nodes
+constexpr int kTileCtaRows = 16; // two row tiles per CTA
+constexpr int kTileMaxNodes = 64;                // nodes of the tile kernel
+constexpr int kTileStride = kTileMaxNodes + 4;   // staged row stride
+constexpr int kTileLoads = kTileCtaRows * kTileMaxNodes / (kTileWarps * 32);
+constexpr int kSplitSlices = 5;
+constexpr int kPrecisionFp64 = 0;
+constexpr int kPrecisionSplit = 1;
+
+struct AngularTileParams {
+  int kind;
+  Arr in;
+  int in_slot;
+  Arr dt;
+  int dt_slot;
+  Arr out;
+  int out_slot;
+  const int* active;
+  // per mode: FP64 fragment offset (doubles), split fragment offset (uint2),
+  // split column-scale offset (doubles); 3 ints per mode
+  const int* offsets;
+  const double* fp64;    // [n8][k4][lane] B fragments of T^T
+  const uint2* split;    // [n8][k16][slice][lane] BF16 digit fragments
+  const double* scales;  // 2^(F_j - 14) per output node
+  int spin, boost;
+};
+
+__device__ __forceinline__ void dmma_tile(double& c0, double& c1, const double a,
+                                          const double b) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, "
+      "{%0,%1};\n"
+      : "+d"(c0), "+d"(c1)
+      : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void hmma_bf16(float (&c)[4], const unsigned (&a)[4],
+                                          const uint2 b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+      "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b.x), "r"(b.y));
+}
+
+// Five signed 8-bit digits of w (|w| < 1): w = sum_s t_s 2^(-7-8s) up to
+// 2^-40; every step is exact in binary64.
+__device__ __forceinline__ void split_digits(const double w, float (&t)[kSplitSlices]) {
+  double r = w * 128.0;
+#pragma unroll
+  for (int s = 0; s < kSplitSlices; ++s) {
+    const double d = rint(r);
+    t[s] = static_cast<float>(d);
+    r = (r - d) * 256.0;
+  }
+}
+
+// Two BF16 values in one register, `lo` in the low half (exact: the digits
+// are integers of at most 8 bits).
+__device__ __forceinline__ unsigned pack_bf16(const float lo, const float hi) {
+  return (__float_as_uint(lo) >> 16) | (__float_as_uint(hi) & 0xffff0000u);
+}
+
+// Power-of-two scale that brings |v| <= m below 1: returns 2^-e with
+// m = f 2^e, f in [0.5, 1) (e >= -1000 so the scale stays finite).
+__device__ __forceinline__ int scale_exponent(const double m) {
+  int e = 0;
+  frexp(m, &e);
+  return m == 0.0 ? 0 : max(e, -1000);
+}
+
+// Stages rows [r0, r0 + rows) of one (mode, slot) plane into split real /
+// imaginary shared arrays, K padded with zeros; every thread issues all of
+// its loads before its first store.
+__device__ __forceinline__ void stage_tile_rows(const double2* src,
+                                                const int rows, const int nt,
+                                                const int kpad,
+                                                double (*re)[kTileStride],
+                                                double (*im)[kTileStride]) {
+  double2 v[kTileLoads];
+#pragma unroll
+  for (int u = 0; u < kTileLoads; ++u) {
+    const int i = threadIdx.x + u * kTileWarps * 32;
+    const int row = i / kpad, k = i - row * kpad;
+    v[u] = make_double2(0.0, 0.0);
+    if (row < rows && k < nt) v[u] = src[row * nt + k];
+  }
+#pragma unroll
+  for (int u = 0; u < kTileLoads; ++u) {
+    const int i = threadIdx.x + u * kTileWarps * 32;
+    const int row = i / kpad, k = i - row * kpad;
+    if (row < kTileCtaRows) {
+      re[row][k] = v[u].x;
+      im[row][k] = v[u].y;
+    }
+  }
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(kTileWarps * 32)
+    angular_tile_kernel(const Geo g, const Trig tr, const AngularTileParams p) {
+  __shared__ double xr[kTileCtaRows][kTileStride];
+  __shared__ double xi[kTileCtaRows][kTileStride];
+  __shared__ double dr[kTileCtaRows][kTileStride];  // d_T x (eth / eth')
+  __shared__ double di[kTileCtaRows][kTileStride];
+  const int nt = g.nt;
+  const int tiles = (g.nr + kTileCtaRows - 1) / kTileCtaRows;
+  const int mode = blockIdx.x / tiles;
+  const int r0 = (blockIdx.x - mode * tiles) * kTileCtaRows;
+  const int rows = min(kTileCtaRows, g.nr - r0);
+  double2* out = p.out.at(g, mode, p.out_slot, r0, 0);
+  if (!p.active[mode]) {
+    for (int i = threadIdx.x; i < rows * nt; i += blockDim.x) {
+      out[i] = make_double2(0.0, 0.0);
+    }
+    return;
+  }
+  const bool ghp = p.kind == kEth || p.kind == kEthPrime;
+  // K padded to the MMA's k granularity; padding columns and rows past the
+  // grid are zero
+  const int kpad = PREC == kPrecisionSplit ? (nt + 15) / 16 * 16 : (nt + 3) / 4 * 4;
+  stage_tile_rows(p.in.at(g, mode, p.in_slot, r0, 0), rows, nt, kpad, xr, xi);
+  if (ghp) stage_tile_rows(p.dt.at(g, mode, p.dt_slot, r0, 0), rows, nt, kpad, dr, di);
+  // every read of the input rows happens before any store below (the
+  // operation may run in place)
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = lane >> 2, q = lane & 3;
+  const int half = warp & 1;                        // output node tiles n % 2
+  const int row = (warp >> 1) * kTileRows + grp;    // CTA-local row of this lane
+  const int n8 = (nt + 7) / 8;
+  const double R = g.spacing * static_cast<double>(r0 + row);
+  const bool live = row < rows;
+  const auto finish = [&](const int j, double re, double im) {
+    if (!live || j >= nt) return;
+    C2 v = mk(re, im);
+    if (ghp) {
+      const C2 x = mk(xr[row][j], xi[row][j]);
+      const C2 dtv = mk(dr[row][j], di[row][j]);
+      v = p.kind == kEth ? eth_point(g, x, dtv, v, p.spin, p.boost, R,
+                                     tr.grid_sin[j], tr.grid_cos[j])
+                         : ethprime_point(g, x, dtv, v, p.spin, p.boost, R,
+                                          tr.grid_sin[j], tr.grid_cos[j]);
+    }
+    out[row * nt + j] = st(v);
+  };
+  constexpr int kHalfN8 = kTileMaxNodes / 16;  // n tiles of one warp
+  if constexpr (PREC == kPrecisionFp64) {
+    const int k4 = kpad / 4;
+    const double* frag = p.fp64 + p.offsets[3 * mode];
+    double acc[kHalfN8][4];
+#pragma unroll
+    for (int h = 0; h < kHalfN8; ++h) {
+      acc[h][0] = acc[h][1] = acc[h][2] = acc[h][3] = 0.0;
+    }
+    // unrolled over the largest K so the fragment loads of later k steps
+    // issue ahead of the MMAs that wait for earlier ones
+#pragma unroll
+    for (int ks = 0; ks < kTileMaxNodes / 4; ++ks) {
+      if (ks < k4) {
+        const double ar = xr[row][ks * 4 + q];
+        const double ai = xi[row][ks * 4 + q];
+#pragma unroll
+        for (int h = 0; h < kHalfN8; ++h) {
+          const int n = 2 * h + half;
+          if (n < n8) {
+            const double b = __ldg(frag + (n * k4 + ks) * 32 + lane);
+            dmma_tile(acc[h][0], acc[h][1], ar, b);
+            dmma_tile(acc[h][2], acc[h][3], ai, b);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < kHalfN8; ++h) {
+      const int n = 2 * h + half;
+      if (n < n8) {
+        finish(n * 8 + 2 * q, acc[h][0], acc[h][2]);
+        finish(n * 8 + 2 * q + 1, acc[h][1], acc[h][3]);
+      }
+    }
+  } else {
+    const int k16 = kpad / 16;
+    constexpr int kMaxK16 = kTileMaxNodes / 16;
+    // per real row (this lane's row: real part, imaginary part) scale over
+    // the K nodes; the four lanes of a quad hold the whole row
+    double mr = 0.0, mi = 0.0;
+#pragma unroll
+    for (int ks = 0; ks < kMaxK16; ++ks) {
+      if (ks < k16) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int k = ks * 16 + 2 * q + (e & 1) + 8 * (e >> 1);
+          mr = fmax(mr, fabs(xr[row][k]));
+          mi = fmax(mi, fabs(xi[row][k]));
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 1; o <= 2; o <<= 1) {
+      mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+      mi = fmax(mi, __shfl_xor_sync(0xffffffffu, mi, o));
+    }
+    const int er = scale_exponent(mr), ei = scale_exponent(mi);
+    const double down_r = ldexp(1.0, -er), down_i = ldexp(1.0, -ei);
+    // A fragments: rows 0-7 real parts, rows 8-15 imaginary parts of the
+    // tile's 8 complex rows; every slice of every k step
+    unsigned a[kMaxK16][kSplitSlices][4];
+#pragma unroll
+    for (int ks = 0; ks < kMaxK16; ++ks) {
+      if (ks < k16) {
+        float t[4][2][kSplitSlices];  // [k offset][re, im][slice]
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int k = ks * 16 + 2 * q + (e & 1) + 8 * (e >> 1);
+          split_digits(xr[row][k] * down_r, t[e][0]);
+          split_digits(xi[row][k] * down_i, t[e][1]);
+        }
+#pragma unroll
+        for (int s = 0; s < kSplitSlices; ++s) {
+          a[ks][s][0] = pack_bf16(t[0][0][s], t[1][0][s]);
+          a[ks][s][1] = pack_bf16(t[0][1][s], t[1][1][s]);
+          a[ks][s][2] = pack_bf16(t[2][0][s], t[3][0][s]);
+          a[ks][s][3] = pack_bf16(t[2][1][s], t[3][1][s]);
+        }
+      }
+    }
+    const uint2* frag = p.split + p.offsets[3 * mode + 1];
+    const double* colscale = p.scales + p.offsets[3 * mode + 2];
+    const double up_r = ldexp(1.0, er), up_i = ldexp(1.0, ei);
+    for (int n = half; n < n8; n += 2) {
+      float d[kSplitSlices][4];  // accumulator of digit pairs with s + t = u
+#pragma unroll
+      for (int u = 0; u < kSplitSlices; ++u) {
+        d[u][0] = d[u][1] = d[u][2] = d[u][3] = 0.0f;
+      }
+#pragma unroll
+      for (int ks = 0; ks < kMaxK16; ++ks) {
+        if (ks < k16) {
+          uint2 b[kSplitSlices];
+#pragma unroll
+          for (int t = 0; t < kSplitSlices; ++t) {
+            b[t] = __ldg(frag + ((n * k16 + ks) * kSplitSlices + t) * 32 + lane);
+          }
+#pragma unroll
+          for (int s = 0; s < kSplitSlices; ++s) {
+#pragma unroll
+            for (int t = 0; t + s < kSplitSlices; ++t) {
+              hmma_bf16(d[s + t], a[ks][s], b[t]);
+            }
+          }
+        }
+      }
+      double v[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        double sum = static_cast<double>(d[kSplitSlices - 1][c]);
+#pragma unroll
+        for (int u = kSplitSlices - 2; u >= 0; --u) {
+          sum = fma(sum, 1.0 / 256.0, static_cast<double>(d[u][c]));
+        }
+        v[c] = sum;
+      }
+      const int j = n * 8 + 2 * q;
+      const double s0 = colscale[j], s1 = colscale[j + 1];
+      finish(j, v[0] * up_r * s0, v[2] * up_i * s0);
+      finish(j + 1, v[1] * up_r * s1, v[3] * up_i * s1);
+    }
   }
 }
 
@@ -1060,6 +1352,11 @@ struct NodalPipeline::Buffers {
           *proj = nullptr, *proj_t = nullptr, *ethp_t = nullptr,
           *source = nullptr, *forcing = nullptr;
   double* pool = nullptr;
+  // composite tile operators (angular_tile_kernel)
+  double* tile_fp64 = nullptr;
+  uint2* tile_split = nullptr;
+  double* tile_scales = nullptr;
+  const int* tile_offsets[cCount][4] = {};
   double* trig_data = nullptr;
   int* ints = nullptr;
   double* norm_acc = nullptr;
@@ -1090,8 +1387,11 @@ struct NodalPipeline::Buffers {
   }
 };
 
-NodalPipeline::NodalPipeline(const InstancePlan& plan)
-    : plan_(plan), buf_(std::make_unique<Buffers>()) {
+NodalPipeline::NodalPipeline(const InstancePlan& plan, const int precision)
+    : plan_(plan), precision_(precision), buf_(std::make_unique<Buffers>()) {
+  if (precision != kPrecisionFp64 && precision != kPrecisionSplit) {
+    throw std::invalid_argument("unknown transform precision");
+  }
   const Config& c = plan_.config;
   if (c.ntheta > kMaxNodes) {
     throw std::invalid_argument(
@@ -1173,6 +1473,12 @@ NodalPipeline::NodalPipeline(const InstancePlan& plan)
   b.pairs_t = b.alloc<double2>(std::max<size_t>(pair_index1_.size(), 1) * 2 * b.plane);
 
   build_coordinators();
+  tile_operators_ = c.ntheta <= kTileMaxNodes;
+  if (precision_ == kPrecisionSplit && !tile_operators_) {
+    throw std::invalid_argument(
+        "split-precision transforms support at most 64 theta nodes");
+  }
+  if (tile_operators_) build_tile_operators();
 
   // integer tables: mvals, sharp, pairs, coordinator tables
   std::vector<int> ints;
@@ -1235,6 +1541,38 @@ NodalPipeline::NodalPipeline(const InstancePlan& plan)
   check(cudaMemcpy(b.pool, matrices_.data(), matrices_.size() * sizeof(double),
                    cudaMemcpyHostToDevice),
         "upload matrices");
+  if (tile_operators_) {
+    b.tile_fp64 = b.alloc<double>(tile_fp64_.size());
+    b.tile_split = b.alloc<uint2>(tile_split_.size());
+    b.tile_scales = b.alloc<double>(tile_scales_.size());
+    check(cudaMemcpy(b.tile_fp64, tile_fp64_.data(),
+                     tile_fp64_.size() * sizeof(double), cudaMemcpyHostToDevice),
+          "upload tile operators");
+    check(cudaMemcpy(b.tile_split, tile_split_.data(),
+                     tile_split_.size() * sizeof(uint2), cudaMemcpyHostToDevice),
+          "upload split tile operators");
+    check(cudaMemcpy(b.tile_scales, tile_scales_.data(),
+                     tile_scales_.size() * sizeof(double), cudaMemcpyHostToDevice),
+          "upload tile operator scales");
+    std::vector<int> offs;
+    for (int k = 0; k < cCount; ++k) {
+      for (int kind = 0; kind < 4; ++kind) {
+        const auto& v = tile_offsets_[k][kind];
+        offs.insert(offs.end(), v.begin(), v.end());
+      }
+    }
+    int* d_offs = b.alloc<int>(offs.size());
+    check(cudaMemcpy(d_offs, offs.data(), offs.size() * sizeof(int),
+                     cudaMemcpyHostToDevice),
+          "upload tile operator offsets");
+    size_t at = 0;
+    for (int k = 0; k < cCount; ++k) {
+      for (int kind = 0; kind < 4; ++kind) {
+        b.tile_offsets[k][kind] = d_offs + at;
+        at += tile_offsets_[k][kind].size();
+      }
+    }
+  }
   // trig: theta_sin, theta_cos, grid_sin, grid_cos
   const size_t nt = static_cast<size_t>(c.ntheta);
   std::vector<double> trig(4 * nt);
@@ -1379,6 +1717,124 @@ void NodalPipeline::build_coordinators() {
   }
 }
 
+// Host digits of w (|w| < 1), the same cut as split_digits on the device.
+static void host_split_digits(const double w, float (&t)[kSplitSlices]) {
+  double r = w * 128.0;
+  for (int s = 0; s < kSplitSlices; ++s) {
+    const double d = std::nearbyint(r);
+    t[s] = static_cast<float>(d);
+    r = (r - d) * 256.0;
+  }
+}
+
+static unsigned host_pack_bf16(const float lo, const float hi) {
+  unsigned a = 0, b = 0;
+  std::memcpy(&a, &lo, sizeof(a));
+  std::memcpy(&b, &hi, sizeof(b));
+  return (a >> 16) | (b & 0xffff0000u);
+}
+
+// Composite nodal matrices T = S_out diag(d) A of every (coordinator,
+// operation, active mode), accumulated in long double and rounded once, and
+// their tensor-core fragment layouts: FP64 B fragments of T^T for
+// mma.sync m8n8k4, and BF16 digit fragments with per-column power-of-two
+// scales for the split-precision m16n8k16 path.
+void NodalPipeline::build_tile_operators() {
+  const Config& c = plan_.config;
+  const int nt = c.ntheta;
+  const size_t nm = c.modes.size();
+  const int n8 = (nt + 7) / 8, k4 = (nt + 3) / 4, k16 = (nt + 15) / 16;
+  std::vector<double> T(static_cast<size_t>(nt) * nt);
+  for (int k = 0; k < cCount; ++k) {
+    const AngularCoordinator& a = coordinators_[k];
+    for (int kind = 0; kind < 4; ++kind) {
+      std::vector<int>& offs = tile_offsets_[k][kind];
+      offs.assign(3 * nm, 0);
+      for (size_t i = 0; i < nm; ++i) {
+        if (!a.active[i]) continue;
+        const int ne = a.n_ell[i], lmin = a.ell_min[i];
+        int o_off = a.synthesis[i], ne_o = ne, lmin_o = lmin, diag = -1;
+        if (kind == kLaplacian) diag = coordinator_diag_[k][0][i];
+        if (kind == kEth) {
+          o_off = a.raised[i];
+          ne_o = a.n_ell_up[i];
+          lmin_o = a.ell_min_up[i];
+          diag = coordinator_diag_[k][1][i];
+        } else if (kind == kEthPrime) {
+          o_off = a.lowered[i];
+          ne_o = a.n_ell_down[i];
+          lmin_o = a.ell_min_down[i];
+          diag = coordinator_diag_[k][2][i];
+        }
+        const int shift = lmin_o - lmin;
+        const double* A = matrices_.data() + a.analysis[i];  // [node][ell]
+        const double* S = matrices_.data() + o_off;          // [ell][node]
+        for (int j = 0; j < nt; ++j) {
+          for (int kk = 0; kk < nt; ++kk) {
+            long double v = 0.0L;
+            for (int l = 0; l < ne_o; ++l) {
+              const int src = l + shift;
+              if (src < 0 || src >= ne) continue;
+              long double term = static_cast<long double>(S[l * nt + j]) *
+                                 static_cast<long double>(A[kk * ne + src]);
+              if (diag >= 0) term *= static_cast<long double>(matrices_[diag + src]);
+              v += term;
+            }
+            T[static_cast<size_t>(j) * nt + kk] = static_cast<double>(v);
+          }
+        }
+        const auto at = [&](const int j, const int kk) {
+          return (j < nt && kk < nt) ? T[static_cast<size_t>(j) * nt + kk] : 0.0;
+        };
+        offs[3 * i] = static_cast<int>(tile_fp64_.size());
+        for (int n = 0; n < n8; ++n) {
+          for (int ks = 0; ks < k4; ++ks) {
+            for (int lane = 0; lane < 32; ++lane) {
+              tile_fp64_.push_back(at(n * 8 + lane / 4, ks * 4 + lane % 4));
+            }
+          }
+        }
+        // split: per output node j a power-of-two scale and five digits
+        std::vector<float> digits(static_cast<size_t>(n8) * 8 * k16 * 16 * kSplitSlices, 0.0f);
+        const auto digit = [&](const int j, const int kk, const int t) -> float& {
+          return digits[((static_cast<size_t>(j) * k16 * 16) + kk) * kSplitSlices + t];
+        };
+        offs[3 * i + 2] = static_cast<int>(tile_scales_.size());
+        for (int j = 0; j < n8 * 8; ++j) {
+          double m = 0.0;
+          for (int kk = 0; kk < nt; ++kk) m = std::max(m, std::fabs(at(j, kk)));
+          int e = 0;
+          std::frexp(m, &e);
+          e = m == 0.0 ? 0 : std::max(e, -1000);
+          tile_scales_.push_back(j < nt ? std::ldexp(1.0, e - 14) : 0.0);
+          for (int kk = 0; kk < nt; ++kk) {
+            float t[kSplitSlices];
+            host_split_digits(at(j, kk) * std::ldexp(1.0, -e), t);
+            for (int s = 0; s < kSplitSlices; ++s) digit(j, kk, s) = t[s];
+          }
+        }
+        offs[3 * i + 1] = static_cast<int>(tile_split_.size());
+        for (int n = 0; n < n8; ++n) {
+          for (int ks = 0; ks < k16; ++ks) {
+            for (int t = 0; t < kSplitSlices; ++t) {
+              for (int lane = 0; lane < 32; ++lane) {
+                const int j = n * 8 + lane / 4, kk = ks * 16 + 2 * (lane % 4);
+                uint2 f;
+                f.x = host_pack_bf16(digit(j, kk, t), digit(j, kk + 1, t));
+                f.y = host_pack_bf16(digit(j, kk + 8, t), digit(j, kk + 9, t));
+                tile_split_.push_back(f);
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  if (tile_fp64_.empty()) tile_fp64_.push_back(0.0);
+  if (tile_split_.empty()) tile_split_.push_back(uint2{0u, 0u});
+  if (tile_scales_.empty()) tile_scales_.push_back(0.0);
+}
+
 void NodalPipeline::sync_check(const char* what) {
   check(cudaGetLastError(), what);
 }
@@ -1428,6 +1884,30 @@ void NodalPipeline::evaluate(const double2* stage_in, double2* out) {
       p.ne_o = d.ne_down;
       p.lmin_o = d.lmin_down;
       p.diag_off = d.lower_diag;
+    }
+    if (tile_operators_) {
+      AngularTileParams tp{};
+      tp.kind = kind;
+      tp.in = in;
+      tp.in_slot = in_slot;
+      tp.dt = dt;
+      tp.dt_slot = dt_slot;
+      tp.out = o;
+      tp.out_slot = out_slot;
+      tp.active = d.active;
+      tp.offsets = b.tile_offsets[coord][kind];
+      tp.fp64 = b.tile_fp64;
+      tp.split = b.tile_split;
+      tp.scales = b.tile_scales;
+      tp.spin = p.spin;
+      tp.boost = p.boost;
+      const int tiles = g.modes * ((g.nr + kTileCtaRows - 1) / kTileCtaRows);
+      if (precision_ == kPrecisionSplit) {
+        angular_tile_kernel<kPrecisionSplit><<<tiles, kTileWarps * 32, 0, s>>>(g, tr, tp);
+      } else {
+        angular_tile_kernel<kPrecisionFp64><<<tiles, kTileWarps * 32, 0, s>>>(g, tr, tp);
+      }
+      return;
     }
     angular_op_kernel<<<ga, kBlock, 0, s>>>(g, tr, p);
   };

@@ -82,7 +82,10 @@ cudaError_t launch_diagnostics(const DiagnosticsLaunch& launch,
 class NodalPipeline {
  public:
   struct Buffers;
-  explicit NodalPipeline(const InstancePlan& plan);
+  // precision 0: FP64 transforms; 1: split-precision (BF16 digits, FP32
+  // accumulation, FP64 recombination) tensor-core transforms
+  explicit NodalPipeline(const InstancePlan& plan, int precision = 0);
+  int precision() const { return precision_; }
   ~NodalPipeline();
   NodalPipeline(const NodalPipeline&) = delete;
   NodalPipeline& operator=(const NodalPipeline&) = delete;
@@ -114,6 +117,7 @@ class NodalPipeline {
 
  private:
   void build_coordinators();
+  void build_tile_operators();
   void evaluate(const double2* stage, double2* out);
   void consider_activation(double accepted_time);
   void advance_fixed(double time, double dt);
@@ -129,6 +133,13 @@ class NodalPipeline {
   void sync_check(const char* what);
 
   InstancePlan plan_;
+  int precision_ = 0;
+  // composite tile operators: used when ntheta <= 64
+  bool tile_operators_ = false;
+  std::vector<double> tile_fp64_;
+  std::vector<uint2> tile_split_;
+  std::vector<double> tile_scales_;
+  std::vector<int> tile_offsets_[10][4];  // [coordinator][operation]: 3 per mode
   std::vector<int> pair_index1_, pair_index2_, pair_offsets_, targets_;
   std::vector<AngularCoordinator> coordinators_;
   // per coordinator: pool offsets of the Laplacian / raising / lowering

@@ -103,6 +103,7 @@ class _ServerOptions(ctypes.Structure):
         ("hbm_budget_bytes", ctypes.c_size_t),
         ("max_active", ctypes.c_int),
         ("graph", ctypes.c_int),
+        ("precision", ctypes.c_int),
     ]
 
 
@@ -830,9 +831,9 @@ class Server:
     one shared batched step, and leave with their waveform records."""
 
     def __init__(self, hbm_budget_bytes: int, max_active: int = 0,
-                 graph: bool = True):
+                 graph: bool = True, precision: int = PRECISION_FP64):
         opts = _ServerOptions(ABI_VERSION, int(hbm_budget_bytes),
-                              int(max_active), int(graph))
+                              int(max_active), int(graph), int(precision))
         handle = ctypes.c_void_p()
         _check(_lib.teuk_b200_server_create(ctypes.byref(opts),
                                             ctypes.byref(handle)))
