@@ -68,6 +68,7 @@ def parse_args():
     p.add_argument("--serve-steps", type=int, default=100,
                    help="RK4 steps per serving request")
     p.add_argument("--no-uneven", action="store_true")
+    p.add_argument("--no-split", action="store_true")
     p.add_argument("--so-steps", type=int, default=20,
                    help="timed RK4 steps of the quadratic-source solve")
     p.add_argument("--uneven-steps", type=int, default=20,
@@ -565,7 +566,7 @@ def reference_arm(args):
 
 
 # ---------------------------------------------------------------- GPU side
-def build_batch(tb, wl, config, pulse, batch_size, seed0, pinned):
+def build_batch(tb, wl, config, pulse, batch_size, seed0, pinned, options=None):
     """A batch of `batch_size` copies of the workload with seeded amplitudes
     and noise.  Initial states are linear combinations of two unit-amplitude
     Gaussian states (the system is linear) plus the seeded noise; they are
@@ -579,7 +580,7 @@ def build_batch(tb, wl, config, pulse, batch_size, seed0, pinned):
                                                    modes=[(2, m, 1.0)]))
         units.append(probe.get_state())
     probe.close()
-    batch = tb.Batch([config] * batch_size)
+    batch = tb.Batch([config] * batch_size, options)
     rng = np.random.Generator(np.random.PCG64(seed0))
     for i in range(batch_size):
         a = 1e-3 * complex(rng.standard_normal(), rng.standard_normal())
@@ -653,6 +654,39 @@ def b200_arm(args):
     kernel = "stream_stage_kernel" if streaming else "stage_kernel"
     traffic = recorded_traffic(kernel, algorithmic_per_launch)
 
+    # the same batch with split-precision transforms (BF16 digit slices,
+    # FP32 accumulation, FP64 recombination), same inputs and steps
+    split = None
+    if not args.no_split:
+        sbatch = build_batch(tb, wl, config, pulse, B, 1000 * (rank + 1), pinned,
+                             tb.LaunchOptions(precision=tb.PRECISION_SPLIT))
+        sbatch.set_stream(stream.cuda_stream)
+        sbatch.step(dts, steps=max(args.warmup, 0), graph=True)
+        sbatch.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        sbatch.step(dts, steps=args.steps, graph=True)
+        s1.record(stream)
+        s1.synchronize()
+        barrier()
+        s_value, s_slowest = td.whole_job_rate(B * gp * args.steps,
+                                               s0.elapsed_time(s1) / 1e3, "cuda")
+        a_end = batch.endpoint_modal()
+        b_end = sbatch.endpoint_modal()
+        dev = float(np.max(np.abs(a_end - b_end)) / max(np.max(np.abs(a_end)), 1e-300))
+        split = {"value": s_value, "unit": UNIT,
+                 "ms_per_step": 1e3 * s_slowest / args.steps,
+                 "vs_fp64": s_value / value,
+                 "endpoint_deviation_vs_fp64": dev,
+                 "method": "streaming-kernel transforms through BF16 digit "
+                           "slices (5 per operand, 15 products), FP32 "
+                           "accumulation, FP64 recombination; stencils, RK "
+                           "and projection FP64"}
+        sbatch.close()
+
     # end-to-end through the C ABI with host buffers
     e2e = None
     if not args.no_e2e:
@@ -718,6 +752,7 @@ def b200_arm(args):
                          "peak_source": f"{peak_kind} hbm_gbs",
                          "algorithmic_bytes_per_launch": algorithmic_per_launch},
             "cpu_baseline": cpu,
+            "split_precision": split,
             "e2e": e2e,
             "serving": serving,
             "uneven_batch": uneven,

@@ -1,8 +1,10 @@
 """Split-precision tensor-core transforms against the FP64 reference (GPU).
 
-With ``LaunchOptions(precision=PRECISION_SPLIT)`` the angular operators
-(project, Laplacian, eth, eth') multiply through BF16 digit slices with FP32
-accumulation and FP64 recombination; everything else stays FP64.  The stated
+With ``LaunchOptions(precision=PRECISION_SPLIT)`` the transforms multiply
+through BF16 digit slices with FP32 accumulation and FP64 recombination
+(split_precision.cuh): in the second-order pipeline the angular operators
+(project, Laplacian, eth, eth'), in the linear streaming kernel the synthesis
+and analysis of the implicit Kerr ell-coupling; everything else stays FP64.  The stated
 bound for this path is 1e-9 relative to each field's maximum modulus against
 the reference build (the plain FP64 path is held to 1e-10 elsewhere), with
 activation records exact.
@@ -87,3 +89,65 @@ def test_split_precision_is_rejected_above_64_nodes(require_gpu):
         discretization=tb.D42, source_mode=tb.SOURCE_UNRESTRICTED)
     with pytest.raises(tb.InvalidArgument, match="at most 64 theta nodes"):
         tb.Pipeline(config, SPLIT)
+
+
+def test_split_kerr_ringdown_nr1025_100_steps(require_gpu):
+    """The linear Kerr ringdown at its full shape (a 0.7, nr 1025, D10-5,
+    m = -4..4, ell <= 16) on the streaming kernel with split-precision
+    transforms: within 1e-9 of the reference after 100 steps."""
+    config, pulse, dt = wl.kerr_ringdown()
+    ref = RefPipeline(config, threads=True)
+    ref.initialize_gaussian(pulse)
+    state = ref.get_state() + ref.project_to_bands(wl.band_noise(config, 7))
+    ref.set_state(state)
+    split = tb.Pipeline(config, SPLIT)
+    split.set_state(state)
+    split.step(0.0, dt, 100)
+    ref.step(0.0, dt, 100)
+    errors = _field_errors(split.get_state(), ref.get_state(), range(3))
+    assert max(errors) < SPLIT_TOL, errors
+
+
+@pytest.mark.parametrize("reduction", [tb.FREE_DAMPED, tb.STAGE_CONSTRAINED])
+def test_split_linear_rhs_and_steps(require_gpu, reduction):
+    """Both reductions of the streaming kernel (D8-4, several strips)."""
+    config = tb.SolveConfig(
+        mass=1.0, spin=0.8, compactification_length=1.0, radial_points=300,
+        theta_nodes=25, ell_max_first=16, ell_max_second=16,
+        modes=tuple(range(-4, 5)), dissipation=0.003,
+        discretization=tb.D84, reduction=reduction)
+    ref = RefPipeline(config)
+    from cases import pulse_for, step_size
+    pulse = pulse_for(config, 3)
+    ref.initialize_gaussian(pulse)
+    split = tb.Pipeline(config, SPLIT)
+    split.initialize_gaussian(pulse)
+    dt = step_size(config, 0.1)
+    split.step(0.0, dt, 20)
+    ref.step(0.0, dt, 20)
+    errors = _field_errors(split.get_state(), ref.get_state(), range(3))
+    assert max(errors) < SPLIT_TOL, errors
+
+
+def test_split_batch_member_equals_solo(require_gpu):
+    """Split-precision results depend only on each row's own data: a solve
+    in a mixed batch equals the same solve alone, bit for bit."""
+    from cases import pulse_for, step_size
+    base = tb.SolveConfig(
+        mass=1.0, spin=0.7, compactification_length=1.0, radial_points=300,
+        theta_nodes=25, ell_max_first=16, ell_max_second=16,
+        modes=tuple(range(-4, 5)), dissipation=0.005, discretization=tb.D105)
+    configs = [base, replace(base, radial_points=129, spin=0.3),
+               replace(base, radial_points=513, spin=0.9, ell_max_first=12,
+                       ell_max_second=12, theta_nodes=19)]
+    pulses = [pulse_for(c, 31 + i) for i, c in enumerate(configs)]
+    dts = [step_size(c, 0.1) for c in configs]
+    batch = tb.Batch(configs, SPLIT)
+    for i, p in enumerate(pulses):
+        batch.initialize_gaussian(i, p)
+    batch.step(dts, 5)
+    for i, c in enumerate(configs):
+        solo = tb.Pipeline(c, SPLIT)
+        solo.initialize_gaussian(pulses[i])
+        solo.step(0.0, dts[i], 5)
+        assert np.array_equal(batch.get_state(i), solo.get_state()), i

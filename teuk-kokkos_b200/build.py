@@ -25,7 +25,7 @@ SOURCES = ["plan.cpp", "checkpoint.cpp", "run_config.cpp", "kernels.cu",
            "second_order.cu",
            "static_scratch.cu", "api.cu"]
 HEADERS = ["engine.h", "kernels.h", "second_order.h", "stream_kernel.cuh", "static_scratch.h",
-           "checkpoint.h", "run_config.h", "sbp_tables.h"]
+           "checkpoint.h", "run_config.h", "sbp_tables.h", "split_precision.cuh"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -30,6 +30,7 @@
 #include "checkpoint.h"
 #include "run_config.h"
 #include "second_order.h"
+#include "split_precision.cuh"
 #include "static_scratch.h"
 #include "teuk_b200.h"
 
@@ -285,6 +286,11 @@ struct Batch {
   std::vector<std::vector<int>> group_segments_;  // segments of each group
   int coef_rows = 0;
   DeviceArray<double> d_mat, d_trig;
+  // split-precision digit records of every segment (streaming kernel)
+  std::vector<uint4> h_split;
+  std::vector<double> h_split_scale;
+  DeviceArray<uint4> d_split;
+  DeviceArray<double> d_split_scale;
   DeviceArray<double2> d_nodal;     // one instance's nodal state (lazy)
   size_t nodal_max = 0;
   DeviceArray<double2> d_endpoint;  // gathered endpoint coefficients
@@ -350,10 +356,6 @@ struct Batch {
       throw std::invalid_argument("a batch needs at least one solve");
     }
     plans = std::move(planned);
-    if (options.precision == TEUK_B200_PRECISION_SPLIT) {
-      throw Unsupported(
-          "split-precision transforms are not built for linear pipelines");
-    }
     for (const InstancePlan& plan : plans) {
       const Config& c = plan.config;
       if (c.source_mode != 0) {
@@ -414,6 +416,7 @@ struct Batch {
             h_mat.push_back(mp.analysis[static_cast<size_t>(l) * nt + j]);
           }
         }
+        append_split_record(mp, nt);
         mp.segment = static_cast<long long>(h_seg.size());
         instance_segments.back().push_back(static_cast<int>(h_seg.size()));
         h_seg.push_back(s);
@@ -540,6 +543,8 @@ struct Batch {
     alloc(d_coef, static_cast<size_t>(std::max(coef_rows, 1)) * kCoefRecord);
     alloc(d_nodes, static_cast<size_t>(std::max(coef_rows, 1)) * kNodeRecord);
     alloc(d_mat, std::max<size_t>(h_mat.size(), 1));
+    alloc(d_split, std::max<size_t>(h_split.size(), 1));
+    alloc(d_split_scale, std::max<size_t>(h_split_scale.size(), 1));
     alloc(d_trig, h_trig.size());
     alloc(d_endpoint,
           std::max<size_t>(h_seg.size(), 1) * 2 * static_cast<size_t>(max_ell));
@@ -578,6 +583,15 @@ struct Batch {
                        cudaMemcpyHostToDevice),
             "upload matrices");
     }
+    if (!h_split.empty()) {
+      check(cudaMemcpy(d_split.ptr, h_split.data(), h_split.size() * sizeof(uint4),
+                       cudaMemcpyHostToDevice),
+            "upload split records");
+      check(cudaMemcpy(d_split_scale.ptr, h_split_scale.data(),
+                       h_split_scale.size() * sizeof(double),
+                       cudaMemcpyHostToDevice),
+            "upload split scales");
+    }
     check(cudaMemcpy(d_trig.ptr, h_trig.data(), h_trig.size() * sizeof(double),
                      cudaMemcpyHostToDevice),
           "upload trig");
@@ -594,6 +608,9 @@ struct Batch {
       g.coef_table = d_coef.ptr;
       g.node_table = d_nodes.ptr;
       g.withhold_chunk = withhold_chunk_;
+      g.precision = options.precision == TEUK_B200_PRECISION_SPLIT ? 1 : 0;
+      g.split_frags = d_split.ptr;
+      g.split_scales = d_split_scale.ptr;
       if (group_first_strip[gi] >= 0) {
         g.strips = d_strips.ptr + group_first_strip[gi];
       } else {
@@ -610,6 +627,74 @@ struct Batch {
       g.acc = acc.ptr;
     }
     if (options.autotune != 0 && options.strip_rows == 0) autotune_strips();
+  }
+
+  // Split-precision digit record of one segment for the streaming kernel's
+  // transforms: BF16 digit fragments of the synthesis matrix S(j, l) (rows =
+  // nodes, one power-of-two scale per node) and of the analysis matrix
+  // A(l, j) (rows = ell, one scale per ell), in the m16n8k16 A-operand
+  // layout of the two transform warps, [synthesis h0, h1, analysis h0,
+  // h1][slice][lane]; then 32 node scales and 16 ell scales 2^(F - 14).
+  // Segments outside the streaming kernel's shapes get a zero record.
+  void append_split_record(const ModePlan& mp, const int nt) {
+    namespace sp = teuk_b200::split;
+    const int ne = mp.n_ell;
+    const bool fits = ne <= kStreamMaxEll && nt <= kStreamMaxNodes;
+    const size_t base = h_split.size();
+    h_split.resize(base + kSplitRecordUint4, uint4{0u, 0u, 0u, 0u});
+    const size_t sbase = h_split_scale.size();
+    h_split_scale.resize(sbase + kSplitScaleDoubles, 0.0);
+    if (!fits) return;
+    const auto S = [&](const int j, const int l) {
+      return (j < nt && l < ne) ? mp.synthesis[static_cast<size_t>(j) * ne + l] : 0.0;
+    };
+    const auto A = [&](const int l, const int j) {
+      return (j < nt && l < ne) ? mp.analysis[static_cast<size_t>(l) * nt + j] : 0.0;
+    };
+    // digits[row][k][slice] of the row-scaled matrices (16 x 32 / 32 x 16)
+    float ds[kStreamMaxNodes][kStreamMaxEll][sp::kSlices] = {};
+    float da[kStreamMaxEll][kStreamMaxNodes][sp::kSlices] = {};
+    for (int j = 0; j < kStreamMaxNodes; ++j) {
+      double m = 0.0;
+      for (int l = 0; l < kStreamMaxEll; ++l) m = std::max(m, std::fabs(S(j, l)));
+      const int e = sp::host_exponent(m);
+      h_split_scale[sbase + j] = std::ldexp(1.0, e - 14);
+      for (int l = 0; l < kStreamMaxEll; ++l) {
+        sp::host_digits(S(j, l) * std::ldexp(1.0, -e), ds[j][l]);
+      }
+    }
+    for (int l = 0; l < kStreamMaxEll; ++l) {
+      double m = 0.0;
+      for (int j = 0; j < kStreamMaxNodes; ++j) m = std::max(m, std::fabs(A(l, j)));
+      const int e = sp::host_exponent(m);
+      h_split_scale[sbase + kStreamMaxNodes + l] = std::ldexp(1.0, e - 14);
+      for (int j = 0; j < kStreamMaxNodes; ++j) {
+        sp::host_digits(A(l, j) * std::ldexp(1.0, -e), da[l][j]);
+      }
+    }
+    for (int h = 0; h < 2; ++h) {
+      for (int sl = 0; sl < sp::kSlices; ++sl) {
+        for (int lane = 0; lane < 32; ++lane) {
+          const int g = lane / 4, q = lane % 4;
+          // synthesis: rows nodes 16h + g (+8), k = ell
+          const int j0 = 16 * h + g, j1 = j0 + 8;
+          uint4 f;
+          f.x = sp::host_pack(ds[j0][2 * q][sl], ds[j0][2 * q + 1][sl]);
+          f.y = sp::host_pack(ds[j1][2 * q][sl], ds[j1][2 * q + 1][sl]);
+          f.z = sp::host_pack(ds[j0][2 * q + 8][sl], ds[j0][2 * q + 9][sl]);
+          f.w = sp::host_pack(ds[j1][2 * q + 8][sl], ds[j1][2 * q + 9][sl]);
+          h_split[base + (h * sp::kSlices + sl) * 32 + lane] = f;
+          // analysis: rows ell g (+8), k = nodes 16h + 2q (+1, +8, +9)
+          const int k0 = 16 * h + 2 * q;
+          uint4 a;
+          a.x = sp::host_pack(da[g][k0][sl], da[g][k0 + 1][sl]);
+          a.y = sp::host_pack(da[g + 8][k0][sl], da[g + 8][k0 + 1][sl]);
+          a.z = sp::host_pack(da[g][k0 + 8][sl], da[g][k0 + 9][sl]);
+          a.w = sp::host_pack(da[g + 8][k0 + 8][sl], da[g + 8][k0 + 9][sl]);
+          h_split[base + ((2 + h) * sp::kSlices + sl) * 32 + lane] = a;
+        }
+      }
+    }
   }
 
   // Radial strips of a streaming launch group (its segments `segs`) for a

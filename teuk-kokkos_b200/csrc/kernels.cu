@@ -20,6 +20,7 @@
 #include <unordered_map>
 
 #include "kernels.h"
+#include "split_precision.cuh"
 
 namespace teuk_b200 {
 
@@ -996,10 +997,13 @@ class KernelSetups {
   std::unordered_map<int, KernelSetup> per_device_;
 };
 
-template <int DISC, int SC>
+static_assert(kSplitRecord == kSplitRecordUint4, "split record size");
+static_assert(kSplitScales == kSplitScaleDoubles, "split scale count");
+
+template <int DISC, int SC, int PREC>
 cudaError_t launch_stream_typed(const StageLaunch& p, cudaStream_t stream) {
   const size_t bytes = StreamLayout(SC).total;
-  auto kernel = stream_stage_kernel<DISC, SC>;
+  auto kernel = stream_stage_kernel<DISC, SC, PREC>;
   static KernelSetups setups;
   int sms = 0;
   const cudaError_t setup_err = setups.with([&](KernelSetup& k, const int device) {
@@ -1039,7 +1043,8 @@ cudaError_t launch_stream_typed(const StageLaunch& p, cudaStream_t stream) {
 template <int DISC, int SC>
 cudaError_t launch_typed(const StageLaunch& p, cudaStream_t stream) {
   if (p.strips != nullptr && p.strip_count > 0) {
-    return launch_stream_typed<DISC, SC>(p, stream);
+    return p.precision == 1 ? launch_stream_typed<DISC, SC, 1>(p, stream)
+                            : launch_stream_typed<DISC, SC, 0>(p, stream);
   }
   const size_t bytes = stage_smem_bytes(p);
   auto kernel = stage_kernel<DISC, SC>;

@@ -55,6 +55,14 @@ struct StageLaunch {
   // 1 / C_T(r, theta_j) of every solve on its Gauss-Legendre nodes,
   // kNodeRecord doubles per radial row (zero beyond the solve's nodes)
   const double* node_table;
+  // Transform precision of Kerr bands on the streaming kernel: 0 FP64,
+  // 1 split precision (BF16 digit slices, split_precision.cuh) with the
+  // per-segment digit records below (kSplitRecordUint4 uint4 and
+  // kSplitScaleDoubles doubles per segment, indexed by segment).  Tile-kernel
+  // bands always run FP64.
+  int precision;
+  const uint4* split_frags;
+  const double* split_scales;
   // Failure-detection test hook (-1: off): in stage-1 launches the producer
   // of CTA 0 never issues this chunk, so the waits for it run out and the
   // launch reports a timeout through `error`.
@@ -66,6 +74,8 @@ struct StageLaunch {
 inline constexpr int kStreamMaxEll = 16;
 inline constexpr int kStreamMaxNodes = 32;
 
+inline constexpr int kSplitRecordUint4 = 4 * 5 * 32;
+inline constexpr int kSplitScaleDoubles = kStreamMaxNodes + kStreamMaxEll;
 inline constexpr int kCoefRecord = 10;
 inline constexpr int kNodeRecord = kStreamMaxNodes;
 // Fills the coefficient table rows of one solve, table[(row0 + r) * 10 + k],

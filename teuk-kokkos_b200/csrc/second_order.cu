@@ -11,6 +11,7 @@
 #include <string>
 
 #include "second_order.h"
+#include "split_precision.cuh"
 #include "teuk_b200.h"
 
 namespace teuk_b200 {
@@ -398,24 +399,15 @@ __global__ void angular_op_kernel(const Geo g, const Trig tr,
 // one mode (a warp 8), stages them in shared memory and multiplies on the
 // tensor cores: in FP64 (mma.sync m8n8k4), or in split precision.
 //
-// Split precision (Ozaki, Ogita, Oishi & Rump, "Error-free transformations
-// of matrix multiplication by using fast routines of matrix multiplication
-// and its applications", Numer. Algorithms 59, 2012): every real row of x and
-// every column of T is scaled by a power of two to below 1 in modulus and cut
-// into five signed 8-bit digits, d = sum_s t_s 2^(-7-8s), |t_s| <= 128, each
-// exact in BF16.  Digit products are integers below 2^14 and a K <= 64 sum of
-// up to five of them stays below 2^24, so the BF16 tensor-core products
-// accumulated in FP32 (mma.sync m16n8k16) are exact; the 15 digit pairs with
-// s + t <= 4 are summed in five FP32 accumulators (one per s + t) and
-// recombined in FP64 with the two scales.  The dropped pairs and the digit
-// remainders leave an error of about 2^-40 of max|x_row| max|T_col| per term.
+// Split precision: the digit scheme of split_precision.cuh (BF16 digit
+// slices, exact FP32 accumulation, FP64 recombination).
 constexpr int kTileRows = 8;     // complex rows of one MMA row tile
 constexpr int kTileWarps = 4;    // two warps per row tile, each half the nodes
 constexpr int kTileCtaRows = 16; // two row tiles per CTA
 constexpr int kTileMaxNodes = 64;                // nodes of the tile kernel
 constexpr int kTileStride = kTileMaxNodes + 4;   // staged row stride
 constexpr int kTileLoads = kTileCtaRows * kTileMaxNodes / (kTileWarps * 32);
-constexpr int kSplitSlices = 5;
+constexpr int kSplitSlices = split::kSlices;
 constexpr int kPrecisionFp64 = 0;
 constexpr int kPrecisionSplit = 1;
 
@@ -444,41 +436,6 @@ __device__ __forceinline__ void dmma_tile(double& c0, double& c1, const double a
       "{%0,%1};\n"
       : "+d"(c0), "+d"(c1)
       : "d"(a), "d"(b));
-}
-
-__device__ __forceinline__ void hmma_bf16(float (&c)[4], const unsigned (&a)[4],
-                                          const uint2 b) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-      "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b.x), "r"(b.y));
-}
-
-// Five signed 8-bit digits of w (|w| < 1): w = sum_s t_s 2^(-7-8s) up to
-// 2^-40; every step is exact in binary64.
-__device__ __forceinline__ void split_digits(const double w, float (&t)[kSplitSlices]) {
-  double r = w * 128.0;
-#pragma unroll
-  for (int s = 0; s < kSplitSlices; ++s) {
-    const double d = rint(r);
-    t[s] = static_cast<float>(d);
-    r = (r - d) * 256.0;
-  }
-}
-
-// Two BF16 values in one register, `lo` in the low half (exact: the digits
-// are integers of at most 8 bits).
-__device__ __forceinline__ unsigned pack_bf16(const float lo, const float hi) {
-  return (__float_as_uint(lo) >> 16) | (__float_as_uint(hi) & 0xffff0000u);
-}
-
-// Power-of-two scale that brings |v| <= m below 1: returns 2^-e with
-// m = f 2^e, f in [0.5, 1) (e >= -1000 so the scale stays finite).
-__device__ __forceinline__ int scale_exponent(const double m) {
-  int e = 0;
-  frexp(m, &e);
-  return m == 0.0 ? 0 : max(e, -1000);
 }
 
 // Stages rows [r0, r0 + rows) of one (mode, slot) plane into split real /
@@ -613,7 +570,7 @@ __global__ void __launch_bounds__(kTileWarps * 32)
       mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
       mi = fmax(mi, __shfl_xor_sync(0xffffffffu, mi, o));
     }
-    const int er = scale_exponent(mr), ei = scale_exponent(mi);
+    const int er = split::exponent(mr), ei = split::exponent(mi);
     const double down_r = ldexp(1.0, -er), down_i = ldexp(1.0, -ei);
     // A fragments: rows 0-7 real parts, rows 8-15 imaginary parts of the
     // tile's 8 complex rows; every slice of every k step
@@ -625,15 +582,15 @@ __global__ void __launch_bounds__(kTileWarps * 32)
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           const int k = ks * 16 + 2 * q + (e & 1) + 8 * (e >> 1);
-          split_digits(xr[row][k] * down_r, t[e][0]);
-          split_digits(xi[row][k] * down_i, t[e][1]);
+          split::digits(xr[row][k] * down_r, t[e][0]);
+          split::digits(xi[row][k] * down_i, t[e][1]);
         }
 #pragma unroll
         for (int s = 0; s < kSplitSlices; ++s) {
-          a[ks][s][0] = pack_bf16(t[0][0][s], t[1][0][s]);
-          a[ks][s][1] = pack_bf16(t[0][1][s], t[1][1][s]);
-          a[ks][s][2] = pack_bf16(t[2][0][s], t[3][0][s]);
-          a[ks][s][3] = pack_bf16(t[2][1][s], t[3][1][s]);
+          a[ks][s][0] = split::pack(t[0][0][s], t[1][0][s]);
+          a[ks][s][1] = split::pack(t[0][1][s], t[1][1][s]);
+          a[ks][s][2] = split::pack(t[2][0][s], t[3][0][s]);
+          a[ks][s][3] = split::pack(t[2][1][s], t[3][1][s]);
         }
       }
     }
@@ -658,21 +615,14 @@ __global__ void __launch_bounds__(kTileWarps * 32)
           for (int s = 0; s < kSplitSlices; ++s) {
 #pragma unroll
             for (int t = 0; t + s < kSplitSlices; ++t) {
-              hmma_bf16(d[s + t], a[ks][s], b[t]);
+              split::mma_bf16(d[s + t], a[ks][s], b[t]);
             }
           }
         }
       }
       double v[4];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        double sum = static_cast<double>(d[kSplitSlices - 1][c]);
-#pragma unroll
-        for (int u = kSplitSlices - 2; u >= 0; --u) {
-          sum = fma(sum, 1.0 / 256.0, static_cast<double>(d[u][c]));
-        }
-        v[c] = sum;
-      }
+      for (int c = 0; c < 4; ++c) v[c] = split::recombine(d, c);
       const int j = n * 8 + 2 * q;
       const double s0 = colscale[j], s1 = colscale[j + 1];
       finish(j, v[0] * up_r * s0, v[2] * up_i * s0);
@@ -1717,23 +1667,6 @@ void NodalPipeline::build_coordinators() {
   }
 }
 
-// Host digits of w (|w| < 1), the same cut as split_digits on the device.
-static void host_split_digits(const double w, float (&t)[kSplitSlices]) {
-  double r = w * 128.0;
-  for (int s = 0; s < kSplitSlices; ++s) {
-    const double d = std::nearbyint(r);
-    t[s] = static_cast<float>(d);
-    r = (r - d) * 256.0;
-  }
-}
-
-static unsigned host_pack_bf16(const float lo, const float hi) {
-  unsigned a = 0, b = 0;
-  std::memcpy(&a, &lo, sizeof(a));
-  std::memcpy(&b, &hi, sizeof(b));
-  return (a >> 16) | (b & 0xffff0000u);
-}
-
 // Composite nodal matrices T = S_out diag(d) A of every (coordinator,
 // operation, active mode), accumulated in long double and rounded once, and
 // their tensor-core fragment layouts: FP64 B fragments of T^T for
@@ -1803,13 +1736,11 @@ void NodalPipeline::build_tile_operators() {
         for (int j = 0; j < n8 * 8; ++j) {
           double m = 0.0;
           for (int kk = 0; kk < nt; ++kk) m = std::max(m, std::fabs(at(j, kk)));
-          int e = 0;
-          std::frexp(m, &e);
-          e = m == 0.0 ? 0 : std::max(e, -1000);
+          const int e = split::host_exponent(m);
           tile_scales_.push_back(j < nt ? std::ldexp(1.0, e - 14) : 0.0);
           for (int kk = 0; kk < nt; ++kk) {
             float t[kSplitSlices];
-            host_split_digits(at(j, kk) * std::ldexp(1.0, -e), t);
+            split::host_digits(at(j, kk) * std::ldexp(1.0, -e), t);
             for (int s = 0; s < kSplitSlices; ++s) digit(j, kk, s) = t[s];
           }
         }
@@ -1820,8 +1751,8 @@ void NodalPipeline::build_tile_operators() {
               for (int lane = 0; lane < 32; ++lane) {
                 const int j = n * 8 + lane / 4, kk = ks * 16 + 2 * (lane % 4);
                 uint2 f;
-                f.x = host_pack_bf16(digit(j, kk, t), digit(j, kk + 1, t));
-                f.y = host_pack_bf16(digit(j, kk + 8, t), digit(j, kk + 9, t));
+                f.x = split::host_pack(digit(j, kk, t), digit(j, kk + 1, t));
+                f.y = split::host_pack(digit(j, kk + 8, t), digit(j, kk + 9, t));
                 tile_split_.push_back(f);
               }
             }

@@ -70,6 +70,10 @@ constexpr int kStreamRegisterDemand =
     32 * kStreamPWarps * kStreamPRegs;
 static_assert(kStreamRegisterDemand <= kStreamThreads * kStreamLaunchRegs,
               "register split fits the launch's registers");
+// split-precision record of one segment: [synthesis h0, h1, analysis h0,
+// h1][slice][lane] uint4, and 48 scales (32 node rows, 16 ell rows)
+constexpr int kSplitRecord = 4 * split::kSlices * 32;
+constexpr int kSplitScales = kStreamMaxTheta + kStreamNep;
 constexpr int kStreamXs = 20;  // padded staging strides (bank-conflict free)
 constexpr int kStreamTs = 36;
 
@@ -195,7 +199,7 @@ struct StreamLoaderState {
 struct StreamLayout {
   static constexpr int kRowMax = 3 * kStreamNep;  // complex per ring row
   size_t bars, loader, uring, xring, aring, pring, qring, coef, nodes, xw,
-      tw, total;
+      tw, ex, total;
   __host__ __device__ explicit StreamLayout(const int sc) {
     size_t o = 0;
     bars = o;
@@ -221,6 +225,8 @@ struct StreamLayout {
     o += static_cast<size_t>(kStreamBlocks) * 16 * kStreamXs * 8;
     tw = o;
     o += static_cast<size_t>(kStreamBlocks) * 8 * kStreamTs * 8;
+    ex = o;  // split precision: per block, 2 warps x 32 lanes x 2 doubles
+    o += static_cast<size_t>(kStreamBlocks) * 128 * 8;
     total = o;
   }
 };
@@ -576,7 +582,173 @@ __device__ __forceinline__ void stream_psi_half(
   }
 }
 
-template <int DISC, int SC>
+// Split-precision fragments of one transform warp (split_precision.cuh):
+// BF16 digits of its synthesis node tile (nodes 16h .. 16h + 15, all ell)
+// and of its half of the analysis K range (all ell, nodes 16h .. 16h + 15),
+// with the power-of-two scales of those matrix rows.
+struct SplitFragments {
+  unsigned s[split::kSlices][4];  // synthesis A operand: S(j, l)
+  unsigned a[split::kSlices][4];  // analysis A operand: A(l, j)
+  double node_scale[2];           // 2^(F_j - 14), j = 16h + grp, 16h + grp + 8
+  double ell_scale[2];            // 2^(F_l - 14), l = grp, grp + 8
+  double gcos[2];                 // 2 s a cos(theta_j), the same two nodes
+};
+
+// Split-precision digits of a B operand column held by a lane quad: the
+// four values of this lane, scaled by the quad's common power of two.
+__device__ __forceinline__ int split_column(const double (&v)[4],
+                                            uint2 (&b)[split::kSlices]) {
+  double m = fmax(fmax(fabs(v[0]), fabs(v[1])), fmax(fabs(v[2]), fabs(v[3])));
+  m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 1));
+  m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 2));
+  const int e = split::exponent(m);
+  const double down = ldexp(1.0, -e);
+  float t[4][split::kSlices];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) split::digits(v[i] * down, t[i]);
+#pragma unroll
+  for (int s = 0; s < split::kSlices; ++s) {
+    b[s].x = split::pack(t[0][s], t[1][s]);
+    b[s].y = split::pack(t[2][s], t[3][s]);
+  }
+  return e;
+}
+
+// The 15 digit-pair products of one m16n8k16 tile into five accumulators.
+__device__ __forceinline__ void split_products(
+    float (&d)[split::kSlices][4], const unsigned (&a)[split::kSlices][4],
+    const uint2 (&b)[split::kSlices]) {
+#pragma unroll
+  for (int u = 0; u < split::kSlices; ++u) d[u][0] = d[u][1] = d[u][2] = d[u][3] = 0.0f;
+#pragma unroll
+  for (int s = 0; s < split::kSlices; ++s) {
+#pragma unroll
+    for (int t = 0; s + t < split::kSlices; ++t) split::mma_bf16(d[s + t], a[s], b[t]);
+  }
+}
+
+// psi_t of the 4-row block at q0 in split precision: the same staging,
+// pointwise step and outputs as stream_psi_half.  Synthesis: this warp's
+// 16 nodes x 16 columns (rows x {v1, psi} x {re, im}) over K = 16 ell, two
+// m16n8k16 tiles.  Analysis: all 16 ell x 8 columns over K = this warp's 16
+// nodes, one tile; the two warps' partial sums are added through the
+// block's exchange buffer `ex` (two parities, so no extra barrier).
+template <int SC>
+__device__ __forceinline__ void stream_psi_split(
+    const int q0, const int qlim, const int h, const StripGeom& sg,
+    const double2* U, const double2* QE, const double* CF, const double* NI,
+    double2* PS, double* xw, double* tw, double* ex, const SplitFragments& F,
+    const int mts, const int bar, const int lane) {
+  const int quad = lane & 3;
+  const int group = lane >> 2;
+  const int ne = sg.ne;
+  const double mm = static_cast<double>(sg.m);
+  {  // stage rows 2h, 2h + 1 of the block: v1 = P + 2K Q - G psi, psi
+    const int rho = 2 * h + (lane >> 4);
+    const int l = lane & 15;
+    const int r = q0 + rho;
+    double2 v1 = make_double2(0.0, 0.0), psi = make_double2(0.0, 0.0);
+    if (r < qlim && l < ne) {
+      const int rr = ring_row(r, sg.shift);
+      const double* cf = CF + rr * kCoefCount;
+      const double2* row = U + rr * sg.rs;
+      const double2 Q = SC ? QE[rr * kStreamNep + l] : row[ne + l];
+      psi = row[2 * ne + l];
+      v1 = csub(cadd(row[l], cscale(2.0 * cf[1], Q)),
+                cmul(make_double2(cf[3], mm * cf[4]), psi));
+    }
+    xw[(rho * 4 + 0) * kStreamXs + l] = v1.x;
+    xw[(rho * 4 + 1) * kStreamXs + l] = v1.y;
+    xw[(rho * 4 + 2) * kStreamXs + l] = psi.x;
+    xw[(rho * 4 + 3) * kStreamXs + l] = psi.y;
+  }
+  named_sync(bar, 64);
+  // synthesis: acc[i][n][c] = C(node 16h + group + 8i, column n * 8 + 2 quad + c)
+  double acc[2][2][2];
+#pragma unroll
+  for (int n = 0; n < 2; ++n) {
+    double v[4];
+    const double* col = xw + (n * 8 + group) * kStreamXs;
+    v[0] = col[2 * quad];
+    v[1] = col[2 * quad + 1];
+    v[2] = col[2 * quad + 8];
+    v[3] = col[2 * quad + 9];
+    uint2 b[split::kSlices];
+    const int e = split_column(v, b);  // scale of column n * 8 + group
+    float d[split::kSlices][4];
+    split_products(d, F.s, b);
+    const double c0 = ldexp(1.0, __shfl_sync(0xffffffffu, e, 8 * quad));
+    const double c1 = ldexp(1.0, __shfl_sync(0xffffffffu, e, 8 * quad + 4));
+    acc[0][n][0] = split::recombine(d, 0) * F.node_scale[0] * c0;
+    acc[0][n][1] = split::recombine(d, 1) * F.node_scale[0] * c1;
+    acc[1][n][0] = split::recombine(d, 2) * F.node_scale[1] * c0;
+    acc[1][n][1] = split::recombine(d, 3) * F.node_scale[1] * c1;
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const int mt = 2 * h + i;
+    if (mt < mts) {
+      const int j = mt * 8 + group;
+      double inv[2];  // 1 / C_T(r, theta_j); zero beyond the solve's nodes
+#pragma unroll
+      for (int n = 0; n < 2; ++n) {
+        const int r = q0 + 2 * n + (quad >> 1);
+        inv[n] = r < qlim ? NI[ring_row(r, sg.shift) * kNodeRecord + j] : 0.0;
+      }
+#pragma unroll
+      for (int n = 0; n < 2; ++n) {
+        // lane quad 0/2 holds a_j of a row, quad 1/3 holds b_j of that row
+        const double o0 = __shfl_xor_sync(0xffffffffu, acc[i][n][0], 1);
+        const double o1 = __shfl_xor_sync(0xffffffffu, acc[i][n][1], 1);
+        if ((quad & 1) == 0) {
+          const int rho = 2 * n + (quad >> 1);
+          tw[(rho * 2 + 0) * kStreamTs + j] =
+              (acc[i][n][0] + F.gcos[i] * o1) * inv[n];
+          tw[(rho * 2 + 1) * kStreamTs + j] =
+              (acc[i][n][1] - F.gcos[i] * o0) * inv[n];
+        }
+      }
+    }
+  }
+  named_sync(bar, 64);
+  // analysis partial: C(ell group + 8i, column 2 quad + c) over this warp's
+  // nodes
+  double part[4];
+  {
+    double v[4];
+    const double* col = tw + group * kStreamTs + 16 * h;
+    v[0] = col[2 * quad];
+    v[1] = col[2 * quad + 1];
+    v[2] = col[2 * quad + 8];
+    v[3] = col[2 * quad + 9];
+    uint2 b[split::kSlices];
+    const int e = split_column(v, b);
+    float d[split::kSlices][4];
+    split_products(d, F.a, b);
+    const double c0 = ldexp(1.0, __shfl_sync(0xffffffffu, e, 8 * quad));
+    const double c1 = ldexp(1.0, __shfl_sync(0xffffffffu, e, 8 * quad + 4));
+    part[0] = split::recombine(d, 0) * F.ell_scale[0] * c0;
+    part[1] = split::recombine(d, 1) * F.ell_scale[0] * c1;
+    part[2] = split::recombine(d, 2) * F.ell_scale[1] * c0;
+    part[3] = split::recombine(d, 3) * F.ell_scale[1] * c1;
+  }
+  // warp 0 finishes ell = group, warp 1 ell = group + 8: each hands the
+  // other half to its partner
+  double* mine = ex + (h * 32 + lane) * 2;
+  double* theirs = ex + ((1 - h) * 32 + lane) * 2;
+  mine[0] = h == 0 ? part[2] : part[0];
+  mine[1] = h == 0 ? part[3] : part[1];
+  named_sync(bar, 64);
+  const double s0 = (h == 0 ? part[0] : part[2]) + theirs[0];
+  const double s1 = (h == 0 ? part[1] : part[3]) + theirs[1];
+  const int l = group + 8 * h;
+  const int r = q0 + quad;
+  if (r < qlim && l < ne) {
+    PS[ring_row(r, sg.shift) * kStreamNep + l] = make_double2(s0, s1);
+  }
+}
+
+template <int DISC, int SC, int PREC>
 __device__ void stream_transform(const StageLaunch& p,
                                  unsigned long long* full,
                                  unsigned long long* ready,
@@ -584,7 +756,7 @@ __device__ void stream_transform(const StageLaunch& p,
                                  const double2* X, double2* PS, double2* QE,
                                  const double* CF, const double* NI,
                                  double* xw_all, double* tw_all,
-                                 const int tt) {
+                                 double* ex_all, const int tt) {
   using T = DiscTraits<DISC>;
   constexpr int P = T::P, HD = T::HALF;
   constexpr int H = SC ? (P > 2 * HD ? P : 2 * HD) : P;
@@ -608,8 +780,29 @@ __device__ void stream_transform(const StageLaunch& p,
     const double inv_h = in.inv_spacing;
     const double mm = static_cast<double>(sg.m);
     PsiFragments F;
+    SplitFragments G;
     const int mts = (nt + 7) / 8, ksa = (nt + 3) / 4;
-    if (kerr) {
+    if (kerr && PREC == 1) {
+      // digit fragments of this segment: [h][slice][lane] uint4 for the
+      // synthesis, then the same for the analysis; 48 scales
+      const uint4* fr = p.split_frags + static_cast<long long>(sg.segment) * kSplitRecord;
+#pragma unroll
+      for (int sl = 0; sl < split::kSlices; ++sl) {
+        const uint4 fs = fr[(h * split::kSlices + sl) * 32 + lane];
+        const uint4 fa = fr[((2 + h) * split::kSlices + sl) * 32 + lane];
+        G.s[sl][0] = fs.x; G.s[sl][1] = fs.y; G.s[sl][2] = fs.z; G.s[sl][3] = fs.w;
+        G.a[sl][0] = fa.x; G.a[sl][1] = fa.y; G.a[sl][2] = fa.z; G.a[sl][3] = fa.w;
+      }
+      const double* sc = p.split_scales + static_cast<long long>(sg.segment) * kSplitScales;
+      const double sa2 = 2.0 * (static_cast<double>(kSpinWeight) * in.spin);
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int j = 16 * h + group + 8 * i;
+        G.node_scale[i] = sc[j];
+        G.ell_scale[i] = sc[kStreamMaxTheta + group + 8 * i];
+        G.gcos[i] = j < nt ? sa2 * p.trig[in.trig_offset + nt + j] : 0.0;
+      }
+    } else if (kerr) {
       const SegmentDesc& seg = p.segments[sg.segment];
       const double* St = p.matrices + seg.mat_offset;  // St[l][j]
       const double* At = St + ne * nt;                 // At[j][l]
@@ -679,7 +872,13 @@ __device__ void stream_transform(const StageLaunch& p,
         pe = min(sg.t1, a1);
       }
       if (pe > pd) {
-        if (kerr) {
+        if (kerr && PREC == 1) {
+          for (int q = pd; q < pe; q += 4 * kStreamBlocks) {
+            stream_psi_split<SC>(q + 4 * blk, pe, h, sg, U, QE, CF, NI, PS, xw,
+                                 tw, ex_all + blk * 128, G, mts,
+                                 kStreamBlockBar + blk, lane);
+          }
+        } else if (kerr) {
           for (int q = pd; q < pe; q += 4 * kStreamBlocks) {
             stream_psi_half<SC>(q + 4 * blk, pe, h, sg, U, QE, CF, NI, PS, xw,
                                 tw, F, mts, ksa, kStreamBlockBar + blk, lane);
@@ -1097,7 +1296,7 @@ __device__ void stream_producer(const StageLaunch& p, StreamLoaderState& L,
   if (*abort_flag != 0) loader_drain(L, full);
 }
 
-template <int DISC, int SC>
+template <int DISC, int SC, int PREC>
 __global__ void __launch_bounds__(kStreamThreads, 1)
     stream_stage_kernel(const StageLaunch p) {
   extern __shared__ __align__(128) unsigned char stream_smem[];
@@ -1119,6 +1318,7 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
   double* NI = reinterpret_cast<double*>(stream_smem + Ls.nodes);
   double* xw = reinterpret_cast<double*>(stream_smem + Ls.xw);
   double* tw = reinterpret_cast<double*>(stream_smem + Ls.tw);
+  double* ex = reinterpret_cast<double*>(stream_smem + Ls.ex);
   const int tid = threadIdx.x;
   if (tid == 0) {
     for (int s = 0; s < kStreamStages; ++s) {
@@ -1134,8 +1334,8 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
   constexpr int H = SC ? (T::P > 2 * T::HALF ? T::P : 2 * T::HALF) : T::P;
   if (tid < kStreamTThreads) {
     set_max_registers<kStreamTRegs>();
-    stream_transform<DISC, SC>(p, full, ready, abort_flag, U, X, PS, QE, CF,
-                               NI, xw, tw, tid);
+    stream_transform<DISC, SC, PREC>(p, full, ready, abort_flag, U, X, PS, QE,
+                                     CF, NI, xw, tw, ex, tid);
   } else if (tid < kStreamTThreads + kStreamSThreads) {
     set_max_registers<kStreamSRegs>();
     stream_stencil<DISC, SC>(p, ready, abort_flag, released, U, X, A, PS, QE,
