@@ -20,7 +20,16 @@ through the C ABI with host buffers (initial-state upload from pinned host
 memory and a per-step device->host read of every solve's endpoint waveform
 inside the timed region).  ``--impl reference`` times the reference's own
 CPU implementation (teuk-kokkos headers built against the Kokkos-API host
-shim, all host threads) on one solve of the same workload.
+shim, all host threads) on the same workload, one RK4 step of one of its
+solves per benchmark step, without mapping the engine library.
+
+Beside the headline the line carries (rank 0, one GPU): ``split_precision``
+(the same batch with split-precision transforms), ``uneven_batch`` (256
+solves of uneven shape in one set of launches against the same solves one
+at a time), ``serving`` (a Poisson stream of the serving mix through the
+continuous-batching server, p50 / p99 time-to-waveform), ``second_order``
+(the quadratic-source solve, FP64 and split precision) and the reference
+build's rate on the host cores (``cpu_baseline``).
 """
 from __future__ import annotations
 
@@ -601,6 +610,7 @@ def b200_arm(args):
     info = td.rank_info()
     world, rank, local = info.world_size, info.rank, info.local_rank
     torch.cuda.set_device(local)
+    tb.set_device(local)  # the engine's own CUDA runtime
     td.init("nccl", device=torch.device("cuda", local))
 
     meta, config, pulse, dt = workload_config(args.batch)

@@ -189,6 +189,15 @@ typedef struct teuk_b200_batch teuk_b200_batch;
 
 const char* teuk_b200_last_error(void);
 int teuk_b200_abi_version(void);
+/* The CUDA device that pipelines, batches and servers created afterwards on
+ * the calling thread use (cudaSetDevice inside the engine).  The engine links
+ * the CUDA runtime statically, so a device chosen through another copy of
+ * the runtime (a framework's, an application's) does not reach it; a
+ * process driving one GPU per rank or thread selects it here.  No
+ * counterpart in the reference (its execution space picks the device at
+ * Kokkos::initialize). */
+int teuk_b200_set_device(int device);
+int teuk_b200_get_device(int* device);
 
 /* ---- single pipeline (one solve) ------------------------------------- */
 int teuk_b200_create(const teuk_b200_config* config,

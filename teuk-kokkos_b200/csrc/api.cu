@@ -1877,6 +1877,22 @@ const char* teuk_b200_last_error(void) {
 
 int teuk_b200_abi_version(void) { return TEUK_B200_ABI_VERSION; }
 
+int teuk_b200_set_device(int device) {
+  return guarded([&] {
+    int count = 0;
+    teuk_b200::check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+    require(device >= 0 && device < count, "CUDA device index out of range");
+    teuk_b200::check(cudaSetDevice(device), "cudaSetDevice");
+  });
+}
+
+int teuk_b200_get_device(int* device) {
+  return guarded([&] {
+    require(device != nullptr, "null argument");
+    teuk_b200::check(cudaGetDevice(device), "cudaGetDevice");
+  });
+}
+
 namespace {
 teuk_b200_batch_options checked_options(const teuk_b200_batch_options* o) {
   teuk_b200_batch_options out{TEUK_B200_ABI_VERSION, TEUK_B200_KERNEL_AUTO,

@@ -393,6 +393,8 @@ def _load() -> ctypes.CDLL:
     sig = {
         "teuk_b200_last_error": ([], ctypes.c_char_p),
         "teuk_b200_abi_version": ([], I),
+        "teuk_b200_set_device": ([I], I),
+        "teuk_b200_get_device": ([ctypes.POINTER(I)], I),
         "teuk_b200_create": ([ctypes.POINTER(_Config), ctypes.POINTER(P)], I),
         "teuk_b200_create_with_options": ([ctypes.POINTER(_Config),
                                            ctypes.POINTER(_BatchOptions),
@@ -501,6 +503,19 @@ _lib = _Library()
 def library() -> ctypes.CDLL:
     """The mapped engine library (loads it on first use)."""
     return _lib.load()
+
+
+def set_device(device: int):
+    """Select the CUDA device of the engine for this thread
+    (teuk_b200_set_device): the engine's statically linked CUDA runtime does
+    not follow torch.cuda.set_device."""
+    _check(_lib.teuk_b200_set_device(int(device)))
+
+
+def get_device() -> int:
+    d = ctypes.c_int()
+    _check(_lib.teuk_b200_get_device(ctypes.byref(d)))
+    return d.value
 
 
 def test_withhold_chunk(chunk: int):
