@@ -426,6 +426,7 @@ struct AngularTileParams {
   const double* fp64;    // [n8][k4][lane] B fragments of T^T
   const uint2* split;    // [n8][k16][slice][lane] BF16 digit fragments
   const double* scales;  // 2^(F_j - 14) per output node
+  int frag_words;        // 8-byte words of one operator's fragments (even)
   int spin, boost;
 };
 
@@ -465,13 +466,34 @@ __device__ __forceinline__ void stage_tile_rows(const double2* src,
   }
 }
 
+// Asynchronous 16-byte global -> shared copies (no register round trip), so
+// every copy of the operator's fragments is in flight at once.
+__device__ __forceinline__ void copy_async_16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
+                   static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void copy_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// Dynamic shared memory of the tile operator: the four staged planes and the
+// operator's fragments (`frag_words` 8-byte words).
+__host__ __device__ constexpr size_t tile_smem_bytes(const int frag_words) {
+  return sizeof(double) * (4 * kTileCtaRows * kTileStride +
+                           static_cast<size_t>(frag_words));
+}
+
 template <int PREC>
 __global__ void __launch_bounds__(kTileWarps * 32)
     angular_tile_kernel(const Geo g, const Trig tr, const AngularTileParams p) {
-  __shared__ double xr[kTileCtaRows][kTileStride];
-  __shared__ double xi[kTileCtaRows][kTileStride];
-  __shared__ double dr[kTileCtaRows][kTileStride];  // d_T x (eth / eth')
-  __shared__ double di[kTileCtaRows][kTileStride];
+  extern __shared__ __align__(16) double tile_smem[];
+  double (*xr)[kTileStride] = reinterpret_cast<double (*)[kTileStride]>(tile_smem);
+  double (*xi)[kTileStride] = xr + kTileCtaRows;
+  double (*dr)[kTileStride] = xi + kTileCtaRows;  // d_T x (eth / eth')
+  double (*di)[kTileStride] = dr + kTileCtaRows;
+  double* sfrag = tile_smem + 4 * kTileCtaRows * kTileStride;
   const int nt = g.nt;
   const int tiles = (g.nr + kTileCtaRows - 1) / kTileCtaRows;
   const int mode = blockIdx.x / tiles;
@@ -488,8 +510,17 @@ __global__ void __launch_bounds__(kTileWarps * 32)
   // K padded to the MMA's k granularity; padding columns and rows past the
   // grid are zero
   const int kpad = PREC == kPrecisionSplit ? (nt + 15) / 16 * 16 : (nt + 3) / 4 * 4;
+  {  // the mode's operator fragments, copied asynchronously while the rows load
+    const double* src = PREC == kPrecisionSplit
+                            ? reinterpret_cast<const double*>(p.split + p.offsets[3 * mode + 1])
+                            : p.fp64 + p.offsets[3 * mode];
+    for (int i = 2 * threadIdx.x; i < p.frag_words; i += 2 * blockDim.x) {
+      copy_async_16(sfrag + i, src + i);
+    }
+  }
   stage_tile_rows(p.in.at(g, mode, p.in_slot, r0, 0), rows, nt, kpad, xr, xi);
   if (ghp) stage_tile_rows(p.dt.at(g, mode, p.dt_slot, r0, 0), rows, nt, kpad, dr, di);
+  copy_async_wait_all();
   // every read of the input rows happens before any store below (the
   // operation may run in place)
   __syncthreads();
@@ -516,7 +547,7 @@ __global__ void __launch_bounds__(kTileWarps * 32)
   constexpr int kHalfN8 = kTileMaxNodes / 16;  // n tiles of one warp
   if constexpr (PREC == kPrecisionFp64) {
     const int k4 = kpad / 4;
-    const double* frag = p.fp64 + p.offsets[3 * mode];
+    const double* frag = sfrag;
     double acc[kHalfN8][4];
 #pragma unroll
     for (int h = 0; h < kHalfN8; ++h) {
@@ -533,7 +564,7 @@ __global__ void __launch_bounds__(kTileWarps * 32)
         for (int h = 0; h < kHalfN8; ++h) {
           const int n = 2 * h + half;
           if (n < n8) {
-            const double b = __ldg(frag + (n * k4 + ks) * 32 + lane);
+            const double b = frag[(n * k4 + ks) * 32 + lane];
             dmma_tile(acc[h][0], acc[h][1], ar, b);
             dmma_tile(acc[h][2], acc[h][3], ai, b);
           }
@@ -594,7 +625,7 @@ __global__ void __launch_bounds__(kTileWarps * 32)
         }
       }
     }
-    const uint2* frag = p.split + p.offsets[3 * mode + 1];
+    const uint2* frag = reinterpret_cast<const uint2*>(sfrag);
     const double* colscale = p.scales + p.offsets[3 * mode + 2];
     const double up_r = ldexp(1.0, er), up_i = ldexp(1.0, ei);
     for (int n = half; n < n8; n += 2) {
@@ -609,7 +640,7 @@ __global__ void __launch_bounds__(kTileWarps * 32)
           uint2 b[kSplitSlices];
 #pragma unroll
           for (int t = 0; t < kSplitSlices; ++t) {
-            b[t] = __ldg(frag + ((n * k16 + ks) * kSplitSlices + t) * 32 + lane);
+            b[t] = frag[((n * k16 + ks) * kSplitSlices + t) * 32 + lane];
           }
 #pragma unroll
           for (int s = 0; s < kSplitSlices; ++s) {
@@ -1428,7 +1459,23 @@ NodalPipeline::NodalPipeline(const InstancePlan& plan, const int precision)
     throw std::invalid_argument(
         "split-precision transforms support at most 64 theta nodes");
   }
-  if (tile_operators_) build_tile_operators();
+  if (tile_operators_) {
+    build_tile_operators();
+    const int n8 = (c.ntheta + 7) / 8;
+    tile_fp64_words_ = n8 * ((c.ntheta + 3) / 4) * 32;
+    tile_split_words_ = n8 * ((c.ntheta + 15) / 16) * kSplitSlices * 32;
+    // the dynamic shared-memory opt-in is an attribute of the function on
+    // the current device: set on every construction (cheap), so pipelines
+    // on any device of the process may launch
+    const int most = static_cast<int>(tile_smem_bytes(
+        (kTileMaxNodes / 8) * (kTileMaxNodes / 16) * kSplitSlices * 32));
+    check(cudaFuncSetAttribute(angular_tile_kernel<kPrecisionFp64>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, most),
+          "tile operator shared memory");
+    check(cudaFuncSetAttribute(angular_tile_kernel<kPrecisionSplit>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, most),
+          "tile operator shared memory");
+  }
 
   // integer tables: mvals, sharp, pairs, coordinator tables
   std::vector<int> ints;
@@ -1833,10 +1880,12 @@ void NodalPipeline::evaluate(const double2* stage_in, double2* out) {
       tp.spin = p.spin;
       tp.boost = p.boost;
       const int tiles = g.modes * ((g.nr + kTileCtaRows - 1) / kTileCtaRows);
+      tp.frag_words = precision_ == kPrecisionSplit ? tile_split_words_ : tile_fp64_words_;
+      const size_t bytes = tile_smem_bytes(tp.frag_words);
       if (precision_ == kPrecisionSplit) {
-        angular_tile_kernel<kPrecisionSplit><<<tiles, kTileWarps * 32, 0, s>>>(g, tr, tp);
+        angular_tile_kernel<kPrecisionSplit><<<tiles, kTileWarps * 32, bytes, s>>>(g, tr, tp);
       } else {
-        angular_tile_kernel<kPrecisionFp64><<<tiles, kTileWarps * 32, 0, s>>>(g, tr, tp);
+        angular_tile_kernel<kPrecisionFp64><<<tiles, kTileWarps * 32, bytes, s>>>(g, tr, tp);
       }
       return;
     }

@@ -136,6 +136,8 @@ class NodalPipeline {
   int precision_ = 0;
   // composite tile operators: used when ntheta <= 64
   bool tile_operators_ = false;
+  int tile_fp64_words_ = 0;   // 8-byte words of one FP64 operator
+  int tile_split_words_ = 0;  // 8-byte words of one split operator
   std::vector<double> tile_fp64_;
   std::vector<uint2> tile_split_;
   std::vector<double> tile_scales_;
