@@ -485,9 +485,24 @@ __host__ __device__ constexpr size_t tile_smem_bytes(const int frag_words) {
                            static_cast<size_t>(frag_words));
 }
 
+// Independent operations launched together: CTAs [first_block[i],
+// first_block[i + 1]) run operation i.
+constexpr int kTileMaxOps = 6;
+struct AngularTileBatch {
+  int count;
+  int first_block[kTileMaxOps + 1];
+  AngularTileParams ops[kTileMaxOps];
+};
+
 template <int PREC>
 __global__ void __launch_bounds__(kTileWarps * 32)
-    angular_tile_kernel(const Geo g, const Trig tr, const AngularTileParams p) {
+    angular_tile_kernel(const Geo g, const Trig tr, const AngularTileBatch batch) {
+  int which = 0;
+  while (which + 1 < batch.count && static_cast<int>(blockIdx.x) >= batch.first_block[which + 1]) {
+    ++which;
+  }
+  const AngularTileParams& p = batch.ops[which];
+  const int block = static_cast<int>(blockIdx.x) - batch.first_block[which];
   extern __shared__ __align__(16) double tile_smem[];
   double (*xr)[kTileStride] = reinterpret_cast<double (*)[kTileStride]>(tile_smem);
   double (*xi)[kTileStride] = xr + kTileCtaRows;
@@ -496,8 +511,8 @@ __global__ void __launch_bounds__(kTileWarps * 32)
   double* sfrag = tile_smem + 4 * kTileCtaRows * kTileStride;
   const int nt = g.nt;
   const int tiles = (g.nr + kTileCtaRows - 1) / kTileCtaRows;
-  const int mode = blockIdx.x / tiles;
-  const int r0 = (blockIdx.x - mode * tiles) * kTileCtaRows;
+  const int mode = block / tiles;
+  const int r0 = (block - mode * tiles) * kTileCtaRows;
   const int rows = min(kTileCtaRows, g.nr - r0);
   double2* out = p.out.at(g, mode, p.out_slot, r0, 0);
   if (!p.active[mode]) {
@@ -1828,6 +1843,82 @@ void NodalPipeline::evaluate(const double2* stage_in, double2* out) {
   const Arr stage{const_cast<double2*>(stage_in), kFieldCount};
   const Arr output{out, kFieldCount};
 
+  // Angular operations on the tile operator are queued and launched
+  // together while they are independent: a queued operation that writes a
+  // plane another queued one reads or writes (or reads a plane one writes)
+  // flushes the queue first, and so does every other kernel below.
+  struct TileQueue {
+    NodalPipeline& self;
+    Buffers& b;
+    const Geo& g;
+    const Trig& tr;
+    cudaStream_t s;
+    struct Plane {
+      const double2* p;
+      int slots, slot;
+      bool operator==(const Plane& o) const {
+        return p == o.p && slots == o.slots && slot == o.slot;
+      }
+    };
+    AngularTileBatch batch{};
+    std::vector<Plane> reads, writes;
+    void flush() {
+      if (batch.count == 0) return;
+      const int tiles = g.modes * ((g.nr + kTileCtaRows - 1) / kTileCtaRows);
+      for (int i = 0; i <= batch.count; ++i) batch.first_block[i] = i * tiles;
+      const int words = self.precision_ == kPrecisionSplit ? self.tile_split_words_
+                                                           : self.tile_fp64_words_;
+      const size_t bytes = tile_smem_bytes(words);
+      const unsigned grid = static_cast<unsigned>(batch.count * tiles);
+      if (self.precision_ == kPrecisionSplit) {
+        angular_tile_kernel<kPrecisionSplit><<<grid, kTileWarps * 32, bytes, s>>>(g, tr, batch);
+      } else {
+        angular_tile_kernel<kPrecisionFp64><<<grid, kTileWarps * 32, bytes, s>>>(g, tr, batch);
+      }
+      batch.count = 0;
+      reads.clear();
+      writes.clear();
+    }
+    static bool contains(const std::vector<Plane>& v, const Plane& x) {
+      return std::find(v.begin(), v.end(), x) != v.end();
+    }
+    void add(const int coord, const int kind, const Arr in, const int in_slot,
+             const Arr dt, const int dt_slot, const Arr o, const int out_slot,
+             const int spin, const int boost) {
+      const bool ghp = kind == kEth || kind == kEthPrime;
+      const Plane r1{in.p, in.slots, in_slot}, r2{dt.p, dt.slots, dt_slot},
+          w{o.p, o.slots, out_slot};
+      if (batch.count == kTileMaxOps || contains(writes, r1) ||
+          (ghp && contains(writes, r2)) || contains(writes, w) ||
+          contains(reads, w)) {
+        flush();
+      }
+      const auto& d = b.coords[coord];
+      AngularTileParams& tp = batch.ops[batch.count++];
+      tp = AngularTileParams{};
+      tp.kind = kind;
+      tp.in = in;
+      tp.in_slot = in_slot;
+      tp.dt = dt;
+      tp.dt_slot = dt_slot;
+      tp.out = o;
+      tp.out_slot = out_slot;
+      tp.active = d.active;
+      tp.offsets = b.tile_offsets[coord][kind];
+      tp.fp64 = b.tile_fp64;
+      tp.split = b.tile_split;
+      tp.scales = b.tile_scales;
+      tp.frag_words = self.precision_ == kPrecisionSplit ? self.tile_split_words_
+                                                         : self.tile_fp64_words_;
+      tp.spin = spin;
+      tp.boost = boost;
+      reads.push_back(r1);
+      if (ghp) reads.push_back(r2);
+      writes.push_back(w);
+    }
+  } tile_queue{*this, b, g, tr, s};
+  const auto flush = [&] { tile_queue.flush(); };
+
   const auto op = [&](const int coord, const int kind, const Arr in,
                       const int in_slot, const Arr dt, const int dt_slot,
                       const Arr o, const int out_slot) {
@@ -1864,29 +1955,8 @@ void NodalPipeline::evaluate(const double2* stage_in, double2* out) {
       p.diag_off = d.lower_diag;
     }
     if (tile_operators_) {
-      AngularTileParams tp{};
-      tp.kind = kind;
-      tp.in = in;
-      tp.in_slot = in_slot;
-      tp.dt = dt;
-      tp.dt_slot = dt_slot;
-      tp.out = o;
-      tp.out_slot = out_slot;
-      tp.active = d.active;
-      tp.offsets = b.tile_offsets[coord][kind];
-      tp.fp64 = b.tile_fp64;
-      tp.split = b.tile_split;
-      tp.scales = b.tile_scales;
-      tp.spin = p.spin;
-      tp.boost = p.boost;
-      const int tiles = g.modes * ((g.nr + kTileCtaRows - 1) / kTileCtaRows);
-      tp.frag_words = precision_ == kPrecisionSplit ? tile_split_words_ : tile_fp64_words_;
-      const size_t bytes = tile_smem_bytes(tp.frag_words);
-      if (precision_ == kPrecisionSplit) {
-        angular_tile_kernel<kPrecisionSplit><<<tiles, kTileWarps * 32, bytes, s>>>(g, tr, tp);
-      } else {
-        angular_tile_kernel<kPrecisionFp64><<<tiles, kTileWarps * 32, bytes, s>>>(g, tr, tp);
-      }
+      tile_queue.add(coord, kind, in, in_slot, dt, dt_slot, o, out_slot,
+                     p.spin, p.boost);
       return;
     }
     angular_op_kernel<<<ga, kBlock, 0, s>>>(g, tr, p);
@@ -1894,6 +1964,7 @@ void NodalPipeline::evaluate(const double2* stage_in, double2* out) {
   const auto teuk = [&](const Arr st_, const int f0, const Arr scratch,
                         const Arr lap, const int lap_slot,
                         const double2* forcing, const Arr o) {
+    flush();
     TeukParams p{st_, f0, scratch, lap, lap_slot, forcing, o};
     teuk_prepare_kernel<<<gp, kBlock, 0, s>>>(g, p);
     teuk_primitives_kernel<<<gp, kBlock, 0, s>>>(g, tr, p);
@@ -1908,13 +1979,16 @@ void NodalPipeline::evaluate(const double2* stage_in, double2* out) {
   const auto chain = [&](const Arr st_, const Arr o, double2* rr_p,
                          double2* ang_p) {
     const Arr rr{rr_p, 7}, ang{ang_p, 6};
+    flush();
     recon_radial_kernel<<<grid_for(points * 7), kBlock, 0, s>>>(g, st_, rr);
     op(cFirst, kEth, st_, kFirstPsi, o, kFirstPsi, ang, aEth1F);
     ReconParams rp{st_, o, rr, ang};
+    flush();
     recon_pass_kernel<1><<<gp, kBlock, 0, s>>>(g, tr, rp);
     op(cG, kProject, o, kG, o, 0, o, kG);
     op(cFirst, kProject, o, kLambda, o, 0, o, kLambda);
     op(cG, kEth, st_, kG, o, kG, ang, aEth2G);
+    flush();
     recon_pass_kernel<2><<<gp, kBlock, 0, s>>>(g, tr, rp);
     op(cScalar, kProject, o, kH, o, 0, o, kH);
     op(cB, kProject, o, kB, o, 0, o, kB);
@@ -1922,9 +1996,11 @@ void NodalPipeline::evaluate(const double2* stage_in, double2* out) {
     op(cC, kProject, o, kC, o, 0, o, kC);
     op(cC, kEth, st_, kC, o, kC, ang, aEth2C);
     op(cPi, kEth, st_, kPi, o, kPi, ang, aEth2Pi);
+    flush();
     pack_sharp_kernel<<<gp, kBlock, 0, s>>>(g, tr, st_, o, sharp);
     op(cBSharp, kEthPrime, sharp, shB, sharp, shBDt, ang, aEthP1BSharp);
     op(cCSharp, kEthPrime, sharp, shC, sharp, shCDt, ang, aEthP2CSharp);
+    flush();
     recon_pass_kernel<3><<<gp, kBlock, 0, s>>>(g, tr, rp);
     op(cScalar, kProject, o, kU, o, 0, o, kU);
   };
@@ -1940,6 +2016,7 @@ void NodalPipeline::evaluate(const double2* stage_in, double2* out) {
   op(cScalar, kEthPrime, stage, kH, output, kH, ind, 1);
   ConstraintParams cp{stage, output, first_scr, Arr{b.rr, 7}, ind,
                       Arr{b.constraints, 3}, Arr{b.terms, 6}};
+  flush();
   constraints_kernel<<<gp, kBlock, 0, s>>>(g, tr, cp);
   // stage tangent (:526-546)
   op(cFirst, kLaplacian, output, kFirstPsi, output, 0, lin, 1);
@@ -1958,6 +2035,7 @@ void NodalPipeline::evaluate(const double2* stage_in, double2* out) {
                        Arr{b.rr_t, 7}, Arr{b.rec_ang, 6}, Arr{b.rec_ang_t, 6},
                        extra,          Arr{b.src_f, 8}, Arr{b.src_ft, 8},
                        Arr{b.src_d, 11}, Arr{b.src_dt, 11}};
+  flush();
   source_inputs_kernel<<<gp, kBlock, 0, s>>>(g, tr, sp);
   check(cudaMemsetAsync(b.sum, 0, sizeof(double2) * g.modes * 2 * b.plane, s),
         "zero inner source");
@@ -1977,6 +2055,7 @@ void NodalPipeline::evaluate(const double2* stage_in, double2* out) {
   op(cT, kProject, sum, 1, sum, 0, proj, 1);
   op(cT, kProject, sum_t, 1, sum_t, 0, proj_t, 1);
   op(cT, kEthPrime, proj, 1, proj_t, 1, Arr{b.ethp_t, 1}, 0);
+  flush();
   outer_source_kernel<<<gp, kBlock, 0, s>>>(g, tr, proj, proj_t, b.ethp_t,
                                             b.source, b.forcing);
   if (!activation_.active) {
@@ -1987,6 +2066,7 @@ void NodalPipeline::evaluate(const double2* stage_in, double2* out) {
   op(cSecond, kLaplacian, stage, kSecondPsi, stage, 0, lin, 2);
   teuk(stage, kSecondP, second_scr, lin, 2, b.forcing, output);
   project3(cSecond, output, kSecondP);
+  flush();
   sync_check("second-order RHS");
 }
 
