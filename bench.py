@@ -230,9 +230,9 @@ def measured_hbm_peak():
 def recorded_traffic(kernel: str, algorithmic_bytes_per_launch: float):
     """DRAM bytes per stage launch from the committed ncu summary of
     `kernel` (key=value lines: dram_bytes_per_launch,
-    algorithmic_bytes_per_launch of the captured case), scaled to this
-    launch by the units processed."""
-    path = REPO / "profiles" / f"{kernel}_kerr_ringdown16_traffic.txt"
+    algorithmic_bytes_per_launch of the captured case, the benchmark's own
+    64-solve size), scaled to this launch by the units processed."""
+    path = REPO / "profiles" / f"{kernel}_kerr_ringdown64_traffic.txt"
     try:
         data = {}
         for line in path.read_text().splitlines():
