@@ -148,3 +148,34 @@ def test_server_rejects_what_it_cannot_run(require_gpu):
         big.submit(config, pulse_for(config, 1), 0.0, 2)
     with pytest.raises(tb.InvalidArgument, match="unknown request id"):
         big.result(12345)
+
+
+def test_split_precision_server_matches_split_alone(require_gpu):
+    """A split-precision server: every request's records equal the same
+    solve run alone with split-precision transforms (second-order requests
+    bit for bit, linear ones to 1e-12 as above)."""
+    split = tb.LaunchOptions(precision=tb.PRECISION_SPLIT)
+    server = tb.Server(hbm_budget_bytes=8 << 30, precision=tb.PRECISION_SPLIT)
+    jobs = []
+    for i, (name, seed, steps) in enumerate([("kerr_d105", 21, 6),
+                                             ("so_unrestricted_d84", 22, 4),
+                                             ("nonparent", 23, 5)]):
+        config = _config(name)
+        pulse = pulse_for(config, seed)
+        dt = step_size(config)
+        jobs.append((server.submit(config, pulse, dt, steps), config, pulse,
+                     dt, steps))
+        server.advance(2)
+    while server.advance(3) > 0:
+        pass
+    for rid, config, pulse, dt, steps in jobs:
+        records, _ = server.result(rid)
+        p = tb.Pipeline(config, split)
+        p.initialize_gaussian(pulse)
+        p.step(0.0, dt, steps)
+        alone = p.sample_endpoint()
+        if config.source_mode != tb.SOURCE_DISABLED:
+            assert _keys(records) == _keys(alone)
+            assert np.array_equal(_values(records), _values(alone))
+        else:
+            _check_same(records, alone)
