@@ -421,12 +421,12 @@ struct AngularTileParams {
   int out_slot;
   const int* active;
   // per mode: FP64 fragment offset (doubles), split fragment offset (uint2),
-  // split column-scale offset (doubles); 3 ints per mode
+  // split column-scale offset (doubles), n_ell of the source band; 4 ints
+  // per mode
   const int* offsets;
   const double* fp64;    // [n8][k4][lane] B fragments of T^T
   const uint2* split;    // [n8][k16][slice][lane] BF16 digit fragments
   const double* scales;  // 2^(F_j - 14) per output node
-  int frag_words;        // 8-byte words of one operator's fragments (even)
   int spin, boost;
 };
 
@@ -478,6 +478,19 @@ __device__ __forceinline__ void copy_async_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
+// 8-byte words of one operator's fragments.  FP64 projections run as two
+// GEMMs, analysis (B = A^T, n_ell columns) then synthesis (B = S^T, K =
+// n_ell), so that their output is the synthesis of band coefficients, band
+// limited to rounding of its own size as the reference's is; the other FP64
+// operations and every split-precision one use the composite nodal matrix.
+__host__ __device__ constexpr int tile_operator_words(const int prec, const int kind,
+                                                      const int nt, const int ne) {
+  const int n8 = (nt + 7) / 8, k4 = (nt + 3) / 4;
+  if (prec == kPrecisionSplit) return n8 * ((nt + 15) / 16) * kSplitSlices * 32;
+  if (kind == kProject) return ((ne + 7) / 8) * k4 * 32 + n8 * ((ne + 3) / 4) * 32;
+  return n8 * k4 * 32;
+}
+
 // Dynamic shared memory of the tile operator: the four staged planes and the
 // operator's fragments (`frag_words` 8-byte words).
 __host__ __device__ constexpr size_t tile_smem_bytes(const int frag_words) {
@@ -527,9 +540,10 @@ __global__ void __launch_bounds__(kTileWarps * 32)
   const int kpad = PREC == kPrecisionSplit ? (nt + 15) / 16 * 16 : (nt + 3) / 4 * 4;
   {  // the mode's operator fragments, copied asynchronously while the rows load
     const double* src = PREC == kPrecisionSplit
-                            ? reinterpret_cast<const double*>(p.split + p.offsets[3 * mode + 1])
-                            : p.fp64 + p.offsets[3 * mode];
-    for (int i = 2 * threadIdx.x; i < p.frag_words; i += 2 * blockDim.x) {
+                            ? reinterpret_cast<const double*>(p.split + p.offsets[4 * mode + 1])
+                            : p.fp64 + p.offsets[4 * mode];
+    const int words = tile_operator_words(PREC, p.kind, nt, p.offsets[4 * mode + 3]);
+    for (int i = 2 * threadIdx.x; i < words; i += 2 * blockDim.x) {
       copy_async_16(sfrag + i, src + i);
     }
   }
@@ -560,7 +574,76 @@ __global__ void __launch_bounds__(kTileWarps * 32)
     out[row * nt + j] = st(v);
   };
   constexpr int kHalfN8 = kTileMaxNodes / 16;  // n tiles of one warp
-  if constexpr (PREC == kPrecisionFp64) {
+  if (PREC == kPrecisionFp64 && p.kind == kProject) {
+    // analysis: band coefficients c(row, l), l < n_ell, over K = nodes
+    const int ne = p.offsets[4 * mode + 3];
+    const int k4 = kpad / 4, n1 = (ne + 7) / 8, kl4 = (ne + 3) / 4;
+    const double* f1 = sfrag;
+    const double* f2 = sfrag + n1 * k4 * 32;
+    double acc[kHalfN8][4];
+#pragma unroll
+    for (int h = 0; h < kHalfN8; ++h) {
+      acc[h][0] = acc[h][1] = acc[h][2] = acc[h][3] = 0.0;
+    }
+#pragma unroll
+    for (int ks = 0; ks < kTileMaxNodes / 4; ++ks) {
+      if (ks < k4) {
+        const double ar = xr[row][ks * 4 + q];
+        const double ai = xi[row][ks * 4 + q];
+#pragma unroll
+        for (int h = 0; h < kHalfN8; ++h) {
+          const int n = 2 * h + half;
+          if (n < n1) {
+            const double b = f1[(n * k4 + ks) * 32 + lane];
+            dmma_tile(acc[h][0], acc[h][1], ar, b);
+            dmma_tile(acc[h][2], acc[h][3], ai, b);
+          }
+        }
+      }
+    }
+    // the coefficients go through the (unused) d_T planes: zero beyond
+    // n_ell (their fragments are zero), K-padded for the synthesis
+#pragma unroll
+    for (int h = 0; h < kHalfN8; ++h) {
+      const int n = 2 * h + half;
+      if (n < n1) {
+        dr[row][n * 8 + 2 * q] = acc[h][0];
+        dr[row][n * 8 + 2 * q + 1] = acc[h][1];
+        di[row][n * 8 + 2 * q] = acc[h][2];
+        di[row][n * 8 + 2 * q + 1] = acc[h][3];
+      }
+    }
+    __syncthreads();
+    // synthesis over K = n_ell
+#pragma unroll
+    for (int h = 0; h < kHalfN8; ++h) {
+      acc[h][0] = acc[h][1] = acc[h][2] = acc[h][3] = 0.0;
+    }
+#pragma unroll
+    for (int ks = 0; ks < kTileMaxNodes / 4; ++ks) {
+      if (ks < kl4) {
+        const double ar = dr[row][ks * 4 + q];
+        const double ai = di[row][ks * 4 + q];
+#pragma unroll
+        for (int h = 0; h < kHalfN8; ++h) {
+          const int n = 2 * h + half;
+          if (n < n8) {
+            const double b = f2[(n * kl4 + ks) * 32 + lane];
+            dmma_tile(acc[h][0], acc[h][1], ar, b);
+            dmma_tile(acc[h][2], acc[h][3], ai, b);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < kHalfN8; ++h) {
+      const int n = 2 * h + half;
+      if (n < n8) {
+        finish(n * 8 + 2 * q, acc[h][0], acc[h][2]);
+        finish(n * 8 + 2 * q + 1, acc[h][1], acc[h][3]);
+      }
+    }
+  } else if constexpr (PREC == kPrecisionFp64) {
     const int k4 = kpad / 4;
     const double* frag = sfrag;
     double acc[kHalfN8][4];
@@ -641,7 +724,7 @@ __global__ void __launch_bounds__(kTileWarps * 32)
       }
     }
     const uint2* frag = reinterpret_cast<const uint2*>(sfrag);
-    const double* colscale = p.scales + p.offsets[3 * mode + 2];
+    const double* colscale = p.scales + p.offsets[4 * mode + 2];
     const double up_r = ldexp(1.0, er), up_i = ldexp(1.0, ei);
     for (int n = half; n < n8; n += 2) {
       float d[kSplitSlices][4];  // accumulator of digit pairs with s + t = u
@@ -1476,14 +1559,16 @@ NodalPipeline::NodalPipeline(const InstancePlan& plan, const int precision)
   }
   if (tile_operators_) {
     build_tile_operators();
-    const int n8 = (c.ntheta + 7) / 8;
-    tile_fp64_words_ = n8 * ((c.ntheta + 3) / 4) * 32;
-    tile_split_words_ = n8 * ((c.ntheta + 15) / 16) * kSplitSlices * 32;
+    // the largest operator: a projection with n_ell = ntheta (FP64), any
+    // operation (split)
+    tile_fp64_words_ = tile_operator_words(kPrecisionFp64, kProject, c.ntheta, c.ntheta);
+    tile_split_words_ = tile_operator_words(kPrecisionSplit, kProject, c.ntheta, c.ntheta);
     // the dynamic shared-memory opt-in is an attribute of the function on
     // the current device: set on every construction (cheap), so pipelines
     // on any device of the process may launch
-    const int most = static_cast<int>(tile_smem_bytes(
-        (kTileMaxNodes / 8) * (kTileMaxNodes / 16) * kSplitSlices * 32));
+    const int most = static_cast<int>(tile_smem_bytes(std::max(
+        tile_operator_words(kPrecisionFp64, kProject, kTileMaxNodes, kTileMaxNodes),
+        tile_operator_words(kPrecisionSplit, kProject, kTileMaxNodes, kTileMaxNodes))));
     check(cudaFuncSetAttribute(angular_tile_kernel<kPrecisionFp64>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, most),
           "tile operator shared memory");
@@ -1744,7 +1829,7 @@ void NodalPipeline::build_tile_operators() {
     const AngularCoordinator& a = coordinators_[k];
     for (int kind = 0; kind < 4; ++kind) {
       std::vector<int>& offs = tile_offsets_[k][kind];
-      offs.assign(3 * nm, 0);
+      offs.assign(4 * nm, 0);
       for (size_t i = 0; i < nm; ++i) {
         if (!a.active[i]) continue;
         const int ne = a.n_ell[i], lmin = a.ell_min[i];
@@ -1781,11 +1866,38 @@ void NodalPipeline::build_tile_operators() {
         const auto at = [&](const int j, const int kk) {
           return (j < nt && kk < nt) ? T[static_cast<size_t>(j) * nt + kk] : 0.0;
         };
-        offs[3 * i] = static_cast<int>(tile_fp64_.size());
-        for (int n = 0; n < n8; ++n) {
-          for (int ks = 0; ks < k4; ++ks) {
-            for (int lane = 0; lane < 32; ++lane) {
-              tile_fp64_.push_back(at(n * 8 + lane / 4, ks * 4 + lane % 4));
+        offs[4 * i] = static_cast<int>(tile_fp64_.size());
+        offs[4 * i + 3] = ne;
+        if (kind == kProject) {
+          // two GEMMs: B fragments of A^T (K = nodes, N = ell), then of S^T
+          // (K = ell, N = nodes)
+          const int n1 = (ne + 7) / 8, kl4 = (ne + 3) / 4;
+          const auto Av = [&](const int l, const int kk) {
+            return (l < ne && kk < nt) ? A[kk * ne + l] : 0.0;
+          };
+          const auto Sv = [&](const int j, const int l) {
+            return (j < nt && l < ne) ? S[l * nt + j] : 0.0;
+          };
+          for (int n = 0; n < n1; ++n) {
+            for (int ks = 0; ks < k4; ++ks) {
+              for (int lane = 0; lane < 32; ++lane) {
+                tile_fp64_.push_back(Av(n * 8 + lane / 4, ks * 4 + lane % 4));
+              }
+            }
+          }
+          for (int n = 0; n < n8; ++n) {
+            for (int ks = 0; ks < kl4; ++ks) {
+              for (int lane = 0; lane < 32; ++lane) {
+                tile_fp64_.push_back(Sv(n * 8 + lane / 4, ks * 4 + lane % 4));
+              }
+            }
+          }
+        } else {
+          for (int n = 0; n < n8; ++n) {
+            for (int ks = 0; ks < k4; ++ks) {
+              for (int lane = 0; lane < 32; ++lane) {
+                tile_fp64_.push_back(at(n * 8 + lane / 4, ks * 4 + lane % 4));
+              }
             }
           }
         }
@@ -1794,7 +1906,7 @@ void NodalPipeline::build_tile_operators() {
         const auto digit = [&](const int j, const int kk, const int t) -> float& {
           return digits[((static_cast<size_t>(j) * k16 * 16) + kk) * kSplitSlices + t];
         };
-        offs[3 * i + 2] = static_cast<int>(tile_scales_.size());
+        offs[4 * i + 2] = static_cast<int>(tile_scales_.size());
         for (int j = 0; j < n8 * 8; ++j) {
           double m = 0.0;
           for (int kk = 0; kk < nt; ++kk) m = std::max(m, std::fabs(at(j, kk)));
@@ -1806,7 +1918,7 @@ void NodalPipeline::build_tile_operators() {
             for (int s = 0; s < kSplitSlices; ++s) digit(j, kk, s) = t[s];
           }
         }
-        offs[3 * i + 1] = static_cast<int>(tile_split_.size());
+        offs[4 * i + 1] = static_cast<int>(tile_split_.size());
         for (int n = 0; n < n8; ++n) {
           for (int ks = 0; ks < k16; ++ks) {
             for (int t = 0; t < kSplitSlices; ++t) {
@@ -1908,8 +2020,6 @@ void NodalPipeline::evaluate(const double2* stage_in, double2* out) {
       tp.fp64 = b.tile_fp64;
       tp.split = b.tile_split;
       tp.scales = b.tile_scales;
-      tp.frag_words = self.precision_ == kPrecisionSplit ? self.tile_split_words_
-                                                         : self.tile_fp64_words_;
       tp.spin = spin;
       tp.boost = boost;
       reads.push_back(r1);
