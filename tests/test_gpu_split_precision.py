@@ -151,3 +151,26 @@ def test_split_batch_member_equals_solo(require_gpu):
         solo.initialize_gaussian(pulses[i])
         solo.step(0.0, dts[i], 5)
         assert np.array_equal(batch.get_state(i), solo.get_state()), i
+
+
+def test_split_second_order_checkpoint_loads_into_the_reference(require_gpu, tmp_path):
+    """Projections run the FP64 two-GEMM path in every precision, so a
+    split-precision pipeline's state stays band limited to the reference's
+    checkpoint tolerance (5e-11 per radial line) and the reference loads it."""
+    config = tb.SolveConfig(
+        mass=1.0, spin=0.7, compactification_length=1.2, radial_points=48,
+        theta_nodes=9, ell_max_first=4, ell_max_second=8,
+        modes=(-4, -2, 0, 2, 4), parents=(-2, 2), targets=(-4, 0, 4),
+        dissipation=0.0, discretization=tb.D84,
+        source_mode=tb.SOURCE_CONSTRAINT_AWARE,
+        normalized_constraint_tolerance=1e30, required_consecutive_passes=2)
+    from cases import pulse_for, step_size
+    split = tb.Pipeline(config, SPLIT)
+    split.initialize_gaussian(pulse_for(config, 3))
+    dt = step_size(config)
+    split.step(0.0, dt, 3)
+    split.checkpoint_write(tmp_path / "split", dt, 3 * dt, 3)
+    ref = RefPipeline(config)
+    ref.checkpoint_load(tmp_path / "split", dt)
+    errors = _field_errors(split.get_state(), ref.get_state(), range(13))
+    assert max(errors) < 1e-12, errors

@@ -1972,22 +1972,34 @@ void NodalPipeline::evaluate(const double2* stage_in, double2* out) {
         return p == o.p && slots == o.slots && slot == o.slot;
       }
     };
-    AngularTileBatch batch{};
+    // pending operations by arithmetic: projections always run the FP64
+    // two-GEMM path (their output must be band limited relative to itself,
+    // as the reference's checkpoints require); the others follow the
+    // pipeline's precision
+    AngularTileBatch batch[2]{};  // [kPrecisionFp64], [kPrecisionSplit]
     std::vector<Plane> reads, writes;
-    void flush() {
-      if (batch.count == 0) return;
+    int pending() const { return batch[0].count + batch[1].count; }
+    void launch(const int prec) {
+      AngularTileBatch& bt = batch[prec];
+      if (bt.count == 0) return;
       const int tiles = g.modes * ((g.nr + kTileCtaRows - 1) / kTileCtaRows);
-      for (int i = 0; i <= batch.count; ++i) batch.first_block[i] = i * tiles;
-      const int words = self.precision_ == kPrecisionSplit ? self.tile_split_words_
-                                                           : self.tile_fp64_words_;
+      for (int i = 0; i <= bt.count; ++i) bt.first_block[i] = i * tiles;
+      const int words = prec == kPrecisionSplit ? self.tile_split_words_
+                                                : self.tile_fp64_words_;
       const size_t bytes = tile_smem_bytes(words);
-      const unsigned grid = static_cast<unsigned>(batch.count * tiles);
-      if (self.precision_ == kPrecisionSplit) {
-        angular_tile_kernel<kPrecisionSplit><<<grid, kTileWarps * 32, bytes, s>>>(g, tr, batch);
+      const unsigned grid = static_cast<unsigned>(bt.count * tiles);
+      if (prec == kPrecisionSplit) {
+        angular_tile_kernel<kPrecisionSplit><<<grid, kTileWarps * 32, bytes, s>>>(g, tr, bt);
       } else {
-        angular_tile_kernel<kPrecisionFp64><<<grid, kTileWarps * 32, bytes, s>>>(g, tr, batch);
+        angular_tile_kernel<kPrecisionFp64><<<grid, kTileWarps * 32, bytes, s>>>(g, tr, bt);
       }
-      batch.count = 0;
+      bt.count = 0;
+    }
+    // the pending operations are mutually independent, so the two launches
+    // may run in either order
+    void flush() {
+      launch(kPrecisionFp64);
+      launch(kPrecisionSplit);
       reads.clear();
       writes.clear();
     }
@@ -2000,13 +2012,14 @@ void NodalPipeline::evaluate(const double2* stage_in, double2* out) {
       const bool ghp = kind == kEth || kind == kEthPrime;
       const Plane r1{in.p, in.slots, in_slot}, r2{dt.p, dt.slots, dt_slot},
           w{o.p, o.slots, out_slot};
-      if (batch.count == kTileMaxOps || contains(writes, r1) ||
+      const int prec = kind == kProject ? kPrecisionFp64 : self.precision_;
+      if (batch[prec].count == kTileMaxOps || contains(writes, r1) ||
           (ghp && contains(writes, r2)) || contains(writes, w) ||
           contains(reads, w)) {
         flush();
       }
       const auto& d = b.coords[coord];
-      AngularTileParams& tp = batch.ops[batch.count++];
+      AngularTileParams& tp = batch[prec].ops[batch[prec].count++];
       tp = AngularTileParams{};
       tp.kind = kind;
       tp.in = in;
