@@ -49,6 +49,11 @@ enum Coord : int {
 enum OpKind : int { kProject = 0, kLaplacian = 1, kEth = 2, kEthPrime = 3 };
 
 constexpr int kBlock = 256;
+// resident 256-thread blocks per SM that the heaviest pointwise kernels
+// (Teukolsky RHS, reconstruction passes 2 and 3; 88-94 registers when
+// unbounded) are compiled for: three blocks instead of two per SM, more warps
+// per scheduler for their latency-bound loops over grid points
+constexpr int kPointBlocks = 3;
 constexpr int kMaxNodes = 96;  // theta nodes per row held by one warp
 constexpr double kTwoPi = 2.0 * std::numbers::pi_v<double>;
 
@@ -837,7 +842,7 @@ __global__ void teuk_primitives_kernel(const Geo g, const Trig tr,
 }
 
 // TeukolskyRhsFunctor (include/teuk/full_spatial.hpp:184-280)
-__global__ void teuk_rhs_kernel(const Geo g, const Trig tr,
+__global__ void __launch_bounds__(kBlock, kPointBlocks) teuk_rhs_kernel(const Geo g, const Trig tr,
                                 const TeukParams p) {
   const long long total = static_cast<long long>(g.modes) * g.nr * g.nt;
   for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
@@ -900,7 +905,7 @@ struct ReconParams {
 // evaluate_sbp_reconstruction_full_pass{1,2,3}
 // (include/teuk/full_spatial.hpp:494-695, reconstruction.hpp:46-121)
 template <int PASS>
-__global__ void recon_pass_kernel(const Geo g, const Trig tr,
+__global__ void __launch_bounds__(kBlock, kPointBlocks) recon_pass_kernel(const Geo g, const Trig tr,
                                   const ReconParams p) {
   const long long total = static_cast<long long>(g.modes) * g.nr * g.nt;
   for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
