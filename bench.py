@@ -366,7 +366,7 @@ def uneven_batch_run(tb, wl, steps: int, options=None, label="fp64"):
 
     solves = wl.uneven_batch()
     configs = [c for c, _, _ in solves]
-    batch = tb.Batch(configs, options)
+    batch = tb.Batch(configs, options or tb.LaunchOptions(autotune=True))
     stream = torch.cuda.Stream()
     batch.set_stream(stream.cuda_stream)
     for i, (_, pulse, _) in enumerate(solves):
@@ -617,7 +617,10 @@ def b200_arm(args):
     shape = config.shape()
     B = args.batch
     pinned = torch.empty((B, *shape), dtype=torch.complex128, pin_memory=True)
-    batch = build_batch(tb, wl, config, pulse, B, 1000 * (rank + 1), pinned)
+    # strip lengths chosen by the engine's autotuner at build (results are
+    # bit-identical for any choice)
+    tuned = tb.LaunchOptions(autotune=True)
+    batch = build_batch(tb, wl, config, pulse, B, 1000 * (rank + 1), pinned, tuned)
     stream = torch.cuda.Stream()
     batch.set_stream(stream.cuda_stream)
     dts = [dt] * B
@@ -662,6 +665,7 @@ def b200_arm(args):
     peak, peak_kind = measured_hbm_peak()
     streaming, _ = batch.stage_kernels()
     kernel = "stream_stage_kernel" if streaming else "stage_kernel"
+    strip_rows = batch.strip_rows()
     traffic = recorded_traffic(kernel, algorithmic_per_launch)
 
     # the same batch with split-precision transforms (BF16 digit slices,
@@ -669,7 +673,8 @@ def b200_arm(args):
     split = None
     if not args.no_split:
         sbatch = build_batch(tb, wl, config, pulse, B, 1000 * (rank + 1), pinned,
-                             tb.LaunchOptions(precision=tb.PRECISION_SPLIT))
+                             tb.LaunchOptions(precision=tb.PRECISION_SPLIT,
+                                              autotune=True))
         sbatch.set_stream(stream.cuda_stream)
         sbatch.step(dts, steps=max(args.warmup, 0), graph=True)
         sbatch.synchronize()
@@ -759,6 +764,8 @@ def b200_arm(args):
                          "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic,
                          "kernel": f"{kernel}<D10-5, free-damped>",
+                         "strip_rows": strip_rows,
+                         "strip_rows_source": "autotuner (batch build)",
                          "peak_source": f"{peak_kind} hbm_gbs",
                          "algorithmic_bytes_per_launch": algorithmic_per_launch},
             "cpu_baseline": cpu,
