@@ -494,13 +494,15 @@ def mapped_repo_libraries():
 
 
 def cpu_reference_samples(config, pulse, dt, warmup: int, samples: int | None,
-                          seconds: float = 15.0):
+                          seconds: float = 15.0, warm_seconds: float = 3.0):
     """The reference implementation on the host cores (oracle/_ref, thread
     pool over every core), else the C restatement (port, one core).  One
-    sample = one RK4 step of one solve of the workload.  `warmup` samples run
-    untimed; then `samples` samples (or as many as fit in about `seconds`)
-    are timed one by one.  Returns (grid-point updates/s over the timed
-    samples, description)."""
+    sample = one RK4 step of one solve of the workload.  Untimed steps run
+    first: at least `warmup`, and for at least `warm_seconds` (the
+    reference's first steps of a fresh pipeline run at about half its
+    steady rate, measured on the GPU boxes' hosts); then `samples` samples
+    (or as many as fit in about `seconds`) are timed one by one.  Returns
+    (grid-point updates/s over the timed samples, description)."""
     sys.path.insert(0, str(REPO / "tests"))
     import oracle_bindings as ob
     from teuk_b200 import workloads as wl
@@ -517,11 +519,14 @@ def cpu_reference_samples(config, pulse, dt, warmup: int, samples: int | None,
         pipe.set_state(state + wl.band_noise(config, 1, 1e-3))
         kind, cores = "port", 1
     t = 0.0
-    for _ in range(max(warmup, 1)):
+    untimed = 0
+    warm_start = time.perf_counter()
+    while untimed < max(warmup, 1) or time.perf_counter() - warm_start < warm_seconds:
         t0 = time.perf_counter()
         pipe.step(t, dt, 1)
         last = time.perf_counter() - t0
         t += dt
+        untimed += 1
     if samples is None:
         samples = max(3, min(2000, int(seconds / max(last, 1e-6))))
     times = []
@@ -536,8 +541,9 @@ def cpu_reference_samples(config, pulse, dt, warmup: int, samples: int | None,
     rates = sorted(gp / x for x in times)
     return gp * samples / total, {
         "kind": kind, "cores": cores,
-        "sample": f"{samples} timed RK4 steps (after {max(warmup, 1)} untimed) "
-                  f"of one solve of the workload ({gp} grid points per step)",
+        "sample": f"{samples} timed RK4 steps (after {untimed} untimed, at least "
+                  f"{warm_seconds:g} s) of one solve of the workload ({gp} grid "
+                  "points per step)",
         "seconds": total, "steps": samples,
         "per_step_rate": {"min": rates[0], "median": statistics.median(rates),
                           "max": rates[-1]},
