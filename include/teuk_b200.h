@@ -352,8 +352,9 @@ typedef struct teuk_b200_batch_options {
   /* streaming-kernel strip length in radial rows (0: the autotuner's or the
    * built-in choice; otherwise at least 64) */
   int strip_rows;
-  /* 1: time the candidate strip lengths of every streaming launch group at
-   * build and keep the fastest (cached per shape class for the process) */
+  /* 1: time the candidate strip lengths (64 to 4096 rows) of every
+   * streaming launch group at build and keep the fastest (cached per shape
+   * class for the process) */
   int autotune;
 } teuk_b200_batch_options;
 /* teuk_b200_create with launch choices (one solve; the second-order

@@ -16,7 +16,7 @@ from cases import CASES, pulse_for, step_size
 
 pytestmark = pytest.mark.gpu
 
-CANDIDATES = {64, 96, 128, 192, 256, 384, 512, 768, 1024}
+CANDIDATES = {64, 96, 128, 192, 256, 384, 512, 768, 1024, 1536, 2048, 4096}
 
 
 def _configs():

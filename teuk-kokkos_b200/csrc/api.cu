@@ -777,7 +777,8 @@ struct Batch {
 
   // The strip-length autotuner.  For every streaming launch group it times
   // one RK4 step (the four stage launches) of the group for each candidate
-  // strip length and keeps the fastest; the choice is cached for the
+  // strip length (64 to 4096 rows, up to the longest segment) and keeps the
+  // fastest; the choice is cached for the
   // process by (discretization, reduction, widest band, rows rounded to a
   // quarter octave, SM count).  Strips only decide which CTA streams which
   // rows: every row gets the same sums in the same order for any choice,
@@ -787,7 +788,8 @@ struct Batch {
   void autotune_strips() {
     static std::mutex cache_mutex;
     static std::map<std::tuple<int, int, int, int, int>, int> cache;
-    static const int kCandidates[] = {64, 96, 128, 192, 256, 384, 512, 768, 1024};
+    static const int kCandidates[] = {64,  96,  128,  192,  256,  384,
+                                      512, 768, 1024, 1536, 2048, 4096};
     const int sms = device_sms();
     cudaEvent_t ev[2] = {nullptr, nullptr};
     for (cudaEvent_t& e : ev) check(cudaEventCreate(&e), "cudaEventCreate");
