@@ -280,9 +280,10 @@ def one_at_a_time_rate(tb, wl, kinds, steps: int):
 
 
 def serving_run(tb, wl, capacity: float, requests: int, steps: int,
-                seed: int = 20260101):
+                seed: int = 20260101, precision: int = 0):
     """Poisson stream of the serving mix through the continuous-batching
-    server at ~80 % of its capacity; returns the 'serving' record."""
+    server (transforms in `precision`) at ~80 % of its capacity, against the
+    plain FP64 path one solve at a time; returns the 'serving' record."""
     import torch
 
     mix = wl.serving_mix(requests, seed)
@@ -302,7 +303,7 @@ def serving_run(tb, wl, capacity: float, requests: int, steps: int,
     arrivals -= arrivals[0]
     free, _ = torch.cuda.mem_get_info()
     budget = int(min(150e9, 0.8 * free))
-    server = tb.Server(hbm_budget_bytes=budget)
+    server = tb.Server(hbm_budget_bytes=budget, precision=precision)
     ids = []
     t0 = time.perf_counter()
     while True:
@@ -328,6 +329,7 @@ def serving_run(tb, wl, capacity: float, requests: int, steps: int,
     device_rate = st.grid_point_updates / st.device_seconds
     counts = {k: len(v) for k, v in by_kind.items()}
     return {
+        "precision": "split" if precision == tb.PRECISION_SPLIT else "fp64",
         "requests": requests,
         "mix": "40% schwarzschild a=0 nr=257 d8-4 ell<=8; 30% kerr_ringdown "
                "a=0.7 nr=1025 d10-5 ell<=16; 20% second_order a=0.9 nr=1025 "
@@ -743,10 +745,14 @@ def b200_arm(args):
     if rank == 0 and world == 1 and not args.no_uneven:
         uneven = uneven_batch_run(tb, wl, args.uneven_steps)
 
-    serving = None
+    serving = serving_split = None
     if rank == 0 and world == 1 and not args.no_serving:
         serving = serving_run(tb, wl, value, args.serve_requests,
                               args.serve_steps)
+        if not args.no_split:
+            serving_split = serving_run(tb, wl, value, args.serve_requests,
+                                        args.serve_steps,
+                                        precision=tb.PRECISION_SPLIT)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -778,6 +784,7 @@ def b200_arm(args):
             "split_precision": split,
             "e2e": e2e,
             "serving": serving,
+            "serving_split_precision": serving_split,
             "uneven_batch": uneven,
             "second_order": second_order,
             "gpu_launches": launches,
