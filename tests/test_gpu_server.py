@@ -179,3 +179,27 @@ def test_split_precision_server_matches_split_alone(require_gpu):
             assert np.array_equal(_values(records), _values(alone))
         else:
             _check_same(records, alone)
+
+
+def test_replicated_second_order_requests_match_alone_exactly(require_gpu):
+    """Same-configuration Unrestricted requests share one replicated nodal
+    pipeline: members join while others run (the pipeline's room grows from
+    two to four replicas, moving the members' states on the device), leave
+    at different steps (the last replica moves into the freed slot), and
+    every record equals the solve alone bit for bit."""
+    config = SECOND_ORDER["so_unrestricted_d84"]
+    dt = step_size(config)
+    server = tb.Server(hbm_budget_bytes=8 << 30)
+    plan = [(31, 7), (32, 3), (33, 5), (34, 2), (35, 6)]
+    jobs = []
+    for i, (seed, steps) in enumerate(plan):
+        pulse = pulse_for(config, seed)
+        jobs.append((server.submit(config, pulse, dt, steps), pulse, steps))
+        server.advance(1)
+    while server.advance(1) > 0:
+        pass
+    for rid, pulse, steps in jobs:
+        records, _ = server.result(rid)
+        alone = _alone(config, pulse, dt, steps)
+        assert _keys(records) == _keys(alone)
+        assert np.array_equal(_values(records), _values(alone)), rid

@@ -10,6 +10,7 @@
 #include <chrono>
 #include <deque>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <exception>
@@ -1362,7 +1363,8 @@ void require_device() {
 // for targets.
 void sample_nodal_endpoint(teuk_b200::NodalPipeline& nodal,
                            teuk_b200_waveform_record* out,
-                           const size_t capacity, size_t* count) {
+                           const size_t capacity, size_t* count,
+                           const int replica = 0) {
   using namespace teuk_b200;
   const InstancePlan& plan = nodal.plan();
   const Config& c = plan.config;
@@ -1376,7 +1378,7 @@ void sample_nodal_endpoint(teuk_b200::NodalPipeline& nodal,
     const std::vector<int>& members = order == 1 ? c.parents : c.targets;
     const int ell_max = order == 1 ? c.ell_max_first : c.ell_max_second;
     for (int boundary = 0; boundary < 2; ++boundary) {
-      nodal.endpoint_slice(field, boundary == 0 ? 0 : c.nr - 1, slice);
+      nodal.endpoint_slice(field, boundary == 0 ? 0 : c.nr - 1, slice, replica);
       for (size_t mode = 0; mode < c.modes.size(); ++mode) {
         const int m = c.modes[mode];
         if (!std::binary_search(members.begin(), members.end(), m)) continue;
@@ -1465,7 +1467,8 @@ void initialize_gaussian(Batch& b, const int instance,
 }
 
 void initialize_nodal_gaussian(teuk_b200::NodalPipeline& p,
-                               const teuk_b200_gaussian* pulse) {
+                               const teuk_b200_gaussian* pulse,
+                               const int replica = -1) {
   require(pulse != nullptr, "null Gaussian pulse");
   require(pulse->mode_count >= 0 &&
               (pulse->mode_count == 0 || pulse->modes != nullptr),
@@ -1482,6 +1485,10 @@ void initialize_nodal_gaussian(teuk_b200::NodalPipeline& p,
   teuk_b200::gaussian_initial_state(p.plan(), pulse->center, pulse->width,
                                     pulse->compact_support != 0, ell, m, re,
                                     im, nodal);
+  if (replica >= 0) {  // one replica of a replicated pipeline
+    p.set_replica_state(replica, nodal.data(), TEUK_B200_HOST);
+    return;
+  }
   p.set_state(nodal.data(), TEUK_B200_HOST);
   p.reset_activation();
 }
@@ -1534,10 +1541,56 @@ struct ServerRequest {
   double time = 0.0;
   std::unique_ptr<teuk_b200::NodalPipeline> nodal;
   cudaEvent_t joined = nullptr;  // end of this request's work of a step
+  // or, when it shares a replicated pipeline: its group and replica slot
+  struct NodalGroup* group = nullptr;
+  int replica = -1;
   ~ServerRequest() {
     if (joined != nullptr) cudaEventDestroy(joined);
   }
 };
+
+// Second-order requests with the Unrestricted source from t = 0 that share
+// their configuration, precision and dt are replicas of one nodal pipeline
+// (stepped by the same launches; each replica's results equal the solve
+// alone bit for bit).  The pipeline's room grows by doubling; a retiring
+// member's slot takes the last replica's state.
+struct NodalGroup {
+  std::string key;
+  teuk_b200::InstancePlan plan;
+  double dt = 0.0;
+  double time = 0.0;  // the source is on throughout: the RHS does not depend on it
+  std::unique_ptr<teuk_b200::NodalPipeline> pipe;
+  std::vector<ServerRequest*> members;  // replica k = members[k]
+  cudaEvent_t joined = nullptr;
+  ~NodalGroup() {
+    pipe.reset();
+    if (joined != nullptr) cudaEventDestroy(joined);
+  }
+};
+
+// Text key of everything a replicated pipeline shares.
+std::string nodal_group_key(const teuk_b200::Config& c, const int precision,
+                            const double dt) {
+  std::string k;
+  const auto num = [&](const double v) {
+    char buf[40];
+    std::snprintf(buf, sizeof(buf), "%a,", v);
+    k += buf;
+  };
+  const auto ints = [&](const std::vector<int>& v) {
+    for (const int x : v) k += std::to_string(x) + " ";
+    k += ";";
+  };
+  num(c.mass); num(c.spin); num(c.length); num(c.damping); num(c.dissipation);
+  num(c.source_start_time); num(c.constraint_tolerance); num(dt);
+  k += std::to_string(c.nr) + "," + std::to_string(c.ntheta) + "," +
+       std::to_string(c.ell_max_first) + "," + std::to_string(c.ell_max_second) +
+       "," + std::to_string(c.reduction) + "," + std::to_string(c.disc) + "," +
+       std::to_string(c.source_mode) + "," + std::to_string(c.required_passes) +
+       "," + std::to_string(precision) + ";";
+  ints(c.modes); ints(c.parents); ints(c.targets);
+  return k;
+}
 
 // Continuous batching over Batch: admitted solves share one batched RK4
 // step; a change of membership rebuilds the batch layout and moves the band
@@ -1680,7 +1733,9 @@ class Server {
       }
       if (active_bytes_ + r->footprint > options_.hbm_budget_bytes) break;
       active_bytes_ += r->footprint;
-      if (r->second_order) {
+      if (r->second_order && groupable(*r)) {
+        join_group(*r);
+      } else if (r->second_order) {
         start_nodal(*r);
       } else {
         changed = true;
@@ -1702,6 +1757,74 @@ class Server {
     teuk_b200::check(cudaEventCreateWithFlags(&r.joined, cudaEventDisableTiming),
                      "cudaEventCreate");
     r.time = 0.0;
+  }
+
+  static bool groupable(const ServerRequest& r) {
+    return r.config.source_mode == TEUK_B200_SOURCE_UNRESTRICTED &&
+           r.config.source_start_time == 0.0;
+  }
+
+  // Adds a second-order request to its group as the next replica, growing
+  // the group's pipeline (state of the members moved on the device) when
+  // it has no room left.
+  void join_group(ServerRequest& r) {
+    const std::string key = nodal_group_key(r.config, options_.precision, r.dt);
+    NodalGroup* g = nullptr;
+    for (const auto& grp : groups_) {
+      if (grp->key == key) g = grp.get();
+    }
+    if (g == nullptr) {
+      auto created = std::make_unique<NodalGroup>();
+      created->key = key;
+      created->plan = r.plan;
+      created->dt = r.dt;
+      teuk_b200::check(
+          cudaEventCreateWithFlags(&created->joined, cudaEventDisableTiming),
+          "cudaEventCreate");
+      g = created.get();
+      groups_.push_back(std::move(created));
+    }
+    const int k = static_cast<int>(g->members.size());
+    if (!g->pipe || k + 1 > g->pipe->replicas()) {
+      collect_step_times();
+      const int room = std::max(k + 1, g->pipe ? 2 * g->pipe->replicas() : 2);
+      auto next = std::make_unique<teuk_b200::NodalPipeline>(
+          g->plan, options_.precision, room);
+      next->set_active_replicas(k + 1);
+      for (int i = 0; i < k; ++i) next->copy_replica_from(*g->pipe, i, i);
+      g->pipe = std::move(next);
+    } else {
+      g->pipe->set_active_replicas(k + 1);
+    }
+    teuk_b200_gaussian pulse = r.pulse;
+    pulse.modes = r.modes.data();
+    initialize_nodal_gaussian(*g->pipe, &pulse, k);
+    g->members.push_back(&r);
+    r.group = g;
+    r.replica = k;
+  }
+
+  // Records of a finished group member; the last replica moves into its
+  // slot.  An empty group releases its pipeline.
+  void leave_group(ServerRequest& r, teuk_b200_waveform_record* out,
+                   const size_t capacity, size_t* count) {
+    NodalGroup* g = r.group;
+    collect_step_times();
+    sample_nodal_endpoint(*g->pipe, out, capacity, count, r.replica);
+    const int last = static_cast<int>(g->members.size()) - 1;
+    if (r.replica != last) {
+      g->pipe->copy_replica_from(*g->pipe, last, r.replica);
+      g->members[static_cast<size_t>(r.replica)] = g->members[static_cast<size_t>(last)];
+      g->members[static_cast<size_t>(r.replica)]->replica = r.replica;
+    }
+    g->members.pop_back();
+    if (g->members.empty()) {
+      g->pipe.reset();
+    } else {
+      g->pipe->set_active_replicas(static_cast<int>(g->members.size()));
+    }
+    r.group = nullptr;
+    r.replica = -1;
   }
 
   std::vector<std::shared_ptr<ServerRequest>> linear_active() const {
@@ -1786,13 +1909,22 @@ class Server {
     teuk_b200::check(cudaEventRecord(start, stream_), "event");
     if (batch_ && !dts.empty()) batch_->step(dts, 1, options_.graph != 0);
     for (const auto& r : active_) {
-      if (!r->second_order) continue;
+      if (!r->second_order || r->group != nullptr) continue;
       teuk_b200::check(cudaStreamWaitEvent(r->nodal->stream(), start, 0),
                        "nodal fork");
       r->nodal->step(r->time, r->dt);
       r->time += r->dt;
       teuk_b200::check(cudaEventRecord(r->joined, r->nodal->stream()), "event");
       teuk_b200::check(cudaStreamWaitEvent(stream_, r->joined, 0), "nodal join");
+    }
+    for (const auto& g : groups_) {
+      if (g->members.empty()) continue;
+      teuk_b200::check(cudaStreamWaitEvent(g->pipe->stream(), start, 0),
+                       "group fork");
+      g->pipe->step(g->time, g->dt);
+      g->time += g->dt;
+      teuk_b200::check(cudaEventRecord(g->joined, g->pipe->stream()), "event");
+      teuk_b200::check(cudaStreamWaitEvent(stream_, g->joined, 0), "group join");
     }
     teuk_b200::check(cudaEventRecord(events_[2 * pending_ + 1], stream_),
                      "event");
@@ -1829,7 +1961,9 @@ class Server {
       size_t count = 0;
       r->records.resize(2 * c.modes.size() *
                         static_cast<size_t>(c.ell_max_first + c.ell_max_second + 2));
-      if (r->second_order) {
+      if (r->group != nullptr) {
+        leave_group(*r, r->records.data(), r->records.size(), &count);
+      } else if (r->second_order) {
         collect_step_times();
         sample_nodal_endpoint(*r->nodal, r->records.data(), r->records.size(),
                               &count);
@@ -1855,6 +1989,7 @@ class Server {
   cudaMemPool_t pool_ = nullptr;     // the arena's memory pool
   int pending_ = 0;
   std::unique_ptr<Batch> batch_;
+  std::vector<std::unique_ptr<NodalGroup>> groups_;  // replicated second order
   std::deque<std::shared_ptr<ServerRequest>> queue_;
   std::vector<std::shared_ptr<ServerRequest>> active_;
   std::unordered_map<uint64_t, std::shared_ptr<ServerRequest>> requests_;

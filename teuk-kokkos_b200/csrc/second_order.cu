@@ -1471,12 +1471,22 @@ struct NodalPipeline::Buffers {
   }
 };
 
-NodalPipeline::NodalPipeline(const InstancePlan& plan, const int precision)
-    : plan_(plan), precision_(precision), buf_(std::make_unique<Buffers>()) {
+NodalPipeline::NodalPipeline(const InstancePlan& plan, const int precision,
+                             const int replicas)
+    : plan_(plan), precision_(precision), replicas_(replicas),
+      active_(replicas), buf_(std::make_unique<Buffers>()) {
   if (precision != kPrecisionFp64 && precision != kPrecisionSplit) {
     throw std::invalid_argument("unknown transform precision");
   }
   const Config& c = plan_.config;
+  if (replicas < 1) throw std::invalid_argument("replica count must be positive");
+  // Replicas share one latch, so only solves whose source is on from the
+  // start (no constraint-driven or time-driven switch) are replicated.
+  if (replicas > 1 && !(c.source_mode == TEUK_B200_SOURCE_UNRESTRICTED &&
+                        c.source_start_time == 0.0)) {
+    throw std::invalid_argument(
+        "replicated second-order pipelines need the Unrestricted source from t = 0");
+  }
   if (c.ntheta > kMaxNodes) {
     throw std::invalid_argument(
         "the second-order pipeline supports at most 96 theta nodes");
@@ -1492,12 +1502,15 @@ NodalPipeline::NodalPipeline(const InstancePlan& plan, const int precision)
   b.geo.dissipation = c.dissipation;
   b.geo.nr = c.nr;
   b.geo.nt = c.ntheta;
-  b.geo.modes = static_cast<int>(c.modes.size());
+  b.geo.modes = static_cast<int>(c.modes.size()) * replicas;
   b.geo.disc = c.disc;
   b.geo.reduction = c.reduction;
   check(upload_nodal_sbp_constants(), "upload SBP constants");
 
-  const size_t nm = c.modes.size();
+  // one replica's modes; buffers and tables hold `replicas` of them, replica
+  // k in modes [k nm, (k + 1) nm)
+  const size_t nm1 = c.modes.size();
+  const size_t nm = nm1 * static_cast<size_t>(replicas);
   b.plane = static_cast<size_t>(c.nr) * static_cast<size_t>(c.ntheta);
   const size_t full = nm * kFieldCount * b.plane;
   b.state = b.alloc<double2>(full);
@@ -1551,8 +1564,28 @@ NodalPipeline::NodalPipeline(const InstancePlan& plan, const int precision)
     }
   }
   pair_offsets_.push_back(static_cast<int>(pair_index1_.size()));
-  b.pair_count = static_cast<int>(pair_index1_.size());
-  b.target_count = static_cast<int>(targets_.size());
+  pairs_per_replica_ = static_cast<int>(pair_index1_.size());
+  targets_per_replica_ = static_cast<int>(targets_.size());
+  // replicate the pair tables, offset by each replica's first mode and pair
+  {
+    const std::vector<int> i1 = pair_index1_, i2 = pair_index2_,
+                           po = pair_offsets_, tg = targets_;
+    const int P = pairs_per_replica_, nmi = static_cast<int>(nm1);
+    pair_offsets_.clear();
+    for (int k = 1; k < replicas; ++k) {
+      for (size_t j = 0; j < i1.size(); ++j) {
+        pair_index1_.push_back(i1[j] + k * nmi);
+        pair_index2_.push_back(i2[j] + k * nmi);
+      }
+      for (const int t : tg) targets_.push_back(t + k * nmi);
+    }
+    for (int k = 0; k < replicas; ++k) {
+      for (size_t j = 0; j + 1 < po.size(); ++j) pair_offsets_.push_back(po[j] + k * P);
+    }
+    pair_offsets_.push_back(P * replicas);
+  }
+  b.pair_count = pairs_per_replica_ * replicas;
+  b.target_count = targets_per_replica_ * replicas;
   b.pairs = b.alloc<double2>(std::max<size_t>(pair_index1_.size(), 1) * 2 * b.plane);
   b.pairs_t = b.alloc<double2>(std::max<size_t>(pair_index1_.size(), 1) * 2 * b.plane);
 
@@ -1590,9 +1623,17 @@ NodalPipeline::NodalPipeline(const InstancePlan& plan, const int precision)
     if (v.empty()) ints.push_back(0);
     return off;
   };
+  // per-mode tables of every replica
+  const auto replicate = [&](const std::vector<int>& v) {
+    std::vector<int> out;
+    for (int k = 0; k < replicas; ++k) out.insert(out.end(), v.begin(), v.end());
+    return out;
+  };
   std::vector<int> sharp(nm);
-  for (size_t i = 0; i < nm; ++i) sharp[i] = index_of(-c.modes[i]);
-  const size_t off_m = push(c.modes), off_sh = push(sharp);
+  for (size_t i = 0; i < nm; ++i) {
+    sharp[i] = index_of(-c.modes[i % nm1]) + static_cast<int>((i / nm1) * nm1);
+  }
+  const size_t off_m = push(replicate(c.modes)), off_sh = push(sharp);
   const size_t off_i1 = push(pair_index1_), off_i2 = push(pair_index2_),
                off_po = push(pair_offsets_), off_tg = push(targets_);
   size_t coord_offsets[cCount][14];
@@ -1603,14 +1644,14 @@ NodalPipeline::NodalPipeline(const InstancePlan& plan, const int precision)
         nullptr, nullptr, nullptr, &a.n_ell, &a.ell_min, &a.n_ell_up,
         &a.ell_min_up, &a.n_ell_down, &a.ell_min_down};
     for (int l = 0; l < 14; ++l) {
-      coord_offsets[k][l] = lists[l] ? push(*lists[l]) : 0;
+      coord_offsets[k][l] = lists[l] ? push(replicate(*lists[l])) : 0;
     }
   }
   // pool offsets of each mode's Laplacian / raising / lowering diagonal
   for (int k = 0; k < cCount; ++k) {
-    coord_offsets[k][5] = push(coordinator_diag_[k][0]);
-    coord_offsets[k][6] = push(coordinator_diag_[k][1]);
-    coord_offsets[k][7] = push(coordinator_diag_[k][2]);
+    coord_offsets[k][5] = push(replicate(coordinator_diag_[k][0]));
+    coord_offsets[k][6] = push(replicate(coordinator_diag_[k][1]));
+    coord_offsets[k][7] = push(replicate(coordinator_diag_[k][2]));
   }
   b.ints = b.alloc<int>(ints.size());
   check(cudaMemcpy(b.ints, ints.data(), ints.size() * sizeof(int),
@@ -1659,7 +1700,7 @@ NodalPipeline::NodalPipeline(const InstancePlan& plan, const int precision)
     std::vector<int> offs;
     for (int k = 0; k < cCount; ++k) {
       for (int kind = 0; kind < 4; ++kind) {
-        const auto& v = tile_offsets_[k][kind];
+        const auto v = replicate(tile_offsets_[k][kind]);  // 4 ints per mode
         offs.insert(offs.end(), v.begin(), v.end());
       }
     }
@@ -1671,7 +1712,7 @@ NodalPipeline::NodalPipeline(const InstancePlan& plan, const int precision)
     for (int k = 0; k < cCount; ++k) {
       for (int kind = 0; kind < 4; ++kind) {
         b.tile_offsets[k][kind] = d_offs + at;
-        at += tile_offsets_[k][kind].size();
+        at += tile_offsets_[k][kind].size() * static_cast<size_t>(replicas);
       }
     }
   }
@@ -2406,17 +2447,64 @@ void NodalPipeline::evaluate_rhs(const double* stage, double* out,
   check(cudaStreamSynchronize(stream_), "evaluate_rhs");
 }
 
+void NodalPipeline::set_active_replicas(const int k) {
+  if (k < 1 || k > replicas_) {
+    throw std::invalid_argument("active replica count outside the pipeline's room");
+  }
+  if (k == active_) return;
+  check(cudaStreamSynchronize(stream_), "replica change");
+  const int nm1 = static_cast<int>(plan_.config.modes.size());
+  active_ = k;
+  buf_->geo.modes = nm1 * k;
+  buf_->target_count = targets_per_replica_ * k;
+  buf_->pair_count = pairs_per_replica_ * k;
+  for (StepGraph& g : graphs_) release_graph(g);  // recorded for the old count
+}
+
+void NodalPipeline::set_replica_state(const int k, const double* state,
+                                      const int memory) {
+  if (k < 0 || k >= replicas_) throw std::invalid_argument("replica index out of range");
+  const size_t n = plan_.value_count();
+  check(cudaMemcpyAsync(buf_->state + static_cast<size_t>(k) * n, state,
+                        n * sizeof(double2),
+                        memory == TEUK_B200_HOST ? cudaMemcpyHostToDevice
+                                                 : cudaMemcpyDeviceToDevice,
+                        stream_),
+        "set replica state");
+  check(cudaStreamSynchronize(stream_), "set replica state");
+}
+
+void NodalPipeline::copy_replica_from(const NodalPipeline& src, const int src_k,
+                                      const int dst_k) {
+  if (src_k < 0 || src_k >= src.replicas_ || dst_k < 0 || dst_k >= replicas_ ||
+      src.plan_.value_count() != plan_.value_count()) {
+    throw std::invalid_argument("replica copy between different shapes");
+  }
+  const size_t n = plan_.value_count();
+  // the source's pending steps come first
+  check(cudaStreamSynchronize(src.stream_), "replica copy");
+  check(cudaMemcpyAsync(buf_->state + static_cast<size_t>(dst_k) * n,
+                        src.buf_->state + static_cast<size_t>(src_k) * n,
+                        n * sizeof(double2), cudaMemcpyDeviceToDevice, stream_),
+        "replica copy");
+  check(cudaStreamSynchronize(stream_), "replica copy");
+}
+
 void NodalPipeline::endpoint_slice(const int field, const int radial,
-                                   std::vector<double2>& out) {
+                                   std::vector<double2>& out, const int replica) {
   const Config& c = plan_.config;
   const size_t nm = c.modes.size(), nt = static_cast<size_t>(c.ntheta);
+  if (replica < 0 || replica >= active_) {
+    throw std::invalid_argument("replica index out of range");
+  }
   out.resize(nm * nt);
-  for (size_t mode = 0; mode < nm; ++mode) {
+  for (size_t mode0 = 0; mode0 < nm; ++mode0) {
+    const size_t mode = mode0 + static_cast<size_t>(replica) * nm;
     const size_t off = ((mode * kFieldCount + static_cast<size_t>(field)) *
                             static_cast<size_t>(c.nr) +
                         static_cast<size_t>(radial)) *
                        nt;
-    check(cudaMemcpyAsync(out.data() + mode * nt, buf_->state + off,
+    check(cudaMemcpyAsync(out.data() + mode0 * nt, buf_->state + off,
                           nt * sizeof(double2), cudaMemcpyDeviceToHost, stream_),
           "endpoint slice");
   }

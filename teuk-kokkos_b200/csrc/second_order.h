@@ -83,15 +83,33 @@ class NodalPipeline {
  public:
   struct Buffers;
   // precision 0: FP64 transforms; 1: split-precision (BF16 digits, FP32
-  // accumulation, FP64 recombination) tensor-core transforms
-  explicit NodalPipeline(const InstancePlan& plan, int precision = 0);
+  // accumulation, FP64 recombination) tensor-core transforms.
+  // replicas > 1: room for that many independent solves of the same plan,
+  // replica k in modes [k n, (k + 1) n) of every array (n = the plan's
+  // modes), all stepped by the same launches; each replica's results equal
+  // the solve alone bit for bit (every kernel works per mode and grid point,
+  // and the pair tables stay inside a replica).  Replicas share one latch,
+  // so they need the Unrestricted source from t = 0.
+  explicit NodalPipeline(const InstancePlan& plan, int precision = 0,
+                         int replicas = 1);
   int precision() const { return precision_; }
+  int replicas() const { return replicas_; }
+  int active_replicas() const { return active_; }
+  // Steps advance replicas [0, k) only (1 <= k <= replicas()).
+  void set_active_replicas(int k);
+  // State of replica k (the plan's value_count() complex values).
+  void set_replica_state(int k, const double* state, int memory);
+  // Device copy of replica src_k of `src` (same plan) into replica dst_k.
+  void copy_replica_from(const NodalPipeline& src, int src_k, int dst_k);
   ~NodalPipeline();
   NodalPipeline(const NodalPipeline&) = delete;
   NodalPipeline& operator=(const NodalPipeline&) = delete;
 
   const InstancePlan& plan() const { return plan_; }
-  size_t value_count() const { return plan_.value_count(); }
+  // complex values of the active replicas' states
+  size_t value_count() const {
+    return plan_.value_count() * static_cast<size_t>(active_);
+  }
   void set_stream(cudaStream_t stream);
   cudaStream_t stream() const { return stream_; }
 
@@ -105,8 +123,10 @@ class NodalPipeline {
   SourceActivation activation() const { return activation_; }
   const ConstraintNorms& constraint_norms() const { return norms_; }
   // Endpoint psi of the first-order (field 2) or second-order (field 12)
-  // state: (mode, theta) nodal values at radial index `radial`.
-  void endpoint_slice(int field, int radial, std::vector<double2>& out);
+  // state of one replica: (mode, theta) nodal values at radial index
+  // `radial`.
+  void endpoint_slice(int field, int radial, std::vector<double2>& out,
+                      int replica = 0);
   // Storage views of the reference pipeline: state, storage rhs (written by
   // the latch check), source_over_r3, forcing.
   const double2* state_device() const;
@@ -134,6 +154,10 @@ class NodalPipeline {
 
   InstancePlan plan_;
   int precision_ = 0;
+  int replicas_ = 1;
+  int active_ = 1;
+  int pairs_per_replica_ = 0;
+  int targets_per_replica_ = 0;
   // composite tile operators: used when ntheta <= 64
   bool tile_operators_ = false;
   int tile_fp64_words_ = 0;   // 8-byte words of one FP64 operator
