@@ -1790,6 +1790,7 @@ class Server {
       const int room = std::max(k + 1, g->pipe ? 2 * g->pipe->replicas() : 2);
       auto next = std::make_unique<teuk_b200::NodalPipeline>(
           g->plan, options_.precision, room);
+      next->reset_activation();  // the source is on from t = 0
       next->set_active_replicas(k + 1);
       for (int i = 0; i < k; ++i) next->copy_replica_from(*g->pipe, i, i);
       g->pipe = std::move(next);
