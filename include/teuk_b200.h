@@ -325,7 +325,16 @@ int teuk_b200_diagnostics_sample(teuk_b200_pipeline* pipeline,
 int teuk_b200_footprint_bytes(const teuk_b200_config* config,
                               size_t* bytes);
 
-/* ---- batched solves: one set of stage launches for all instances ----- */
+/* ---- batched solves: one set of stage launches for all instances -----
+ * Linear solves (source disabled) of any mix of shapes and
+ * discretizations.  Second-order solves batch only as identical
+ * configurations with the Unrestricted source from t = 0: they become the
+ * replicas of one nodal pipeline, whose RHS launches serve all of them at
+ * once; each replica's results equal the solve alone bit for bit.  Such a
+ * batch starts at t = 0 and keeps its own time; it shares one dt across its
+ * instances, has no band endpoint coefficients (Unsupported) and no fixed
+ * launch count (Unsupported).  Any other batch holding a second-order
+ * configuration is Unsupported. */
 int teuk_b200_batch_create(const teuk_b200_config* configs, int count,
                            teuk_b200_batch** out);
 

@@ -208,6 +208,53 @@ def test_second_order_waveforms(require_gpu, name):
         assert relative_error(gv, rv) < TOL
 
 
-def test_batch_rejects_second_order(require_gpu):
+def test_batch_of_identical_second_order_solves(require_gpu):
+    """Identical Unrestricted solves from t = 0 form one batch: the replicas
+    of one nodal pipeline, stepped by shared launches.  Each replica's
+    13-field state and waveform records equal those of the solve alone bit
+    for bit, and one replica is checked against the reference build."""
+    config = SO_CASES["so_unrestricted_d84"]
+    dt = step_size(config)
+    seeds = (21, 22, 23)
+    batch = tb.Batch([config] * len(seeds))
+    assert len(batch) == 3 and batch.strip_rows() == []
+    assert batch.stage_kernels() == (0, 0)
+    for i, seed in enumerate(seeds):
+        batch.initialize_gaussian(i, pulse_for(config, seed))
+    ref = RefPipeline(config)
+    ref.initialize_gaussian(pulse_for(config, seeds[1]))
+    batch.step(dt, 3)
+    batch.step(dt, 2)
+    ref.step(0.0, dt, 5)
+    _compare_fields(batch.get_state(1), ref.get_state())
+    for i, seed in enumerate(seeds):
+        alone = tb.Pipeline(config)
+        alone.initialize_gaussian(pulse_for(config, seed))
+        alone.step(0.0, dt, 5)
+        assert np.array_equal(batch.get_state(i), alone.get_state()), i
+        assert batch.sample_endpoint(i) == alone.sample_endpoint(), i
+    # a state written into one replica changes only that replica
+    state = _generic_state(ref, 43)
+    before = batch.get_state(2)
+    batch.set_state(0, state)
+    assert np.array_equal(batch.get_state(0), state)
+    assert np.array_equal(batch.get_state(2), before)
     with pytest.raises(tb.Unsupported):
-        tb.Batch([SO_CASES["so_unrestricted_d84"]])
+        batch.endpoint_modal()
+    with pytest.raises(IndexError):
+        batch.get_state(3)
+
+
+def test_batch_rejects_other_second_order_mixes(require_gpu):
+    """Second-order batches other than identical Unrestricted-from-zero
+    solves stay with one pipeline each."""
+    un = SO_CASES["so_unrestricted_d84"]
+    cases = [
+        [SO_CASES["so_constraint_d42_sc"]] * 2,
+        [un, SO_CASES["so_kerr_d105_start"]],
+        [un, dataclasses.replace(un, source_mode=tb.SOURCE_DISABLED)],
+        [dataclasses.replace(un, source_start_time=0.5)] * 2,
+    ]
+    for configs in cases:
+        with pytest.raises(tb.Unsupported):
+            tb.Batch(configs)

@@ -1331,6 +1331,10 @@ using teuk_b200::guarded;
 
 struct teuk_b200_batch {
   std::unique_ptr<Batch> batch;
+  // or: identical second-order solves with the Unrestricted source from
+  // t = 0, the replicas of one nodal pipeline
+  std::unique_ptr<teuk_b200::NodalPipeline> nodal;
+  double time = 0.0;
 };
 struct teuk_b200_pipeline {
   // exactly one of the two is set: the band-storage batch of one solve for
@@ -2616,6 +2620,14 @@ int teuk_b200_footprint_bytes(const teuk_b200_config* config, size_t* bytes) {
   });
 }
 
+namespace {
+void nodal_instance(const teuk_b200_batch& b, const int instance) {
+  if (instance < 0 || instance >= b.nodal->replicas()) {
+    throw std::out_of_range("batch instance index is out of range");
+  }
+}
+}  // namespace
+
 int teuk_b200_batch_create_with_options(const teuk_b200_config* configs,
                                         int count,
                                         const teuk_b200_batch_options* options,
@@ -2629,6 +2641,31 @@ int teuk_b200_batch_create_with_options(const teuk_b200_config* configs,
       list.push_back(teuk_b200::to_config(configs[i]));
     }
     auto b = std::make_unique<teuk_b200_batch>();
+    size_t second = 0;
+    for (const auto& c : list) second += c.source_mode != TEUK_B200_SOURCE_DISABLED;
+    if (second > 0) {
+      // validated like every pipeline first, then packed as replicas
+      const teuk_b200::InstancePlan plan = teuk_b200::build_instance_plan(list[0]);
+      const std::string key = nodal_group_key(list[0], opts.precision, 0.0);
+      bool same = second == list.size();
+      for (const auto& c : list) {
+        teuk_b200::build_instance_plan(c);
+        same = same && nodal_group_key(c, opts.precision, 0.0) == key;
+      }
+      if (!same || list[0].source_mode != TEUK_B200_SOURCE_UNRESTRICTED ||
+          list[0].source_start_time != 0.0) {
+        throw teuk_b200::Unsupported(
+            "a batch of second-order solves needs identical configurations "
+            "with the Unrestricted source from t = 0; other second-order "
+            "solves run through teuk_b200_create (one nodal pipeline each)");
+      }
+      require_device();
+      b->nodal = std::make_unique<teuk_b200::NodalPipeline>(
+          plan, opts.precision, static_cast<int>(list.size()));
+      b->nodal->reset_activation();
+      *out = b.release();
+      return;
+    }
     b->batch = std::make_unique<Batch>();
     b->batch->options = opts;
     b->batch->build(list);
@@ -2647,7 +2684,8 @@ int teuk_b200_batch_strip_rows(const teuk_b200_batch* b, int* rows,
     require(b != nullptr && count != nullptr && capacity >= 0 &&
                 (rows != nullptr || capacity == 0),
             "null argument");
-    const auto& v = b->batch->group_strip_rows;
+    static const std::vector<int> none;
+    const auto& v = b->batch ? b->batch->group_strip_rows : none;
     const int n = std::min(capacity, static_cast<int>(v.size()));
     for (int i = 0; i < n; ++i) rows[i] = v[static_cast<size_t>(i)];
     *count = static_cast<int>(v.size());
@@ -2662,7 +2700,8 @@ int teuk_b200_batch_destroy(teuk_b200_batch* batch) {
 int teuk_b200_batch_size(const teuk_b200_batch* b, int* count) {
   return guarded([&] {
     require(b != nullptr && count != nullptr, "null argument");
-    *count = static_cast<int>(b->batch->plans.size());
+    *count = b->nodal ? b->nodal->replicas()
+                      : static_cast<int>(b->batch->plans.size());
   });
 }
 
@@ -2670,6 +2709,11 @@ int teuk_b200_batch_shape(const teuk_b200_batch* b, int instance,
                           size_t shape[4]) {
   return guarded([&] {
     require(b != nullptr && shape != nullptr, "null argument");
+    if (b->nodal) {
+      nodal_instance(*b, instance);
+      fill_shape(b->nodal->plan(), shape);
+      return;
+    }
     b->batch->check_instance(instance);
     fill_shape(b->batch->plans[static_cast<size_t>(instance)], shape);
   });
@@ -2679,6 +2723,14 @@ int teuk_b200_batch_set_state(teuk_b200_batch* b, int instance,
                               const double* state, size_t count, int memory) {
   return guarded([&] {
     require(b != nullptr, "null batch");
+    if (b->nodal) {
+      nodal_instance(*b, instance);
+      require(count == b->nodal->plan().value_count(),
+              "state complex count does not match shape");
+      require(state != nullptr, "null state pointer");
+      b->nodal->set_replica_state(instance, state, memory);
+      return;
+    }
     b->batch->set_state(instance, state, count, memory);
   });
 }
@@ -2687,6 +2739,14 @@ int teuk_b200_batch_get_state(teuk_b200_batch* b, int instance,
                               double* state, size_t count, int memory) {
   return guarded([&] {
     require(b != nullptr, "null batch");
+    if (b->nodal) {
+      nodal_instance(*b, instance);
+      require(count == b->nodal->plan().value_count(),
+              "state complex count does not match shape");
+      require(state != nullptr, "null state pointer");
+      b->nodal->get_replica_state(instance, state, memory);
+      return;
+    }
     b->batch->get_state(instance, state, count, memory);
   });
 }
@@ -2695,6 +2755,11 @@ int teuk_b200_batch_initialize_gaussian(teuk_b200_batch* b, int instance,
                                         const teuk_b200_gaussian* pulse) {
   return guarded([&] {
     require(b != nullptr, "null batch");
+    if (b->nodal) {
+      nodal_instance(*b, instance);
+      initialize_nodal_gaussian(*b->nodal, pulse, instance);
+      return;
+    }
     initialize_gaussian(*b->batch, instance, pulse);
   });
 }
@@ -2703,6 +2768,19 @@ int teuk_b200_batch_step(teuk_b200_batch* b, const double* dt, int steps,
                          int graph) {
   return guarded([&] {
     require(b != nullptr && dt != nullptr, "null argument");
+    if (b->nodal) {
+      require(steps >= 0, "step count must be nonnegative");
+      const int n = b->nodal->replicas();
+      for (int i = 1; i < n; ++i) {
+        require(dt[i] == dt[0], "replicated second-order solves share one time step");
+      }
+      for (int s = 0; s < steps; ++s) {
+        b->nodal->step(b->time, dt[0]);
+        b->time += dt[0];
+      }
+      teuk_b200::check(cudaStreamSynchronize(b->nodal->stream()), "step");
+      return;
+    }
     std::vector<double> list(dt, dt + b->batch->plans.size());
     b->batch->step(list, steps, graph != 0);
   });
@@ -2713,6 +2791,11 @@ int teuk_b200_batch_sample_endpoint(teuk_b200_batch* b, int instance,
                                     size_t capacity, size_t* count) {
   return guarded([&] {
     require(b != nullptr, "null batch");
+    if (b->nodal) {
+      nodal_instance(*b, instance);
+      sample_nodal_endpoint(*b->nodal, out, capacity, count, instance);
+      return;
+    }
     b->batch->sample_endpoint(instance, out, capacity, count);
   });
 }
@@ -2722,6 +2805,10 @@ int teuk_b200_batch_endpoint_modal(teuk_b200_batch* b, double* out,
                                    int memory) {
   return guarded([&] {
     require(b != nullptr, "null batch");
+    if (b->nodal) {
+      throw teuk_b200::Unsupported(
+          "band endpoint coefficients exist for linear batches only");
+    }
     b->batch->endpoint_modal(out, capacity, count, memory);
   });
 }
@@ -2729,6 +2816,10 @@ int teuk_b200_batch_endpoint_modal(teuk_b200_batch* b, double* out,
 int teuk_b200_batch_set_stream(teuk_b200_batch* b, void* cuda_stream) {
   return guarded([&] {
     require(b != nullptr, "null batch");
+    if (b->nodal) {
+      b->nodal->set_stream(static_cast<cudaStream_t>(cuda_stream));
+      return;
+    }
     b->batch->stream = cuda_stream != nullptr
                            ? static_cast<cudaStream_t>(cuda_stream)
                            : b->batch->own_stream;
@@ -2738,6 +2829,10 @@ int teuk_b200_batch_set_stream(teuk_b200_batch* b, void* cuda_stream) {
 int teuk_b200_batch_synchronize(teuk_b200_batch* b) {
   return guarded([&] {
     require(b != nullptr, "null batch");
+    if (b->nodal) {
+      teuk_b200::check(cudaStreamSynchronize(b->nodal->stream()), "synchronize");
+      return;
+    }
     teuk_b200::check(cudaStreamSynchronize(b->batch->stream), "synchronize");
     b->batch->check_kernel_error();
   });
@@ -2747,6 +2842,10 @@ int teuk_b200_batch_launches_per_step(const teuk_b200_batch* b,
                                       int* launches) {
   return guarded([&] {
     require(b != nullptr && launches != nullptr, "null argument");
+    if (b->nodal) {
+      throw teuk_b200::Unsupported(
+          "a second-order batch steps through its nodal stage graph");
+    }
     *launches = 4 * static_cast<int>(b->batch->groups.size());
   });
 }
@@ -2757,6 +2856,11 @@ int teuk_b200_batch_stage_kernels(const teuk_b200_batch* b,
     require(b != nullptr && streaming_groups != nullptr &&
                 tile_groups != nullptr,
             "null argument");
+    if (b->nodal) {
+      *streaming_groups = 0;
+      *tile_groups = 0;
+      return;
+    }
     int streaming = 0;
     for (const teuk_b200::StageLaunch& g : b->batch->groups) {
       if (g.strips != nullptr && g.strip_count > 0) ++streaming;

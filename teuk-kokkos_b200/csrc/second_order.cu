@@ -2474,6 +2474,19 @@ void NodalPipeline::set_replica_state(const int k, const double* state,
   check(cudaStreamSynchronize(stream_), "set replica state");
 }
 
+void NodalPipeline::get_replica_state(const int k, double* state,
+                                      const int memory) {
+  if (k < 0 || k >= replicas_) throw std::invalid_argument("replica index out of range");
+  const size_t n = plan_.value_count();
+  check(cudaMemcpyAsync(state, buf_->state + static_cast<size_t>(k) * n,
+                        n * sizeof(double2),
+                        memory == TEUK_B200_HOST ? cudaMemcpyDeviceToHost
+                                                 : cudaMemcpyDeviceToDevice,
+                        stream_),
+        "get replica state");
+  check(cudaStreamSynchronize(stream_), "get replica state");
+}
+
 void NodalPipeline::copy_replica_from(const NodalPipeline& src, const int src_k,
                                       const int dst_k) {
   if (src_k < 0 || src_k >= src.replicas_ || dst_k < 0 || dst_k >= replicas_ ||

@@ -99,6 +99,7 @@ class NodalPipeline {
   void set_active_replicas(int k);
   // State of replica k (the plan's value_count() complex values).
   void set_replica_state(int k, const double* state, int memory);
+  void get_replica_state(int k, double* state, int memory);
   // Device copy of replica src_k of `src` (same plan) into replica dst_k.
   void copy_replica_from(const NodalPipeline& src, int src_k, int dst_k);
   ~NodalPipeline();
