@@ -2,9 +2,10 @@
 radial strips, against the reference build and against the tile kernel.
 
 The engine runs launch groups with n_ell <= 16 and at most 32 Gauss-Legendre
-nodes through the streaming kernel (persistent CTAs, bulk-copy ring);
-LaunchOptions(stage_kernel=KERNEL_TILE) makes a pipeline use the
-tile kernel instead.  Segments of one launch differ in n_ell (m = -4..4), so
+nodes through the streaming kernel (persistent CTAs, bulk-copy ring), and
+free-damped groups with n_ell <= 24 and at most 48 nodes through its wide
+form (8-row chunks, two transform groups); LaunchOptions(stage_kernel=
+KERNEL_TILE) makes a pipeline use the tile kernel instead.  Segments of one launch differ in n_ell (m = -4..4), so
 the ring also changes its row stride between strips.
 Tolerance: 1e-10 relative to the field's max norm against the reference;
 the two engine kernels agree to 1e-12 (they differ in summation order only).
@@ -40,6 +41,20 @@ LONG = {
     # D8-4 free-damped Schwarzschild without dissipation, odd nr
     "schw_d84_long": replace(CASES["schw_d84"], radial_points=331,
                              dissipation=0.0),
+    # wide kernel: D10-5 Kerr, ell <= 20 (n_ell 17..19 for m = -4..4)
+    "kerr_d105_wide": replace(CASES["kerr_d105"], radial_points=260,
+                              theta_nodes=31, ell_max_first=20,
+                              ell_max_second=20),
+    # wide kernel: near-extremal D8-4 Kerr, ell <= 24, 37 nodes
+    "kerr_d84_wide48": replace(CASES["kerr_d105"], discretization=tb.D84,
+                               spin=0.99, radial_points=240, theta_nodes=37,
+                               ell_max_first=24, ell_max_second=24,
+                               modes=(-2, -1, 0, 1, 2)),
+    # wide kernel: Schwarzschild D4-2 (pointwise psi_t), ell <= 22
+    "schw_d42_wide": replace(CASES["schw_d84"], discretization=tb.D42,
+                             radial_points=203, theta_nodes=34,
+                             ell_max_first=22, ell_max_second=22,
+                             dissipation=0.01),
 }
 
 
@@ -103,11 +118,16 @@ def test_mixed_batch_matches_solo(require_gpu):
                replace(base, radial_points=129, spin=0.3),
                replace(base, radial_points=777, spin=0.9, ell_max_first=12,
                        ell_max_second=12),
-               replace(base, radial_points=64, spin=0.0)]
+               replace(base, radial_points=64, spin=0.0),
+               # bands with n_ell 17..19 (wide kernel) and 37 nodes
+               replace(base, radial_points=301, spin=0.6, theta_nodes=31,
+                       ell_max_first=20, ell_max_second=20),
+               replace(base, radial_points=150, spin=0.95, theta_nodes=37,
+                       ell_max_first=24, ell_max_second=24, modes=(-2, 2))]
     pulses = [pulse_for(c, 31 + i) for i, c in enumerate(configs)]
     dts = [step_size(c, 0.1) for c in configs]
     batch = tb.Batch(configs)
-    assert batch.stage_kernels() == (1, 0)
+    assert batch.stage_kernels() == (2, 0)  # narrow and wide groups
     for i, p in enumerate(pulses):
         batch.initialize_gaussian(i, p)
     batch.step(dts, 5)
@@ -119,11 +139,13 @@ def test_mixed_batch_matches_solo(require_gpu):
 
 
 def test_solve_split_between_stage_kernels(require_gpu):
-    """ell <= 18 with m = -4..4: the m = +-2, +-1, 0 bands (n_ell >= 17) run
-    the tile kernel, the m = +-3, +-4 bands the streaming kernel, in the
-    same step; the result matches the reference."""
+    """Stage-constrained, ell <= 18 with m = -4..4: the m = +-2, +-1, 0 bands
+    (n_ell >= 17; the wide kernel is free-damped only) run the tile kernel,
+    the m = +-3, +-4 bands the streaming kernel, in the same step; the result
+    matches the reference."""
     config = replace(CASES["kerr_d105"], radial_points=220, theta_nodes=29,
-                     ell_max_first=18, ell_max_second=18)
+                     ell_max_first=18, ell_max_second=18,
+                     reduction=tb.STAGE_CONSTRAINED)
     batch = tb.Batch([config])
     assert batch.stage_kernels() == (1, 1)
     ref = RefPipeline(config)

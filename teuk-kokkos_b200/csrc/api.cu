@@ -238,6 +238,20 @@ constexpr int kTargetTileRows = 48;
 constexpr int kStageRowBlock = 2;  // rows per stage-kernel work item
 constexpr size_t kSmemBudget = 200 * 1024;
 
+// Stage kernel of a band: the narrow streaming kernel (n_ell <= 16, at most
+// 32 nodes), the wide one (n_ell <= 24, at most 48 nodes, free-damped) or
+// the tile kernel.
+constexpr int kKindNarrow = 0, kKindWide = 1, kKindTile = 2;
+int stage_kernel_kind(const InstanceDesc& in, const int n_ell,
+                      const bool tile_only) {
+  if (tile_only) return kKindTile;
+  if (n_ell <= kStreamMaxEll && in.ntheta <= kStreamMaxNodes) return kKindNarrow;
+  if (n_ell <= kWideMaxEll && in.ntheta <= kWideMaxNodes && in.reduction == 0) {
+    return kKindWide;
+  }
+  return kKindTile;
+}
+
 int slab_halo(const int disc, const int reduction) {
   const DiscInfo info = disc_info(disc);
   return reduction == 1 ? std::max(info.diss_order, 2 * info.interior_half)
@@ -276,6 +290,8 @@ struct Batch {
   DeviceArray<int> d_error;  // streaming-kernel wait timeouts
   DeviceArray<double> d_coef;  // Teukolsky row coefficients per solve row
   DeviceArray<double> d_nodes;  // 1 / C_T on the nodes per solve row
+  DeviceArray<double> d_nodes_wide;  // the same, kWideMaxNodes per row
+  int wide_rows = 0;  // rows of the wide node table
   int withhold_chunk_ = -1;    // failure-detection test hook
   teuk_b200_batch_options options{TEUK_B200_ABI_VERSION, TEUK_B200_KERNEL_AUTO,
                                   TEUK_B200_PRECISION_FP64, 0, 0};
@@ -436,14 +452,23 @@ struct Batch {
     // do not couple, so a solve may have segments in both.
     const bool tile_only = options.stage_kernel == TEUK_B200_KERNEL_TILE;
     withhold_chunk_ = g_test_withhold_chunk.load();
-    const auto streamable = [&](const size_t s) {
-      const InstanceDesc& in = h_inst[static_cast<size_t>(h_seg[s].instance)];
-      return !tile_only && h_seg[s].n_ell <= kStreamMaxEll &&
-             in.ntheta <= kStreamMaxNodes;
+    const auto kind_of = [&](const size_t s) {
+      return stage_kernel_kind(h_inst[static_cast<size_t>(h_seg[s].instance)],
+                               h_seg[s].n_ell, tile_only);
     };
+    // rows of the wide node table: solves with bands on the wide kernel
+    wide_rows = 0;
+    for (size_t i = 0; i < h_inst.size(); ++i) {
+      bool wide = false;
+      for (const int s : instance_segments[i]) {
+        wide = wide || kind_of(static_cast<size_t>(s)) == kKindWide;
+      }
+      h_inst[i].wide_row0 = wide ? wide_rows : -1;
+      if (wide) wide_rows += h_inst[i].nr;
+    }
     for (int disc = 0; disc < 3; ++disc) {
       for (int red = 0; red < 2; ++red) {
-       for (int kind = 0; kind < 2; ++kind) {  // 0 streaming, 1 tile
+       for (int kind = 0; kind < 3; ++kind) {  // narrow, wide, tile kernel
         StageLaunch g{};
         g.disc = disc;
         g.reduction = red;
@@ -454,7 +479,7 @@ struct Batch {
         for (size_t s = 0; s < h_seg.size(); ++s) {
           const InstanceDesc& in = h_inst[static_cast<size_t>(h_seg[s].instance)];
           if (in.disc != disc || in.reduction != red) continue;
-          if (streamable(s) != (kind == 0)) continue;
+          if (kind_of(s) != kind) continue;
           group_segments.push_back(static_cast<int>(s));
           const int ne = h_seg[s].n_ell;
           const int nr = in.nr;
@@ -482,13 +507,14 @@ struct Batch {
         }
         g.tile_count = static_cast<int>(h_tiles.size()) - first_tile;
         if (g.tile_count > 0) {
-          if (kind == 1 && stage_smem_bytes(g) > kSmemBudget) {
+          if (kind == kKindTile && stage_smem_bytes(g) > kSmemBudget) {
             throw std::invalid_argument(
                 "solve shape exceeds the stage kernel's shared-memory tile");
           }
           g.strips = nullptr;
           g.strip_count = 0;
-          if (kind == 0) {
+          g.wide = kind == kKindWide ? 1 : 0;
+          if (kind != kKindTile) {
             plan_strip_region(g, group_segments);
           } else {
             group_first_strip.push_back(-1);
@@ -543,6 +569,7 @@ struct Batch {
     alloc(d_error, 1);
     alloc(d_coef, static_cast<size_t>(std::max(coef_rows, 1)) * kCoefRecord);
     alloc(d_nodes, static_cast<size_t>(std::max(coef_rows, 1)) * kNodeRecord);
+    alloc(d_nodes_wide, static_cast<size_t>(std::max(wide_rows, 1)) * kWideMaxNodes);
     alloc(d_mat, std::max<size_t>(h_mat.size(), 1));
     alloc(d_split, std::max<size_t>(h_split.size(), 1));
     alloc(d_split_scale, std::max<size_t>(h_split_scale.size(), 1));
@@ -599,17 +626,27 @@ struct Batch {
     for (size_t i = 0; i < h_inst.size(); ++i) {
       check(launch_coefficient_table(d_inst.ptr + i, d_trig.ptr, h_inst[i].nr,
                                      h_inst[i].coef_row0, d_coef.ptr,
-                                     d_nodes.ptr, stream),
+                                     d_nodes.ptr, h_inst[i].coef_row0,
+                                     kNodeRecord, stream),
             "coefficient table");
+      if (h_inst[i].wide_row0 >= 0) {  // node rows only
+        check(launch_coefficient_table(d_inst.ptr + i, d_trig.ptr, h_inst[i].nr,
+                                       0, nullptr, d_nodes_wide.ptr,
+                                       h_inst[i].wide_row0, kWideMaxNodes,
+                                       stream),
+              "wide node table");
+      }
     }
     for (size_t gi = 0; gi < groups.size(); ++gi) {
       StageLaunch& g = groups[gi];
       g.tiles = d_tiles.ptr + group_first_tile[gi];
       g.error = d_error.ptr;
       g.coef_table = d_coef.ptr;
-      g.node_table = d_nodes.ptr;
+      g.node_table = g.wide ? d_nodes_wide.ptr : d_nodes.ptr;
       g.withhold_chunk = withhold_chunk_;
-      g.precision = options.precision == TEUK_B200_PRECISION_SPLIT ? 1 : 0;
+      // the wide kernel and the tile kernel transform in FP64
+      g.precision =
+          options.precision == TEUK_B200_PRECISION_SPLIT && !g.wide ? 1 : 0;
       g.split_frags = d_split.ptr;
       g.split_scales = d_split_scale.ptr;
       if (group_first_strip[gi] >= 0) {
@@ -747,7 +784,10 @@ struct Batch {
   // Reserves the strip region of a new streaming group and fills it with
   // the strips of the requested (or built-in) strip length.
   void plan_strip_region(StageLaunch& g, const std::vector<int>& segs) {
-    if (g.max_ell > kStreamMaxEll || g.max_theta > kStreamMaxNodes) {
+    const int max_ell = g.wide ? kWideMaxEll : kStreamMaxEll;
+    const int max_theta = g.wide ? kWideMaxNodes : kStreamMaxNodes;
+    if (g.max_ell > max_ell || g.max_theta > max_theta ||
+        (g.wide && g.reduction != 0)) {
       throw std::logic_error("segment outside the streaming kernel's shapes");
     }
     const int target = options.strip_rows > 0
@@ -780,15 +820,15 @@ struct Batch {
   // one RK4 step (the four stage launches) of the group for each candidate
   // strip length (64 to 4096 rows, up to the longest segment) and keeps the
   // fastest; the choice is cached for the
-  // process by (discretization, reduction, widest band, rows rounded to a
-  // quarter octave, SM count).  Strips only decide which CTA streams which
+  // process by (kernel, discretization, reduction, widest band, rows
+  // rounded to a quarter octave, SM count).  Strips only decide which CTA streams which
   // rows: every row gets the same sums in the same order for any choice,
   // so results are bit-identical across choices.  Runs at build, on the
   // zero state (every stage of a zero state is zero, and stages 2-4 read
   // only what the stages before them wrote).
   void autotune_strips() {
     static std::mutex cache_mutex;
-    static std::map<std::tuple<int, int, int, int, int>, int> cache;
+    static std::map<std::tuple<int, int, int, int, int, int>, int> cache;
     static const int kCandidates[] = {64,  96,  128,  192,  256,  384,
                                       512, 768, 1024, 1536, 2048, 4096};
     const int sms = device_sms();
@@ -803,7 +843,7 @@ struct Batch {
         max_nr = std::max(max_nr, h_inst[static_cast<size_t>(h_seg[static_cast<size_t>(s)].instance)].nr);
       }
       const auto key = std::make_tuple(
-          groups[gi].disc, groups[gi].reduction, groups[gi].max_ell,
+          groups[gi].wide, groups[gi].disc, groups[gi].reduction, groups[gi].max_ell,
           static_cast<int>(std::lround(4.0 * std::log2(static_cast<double>(rows)))),
           sms);
       int best = -1;
@@ -1511,9 +1551,21 @@ size_t linear_footprint(const teuk_b200::InstancePlan& plan) {
     complex_count += (count + 15) / 16 * 16;
     matrix += 2 * static_cast<size_t>(mp.n_ell * plan.config.ntheta);
   }
+  // bands on the wide streaming kernel add a row of the wide node table
+  bool wide = false;
+  const int nt = plan.config.ntheta;
+  for (const auto& mp : plan.modes) {
+    if (!mp.parent) continue;
+    const bool narrow =
+        mp.n_ell <= teuk_b200::kStreamMaxEll && nt <= teuk_b200::kStreamMaxNodes;
+    wide = wide || (!narrow && mp.n_ell <= teuk_b200::kWideMaxEll &&
+                    nt <= teuk_b200::kWideMaxNodes && plan.config.reduction == 0);
+  }
+  const size_t node_record =
+      teuk_b200::kNodeRecord + (wide ? teuk_b200::kWideMaxNodes : 0);
   return 4 * complex_count * sizeof(double2) + matrix * sizeof(double) +
          static_cast<size_t>(plan.config.nr) *
-             (teuk_b200::kCoefRecord + teuk_b200::kNodeRecord) * sizeof(double) +
+             (teuk_b200::kCoefRecord + node_record) * sizeof(double) +
          plan.value_count() * sizeof(double2);
 }
 

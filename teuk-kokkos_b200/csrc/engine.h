@@ -59,6 +59,7 @@ struct InstanceDesc {
   int reduction;    // 0 free damped, 1 stage constrained
   int disc;
   int coef_row0;    // first row of this solve in the coefficient table
+  int wide_row0;    // first row in the wide node table (-1: no wide bands)
 };
 
 struct SegmentDesc {

@@ -1040,9 +1040,50 @@ cudaError_t launch_stream_typed(const StageLaunch& p, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
+template <int DISC>
+cudaError_t launch_wide_typed(const StageLaunch& p, cudaStream_t stream) {
+  const size_t bytes = WideLayout().total;
+  auto kernel = stream_wide_kernel<DISC>;
+  static KernelSetups setups;
+  int sms = 0;
+  const cudaError_t setup_err = setups.with([&](KernelSetup& k, const int device) {
+    if (k.configured_bytes != static_cast<int>(bytes)) {
+      const cudaError_t err = cudaFuncSetAttribute(
+          kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+          static_cast<int>(bytes));
+      if (err != cudaSuccess) return err;
+      k.configured_bytes = static_cast<int>(bytes);
+    }
+    if (k.sms == 0) {
+      const cudaError_t err = cudaDeviceGetAttribute(
+          &k.sms, cudaDevAttrMultiProcessorCount, device);
+      if (err != cudaSuccess) return err;
+    }
+    // the setmaxnreg requests must fit the launch allocation
+    if (k.launch_regs < 0) {
+      cudaFuncAttributes attributes{};
+      const cudaError_t err = cudaFuncGetAttributes(&attributes, kernel);
+      if (err != cudaSuccess) return err;
+      k.launch_regs = attributes.numRegs;
+    }
+    if (k.launch_regs != kStreamLaunchRegs) return cudaErrorInvalidConfiguration;
+    sms = k.sms;
+    return cudaSuccess;
+  });
+  if (setup_err != cudaSuccess) return setup_err;
+  const int grid = p.strip_count < sms ? p.strip_count : sms;
+  kernel<<<grid, kStreamThreads, bytes, stream>>>(p);
+  return cudaGetLastError();
+}
+
 template <int DISC, int SC>
 cudaError_t launch_typed(const StageLaunch& p, cudaStream_t stream) {
   if (p.strips != nullptr && p.strip_count > 0) {
+    if (p.wide != 0) {
+      // free-damped FP64 only (the host never builds other wide groups)
+      if (SC != 0 || p.precision != 0) return cudaErrorInvalidValue;
+      return launch_wide_typed<DISC>(p, stream);
+    }
     return p.precision == 1 ? launch_stream_typed<DISC, SC, 1>(p, stream)
                             : launch_stream_typed<DISC, SC, 0>(p, stream);
   }
@@ -1200,16 +1241,21 @@ size_t stage_smem_bytes(const StageLaunch& p) {
 cudaError_t launch_coefficient_table(const InstanceDesc* instance_device,
                                      const double* trig, const int nr,
                                      const int row0, double* table,
-                                     double* node_table, cudaStream_t stream) {
+                                     double* node_table, const int node_row0,
+                                     const int node_record,
+                                     cudaStream_t stream) {
   if (nr <= 0) return cudaSuccess;
   coefficient_table_kernel<<<(nr + 127) / 128, 128, 0, stream>>>(
       instance_device, trig, nr,
-      table + static_cast<long long>(row0) * kCoefCount,
-      node_table + static_cast<long long>(row0) * kNodeRecord);
+      table != nullptr ? table + static_cast<long long>(row0) * kCoefCount
+                       : nullptr,
+      node_table + static_cast<long long>(node_row0) * node_record,
+      node_record);
   return cudaGetLastError();
 }
 
-size_t stream_smem_bytes(const int reduction) {
+size_t stream_smem_bytes(const int reduction, const bool wide) {
+  if (wide) return WideLayout().total;
   return StreamLayout(reduction == 1 ? 1 : 0).total;
 }
 

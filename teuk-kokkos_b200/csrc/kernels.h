@@ -63,6 +63,9 @@ struct StageLaunch {
   int precision;
   const uint4* split_frags;
   const double* split_scales;
+  // 1: the strips run the wide streaming kernel (WideGeom), whose node
+  // table rows have kWideMaxNodes doubles
+  int wide;
   // Failure-detection test hook (-1: off): in stage-1 launches the producer
   // of CTA 0 never issues this chunk, so the waits for it run out and the
   // launch reports a timeout through `error`.
@@ -73,23 +76,31 @@ struct StageLaunch {
 // most 32 Gauss-Legendre nodes per row in its solve.
 inline constexpr int kStreamMaxEll = 16;
 inline constexpr int kStreamMaxNodes = 32;
+// Wide streaming kernel eligibility: n_ell <= 24, at most 48 nodes, the
+// free-damped reduction and FP64 transforms.  Its node table has
+// kWideMaxNodes doubles per radial row.
+inline constexpr int kWideMaxEll = 24;
+inline constexpr int kWideMaxNodes = 48;
 
 inline constexpr int kSplitRecordUint4 = 4 * 5 * 32;
 inline constexpr int kSplitScaleDoubles = kStreamMaxNodes + kStreamMaxEll;
 inline constexpr int kCoefRecord = 10;
 inline constexpr int kNodeRecord = kStreamMaxNodes;
-// Fills the coefficient table rows of one solve, table[(row0 + r) * 10 + k],
-// and its node-inverse rows, node_table[(row0 + r) * kNodeRecord + j];
+// Fills the coefficient table rows of one solve, table[(row0 + r) * 10 + k]
+// (none when table is null), and its node-inverse rows,
+// node_table[(node_row0 + r) * node_record + j] (node_record: kNodeRecord,
+// or kWideMaxNodes for the wide table);
 // `trig` is the device trig pool the instance's trig_offset points into.
 cudaError_t launch_coefficient_table(const InstanceDesc* instance_device,
                                      const double* trig, int nr, int row0,
                                      double* table, double* node_table,
+                                     int node_row0, int node_record,
                                      cudaStream_t stream);
 inline constexpr int kStripMinRows = 64;
 // Radial strips per CTA the host aims for when it splits segments.
 inline constexpr int kStripsPerCta = 8;
-// Dynamic shared memory of the streaming kernel.
-size_t stream_smem_bytes(int reduction);
+// Dynamic shared memory of the streaming kernel (wide: its wide form).
+size_t stream_smem_bytes(int reduction, bool wide = false);
 
 // Dynamic shared memory bytes for one launch description.
 size_t stage_smem_bytes(const StageLaunch& launch);

@@ -77,6 +77,35 @@ constexpr int kSplitScales = kStreamMaxTheta + kStreamNep;
 constexpr int kStreamXs = 20;  // padded staging strides (bank-conflict free)
 constexpr int kStreamTs = 36;
 
+// Ring geometry of a streaming launch.  NarrowGeom: n_ell <= 16, at most 32
+// nodes, 16-row chunks in a 4-stage ring that also holds the RK
+// accumulator rows.  WideGeom: n_ell <= 24, at most 48 nodes (free-damped
+// reduction), the same chunks and stages; the RK update reads the
+// accumulator, and the transforms the 1 / C_T node values, straight from
+// global memory (three 24-lane rings of 64 rows do not fit in shared memory,
+// two do).
+struct NarrowGeom {
+  static constexpr int kNep = kStreamNep;        // ell lanes per row
+  static constexpr int kChunk = kStreamChunk;    // rows per copy
+  static constexpr int kStages = kStreamStages;  // ring stages
+  static constexpr int kRing = kStreamRing;      // ring rows
+  static constexpr int kPairs = kStreamSThreads / kStreamNep;  // row pairs
+  static constexpr int kNodeRec = kStreamMaxTheta;  // node-table record
+  static constexpr bool kRingA = true;  // accumulator rows in the ring
+};
+struct WideGeom {
+  static constexpr int kNep = 24;
+  static constexpr int kChunk = kStreamChunk;
+  static constexpr int kStages = kStreamStages;
+  static constexpr int kRing = kChunk * kStages;
+  static constexpr int kPairs = kStreamSThreads / kNep;  // 5 (8 threads idle)
+  static constexpr int kNodeRec = 48;
+  static constexpr bool kRingA = false;  // no accumulator or node-row ring
+};
+static_assert(2 * NarrowGeom::kPairs == NarrowGeom::kChunk, "narrow pass");
+static_assert(WideGeom::kNep == kWideMaxEll && WideGeom::kNodeRec == kWideMaxNodes,
+              "wide limits");
+
 __device__ __forceinline__ unsigned smem_u32(const void* ptr) {
   return static_cast<unsigned>(__cvta_generic_to_shared(ptr));
 }
@@ -175,12 +204,13 @@ __device__ bool stream_wait(unsigned long long* bar, const unsigned parity,
 struct StripGeom {
   long long seg_offset;  // complex offset of row 0 of the segment
   int segment, instance, m, ne, rs, nr, coef_row0;
+  int node_row0;  // first row of the solve in this geometry's node table
   int kerr;  // the transform reads 1 / C_T node rows
   int r0, r1;  // output rows
   int s0, s1;  // input rows (with halo)
   int t0, t1;  // psi_t / effective-Q rows
   int chunks;
-  int shift;  // ring row of absolute row q: (q + shift) & (kStreamRing - 1)
+  int shift;  // ring row of absolute row q: (q + shift) mod ring rows
 };
 
 // Loader state, kept in shared memory (only its one thread touches it).
@@ -231,7 +261,7 @@ struct StreamLayout {
   }
 };
 
-template <int H, int HD>
+template <int H, int HD, class G = NarrowGeom>
 __device__ __forceinline__ StripGeom strip_geom(const StageLaunch& p,
                                                 const int strip,
                                                 const int first_chunk) {
@@ -247,6 +277,7 @@ __device__ __forceinline__ StripGeom strip_geom(const StageLaunch& p,
   g.rs = 3 * seg.n_ell;
   g.nr = in.nr;
   g.coef_row0 = in.coef_row0;
+  g.node_row0 = G::kRingA ? in.coef_row0 : in.wide_row0;
   g.kerr = in.spin != 0.0 ? 1 : 0;
   g.r0 = t.r0;
   g.r1 = t.r1;
@@ -254,13 +285,37 @@ __device__ __forceinline__ StripGeom strip_geom(const StageLaunch& p,
   g.s1 = min(g.nr, t.r1 + H);
   g.t0 = max(0, t.r0 - HD);
   g.t1 = min(g.nr, t.r1 + HD);
-  g.chunks = (g.s1 - g.s0 + kStreamChunk - 1) / kStreamChunk;
-  g.shift = first_chunk * kStreamChunk - g.s0;
+  g.chunks = (g.s1 - g.s0 + G::kChunk - 1) / G::kChunk;
+  g.shift = first_chunk * G::kChunk - g.s0;
   return g;
 }
 
+template <class G = NarrowGeom>
 __device__ __forceinline__ int ring_row(const int q, const int shift) {
-  return (q + shift) & (kStreamRing - 1);
+  if constexpr ((G::kRing & (G::kRing - 1)) == 0) {
+    return (q + shift) & (G::kRing - 1);
+  } else {  // q + shift >= 0 for every row read
+    return static_cast<int>(static_cast<unsigned>(q + shift) %
+                            static_cast<unsigned>(G::kRing));
+  }
+}
+
+// Ring rows of the consecutive rows q0, q0 + 1, ..., q0 + N - 1 (N <= ring
+// rows): one modulo, then a wrap test per row.
+template <class G, int N>
+__device__ __forceinline__ void ring_rows(int (&rows)[N], const int q0,
+                                          const int shift) {
+  static_assert(N <= G::kRing, "window longer than the ring");
+  if constexpr ((G::kRing & (G::kRing - 1)) == 0) {
+#pragma unroll
+    for (int i = 0; i < N; ++i) rows[i] = ring_row<G>(q0 + i, shift);
+  } else {
+    const int b = ring_row<G>(q0, shift);
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      rows[i] = b + i < G::kRing ? b + i : b + i - G::kRing;
+    }
+  }
 }
 
 // First row that is not yet computable for a stencil of half width `half`
@@ -327,25 +382,28 @@ __device__ __forceinline__ double2 ring_dissipation(const Row& at, const int r,
 // the last K rows (r >= nr - BR) of the radial line, K = SPECIAL + P (the
 // widest closure stencil).  Two partial sums halve the dependency chain;
 // table entries beyond a row's stencil are zero.
-template <int DISC>
+template <int DISC, class G = NarrowGeom>
 __device__ __forceinline__ double2 edge_derivative(const double2* column,
                                                    const int r, const int nr,
                                                    const int shift,
                                                    const int stride) {
   using T = DiscTraits<DISC>;
   double2 a0 = make_double2(0.0, 0.0), a1 = a0;
+  int rows[T::W];  // ring rows of the first / last W rows of the line
   if (r < T::BR) {
+    ring_rows<G>(rows, 0, shift);
 #pragma unroll
     for (int c = 0; c < T::W; ++c) {
-      const double2 v = column[ring_row(c, shift) * stride];
+      const double2 v = column[rows[c] * stride];
       if (c & 1) a1 = cfma(c_sbp.left[DISC][r][c], v, a1);
       else a0 = cfma(c_sbp.left[DISC][r][c], v, a0);
     }
   } else {
     const int rr = nr - 1 - r;
+    ring_rows<G>(rows, nr - T::W, shift);
 #pragma unroll
     for (int c = 0; c < T::W; ++c) {
-      const double2 v = column[ring_row(nr - 1 - c, shift) * stride];
+      const double2 v = column[rows[T::W - 1 - c] * stride];  // row nr - 1 - c
       if (c & 1) a1 = cfma(-c_sbp.left[DISC][rr][c], v, a1);
       else a0 = cfma(-c_sbp.left[DISC][rr][c], v, a0);
     }
@@ -353,7 +411,7 @@ __device__ __forceinline__ double2 edge_derivative(const double2* column,
   return cadd(a0, a1);
 }
 
-template <int DISC>
+template <int DISC, class G = NarrowGeom>
 __device__ __forceinline__ double2 edge_dissipation(const double2* column,
                                                     const int r, const int nr,
                                                     const int shift,
@@ -363,9 +421,11 @@ __device__ __forceinline__ double2 edge_dissipation(const double2* column,
   double2 a0 = make_double2(0.0, 0.0), a1 = a0;
   const bool left = r < T::SPECIAL;
   const int rr = left ? r : nr - 1 - r;
+  int rows[K];  // ring rows of the first / last K rows of the line
+  ring_rows<G>(rows, left ? 0 : nr - K, shift);
 #pragma unroll
   for (int j = 0; j < K; ++j) {
-    const double2 v = column[ring_row(left ? j : nr - 1 - j, shift) * stride];
+    const double2 v = column[rows[left ? j : K - 1 - j] * stride];
     if (j & 1) a1 = cfma(c_sbp.diss_left[DISC][rr][j], v, a1);
     else a0 = cfma(c_sbp.diss_left[DISC][rr][j], v, a0);
   }
@@ -376,7 +436,7 @@ __device__ __forceinline__ double2 edge_dissipation(const double2* column,
 // Issues the bulk copies of the CTA's chunk sequence (strips blockIdx.x,
 // blockIdx.x + gridDim.x, ...; chunks of kStreamChunk rows each), one
 // chunk per free ring stage.  Run by one thread.
-template <int H, int HD>
+template <int H, int HD, class G = NarrowGeom>
 __device__ void loader_init(const StageLaunch& p, StreamLoaderState& L) {
   L.src_x = nullptr;
   L.src_a = nullptr;
@@ -390,18 +450,18 @@ __device__ void loader_init(const StageLaunch& p, StreamLoaderState& L) {
   L.c = 0;
   L.g = 0;
   L.prev_rs = -1;
-  if (L.strip < p.strip_count) L.sg = strip_geom<H, HD>(p, L.strip, 0);
+  if (L.strip < p.strip_count) L.sg = strip_geom<H, HD, G>(p, L.strip, 0);
 }
 
 // Load chunks while ring stages are free.  `released` = chunks handed back
 // so far.  A strip with another row stride starts only on an empty ring
 // (its rows would overlap the live stages' rows otherwise).
-template <int H, int HD>
+template <int H, int HD, class G = NarrowGeom>
 __device__ void loader_pump(const StageLaunch& p, StreamLoaderState& state,
                             unsigned long long* full, double2* U, double2* X,
                             double2* A, double* CF, double* NI,
                             const int released) {
-  if (state.strip >= p.strip_count || state.g >= released + kStreamStages) {
+  if (state.strip >= p.strip_count || state.g >= released + G::kStages) {
     return;
   }
   // Every reader of a released stage finished before the release was
@@ -409,39 +469,39 @@ __device__ void loader_pump(const StageLaunch& p, StreamLoaderState& state,
   __threadfence_block();
   fence_proxy_async_smem();
   StreamLoaderState L = state;
-  while (L.strip < p.strip_count && L.g < released + kStreamStages) {
+  while (L.strip < p.strip_count && L.g < released + G::kStages) {
     const StripGeom& sg = L.sg;
     if (L.c == 0 && L.prev_rs >= 0 && sg.rs != L.prev_rs && released < L.g) {
       break;
     }
-    const int s = L.g % kStreamStages;
-    const int a0 = sg.s0 + L.c * kStreamChunk;
-    const int a1 = min(sg.s1, a0 + kStreamChunk);
+    const int s = L.g % G::kStages;
+    const int a0 = sg.s0 + L.c * G::kChunk;
+    const int a1 = min(sg.s1, a0 + G::kChunk);
     const unsigned row_bytes = static_cast<unsigned>(sg.rs) * 16u;
     const unsigned bytes_u = static_cast<unsigned>(a1 - a0) * row_bytes;
     const unsigned bytes_x = L.src_x != nullptr ? bytes_u : 0u;
     const int o0 = max(a0, sg.r0), o1 = min(a1, sg.r1);
-    const unsigned bytes_a = (L.src_a != nullptr && o1 > o0)
+    const unsigned bytes_a = (G::kRingA && L.src_a != nullptr && o1 > o0)
                                  ? static_cast<unsigned>(o1 - o0) * row_bytes
                                  : 0u;
     const unsigned bytes_c =
         static_cast<unsigned>(a1 - a0) * kCoefCount * sizeof(double);
-    const unsigned bytes_n =
-        sg.kerr ? static_cast<unsigned>(a1 - a0) * kNodeRecord * sizeof(double)
-                : 0u;
+    const unsigned bytes_n = (G::kRingA && sg.kerr)
+        ? static_cast<unsigned>(a1 - a0) * G::kNodeRec * sizeof(double)
+        : 0u;
     const bool withheld = L.g == p.withhold_chunk && p.stage == kStage1 &&
                           blockIdx.x == 0;  // failure-detection test hook
     if (!withheld) {
       mbar_arrive_expect_tx(&full[s],
                             bytes_u + bytes_x + bytes_a + bytes_c + bytes_n);
       const long long gsrc = sg.seg_offset + static_cast<long long>(a0) * sg.rs;
-      const int ra0 = ring_row(a0, sg.shift);
+      const int ra0 = ring_row<G>(a0, sg.shift);
       bulk_copy_g2s(U + ra0 * sg.rs, L.src_u + gsrc, bytes_u, &full[s]);
       if (bytes_x != 0u) {
         bulk_copy_g2s(X + ra0 * sg.rs, L.src_x + gsrc, bytes_x, &full[s]);
       }
       if (bytes_a != 0u) {
-        bulk_copy_g2s(A + ring_row(o0, sg.shift) * sg.rs,
+        bulk_copy_g2s(A + ring_row<G>(o0, sg.shift) * sg.rs,
                       L.src_a + sg.seg_offset + static_cast<long long>(o0) * sg.rs,
                       bytes_a, &full[s]);
       }
@@ -450,9 +510,9 @@ __device__ void loader_pump(const StageLaunch& p, StreamLoaderState& state,
                         static_cast<long long>(sg.coef_row0 + a0) * kCoefCount,
                     bytes_c, &full[s]);
       if (bytes_n != 0u) {
-        bulk_copy_g2s(NI + ra0 * kNodeRecord,
-                      p.node_table + static_cast<long long>(sg.coef_row0 + a0) *
-                                         kNodeRecord,
+        bulk_copy_g2s(NI + ra0 * G::kNodeRec,
+                      p.node_table + static_cast<long long>(sg.node_row0 + a0) *
+                                         G::kNodeRec,
                       bytes_n, &full[s]);
       }
     }
@@ -461,20 +521,21 @@ __device__ void loader_pump(const StageLaunch& p, StreamLoaderState& state,
     if (++L.c == sg.chunks) {
       L.c = 0;
       L.strip += gridDim.x;
-      if (L.strip < p.strip_count) L.sg = strip_geom<H, HD>(p, L.strip, L.g);
+      if (L.strip < p.strip_count) L.sg = strip_geom<H, HD, G>(p, L.strip, L.g);
     }
   }
   state = L;
 }
 
 // After an abort: copies still in flight land before the CTA exits.
+template <class G = NarrowGeom>
 __device__ void loader_drain(const StreamLoaderState& L,
                              unsigned long long* full) {
-  for (int back = 1; back <= kStreamStages && L.g - back >= 0; ++back) {
+  for (int back = 1; back <= G::kStages && L.g - back >= 0; ++back) {
     const int gb = L.g - back;
     const unsigned long long t0 = global_ns();
-    while (!mbar_try_wait(&full[gb % kStreamStages],
-                          static_cast<unsigned>(gb / kStreamStages) & 1u)) {
+    while (!mbar_try_wait(&full[gb % G::kStages],
+                          static_cast<unsigned>(gb / G::kStages) & 1u)) {
       if (global_ns() - t0 > kStreamWaitNs) break;
     }
   }
@@ -912,10 +973,14 @@ __device__ void stream_transform(const StageLaunch& p,
 
 // ------------------------------------------------------------- stencils
 // RK update of field f of one row from the stage slope k (global stores).
+// (WideGeom: with `pre` the caller loaded this entry's accumulator value
+// `a_pre` ahead, else it is read from global memory here.)
+template <class G = NarrowGeom>
 __device__ __forceinline__ void stream_rk_update(
     const StageLaunch& p, const StripGeom& sg, const double2* X,
     const double2* A, const long long gi, const int ri, const double2 k,
-    const double dt, const double dt6) {
+    const double dt, const double dt6, const bool pre = false,
+    const double2 a_pre = make_double2(0.0, 0.0)) {
   switch (p.stage) {
     case kStage2:  // X = k1
       p.kB[gi] = k;
@@ -923,12 +988,13 @@ __device__ __forceinline__ void stream_rk_update(
       break;
     case kStage3: {  // X = y, A = k1 + 2 k2
       const double2 y0 = X[ri];
-      p.acc[gi] = cfma(dt6, cfma(2.0, k, A[ri]), y0);
+      const double2 a = G::kRingA ? A[ri] : (pre ? a_pre : p.acc[gi]);
+      p.acc[gi] = cfma(dt6, cfma(2.0, k, a), y0);
       p.kA[gi] = cfma(dt, k, y0);
       break;
     }
     case kStage4:  // A = y + dt/6 (k1 + 2 k2 + 2 k3)
-      p.y[gi] = cfma(dt6, k, A[ri]);
+      p.y[gi] = cfma(dt6, k, G::kRingA ? A[ri] : (pre ? a_pre : p.acc[gi]));
       break;
     default:  // stage 1 and the RHS-only evaluation
       p.kA[gi] = k;
@@ -971,7 +1037,7 @@ __device__ __forceinline__ double2 taps_derivative(const double2 (&w)[N],
 
 // Terms of interior rows r and r + 1: one window of 2P + 2 ring rows per
 // field serves both rows (12 of the 14 rows overlap for D10-5).
-template <int DISC, int SC>
+template <int DISC, int SC, class G = NarrowGeom>
 __device__ __forceinline__ void pair_terms(
     StencilTerms (&t)[2], const double2* cpsi, const double2* cQ,
     const double2* cP, const double2* cpt, const double2* cqe, const int r,
@@ -979,8 +1045,7 @@ __device__ __forceinline__ void pair_terms(
   using T = DiscTraits<DISC>;
   constexpr int P = T::P, HD = T::HALF, N = 2 * P + 2, M = 2 * HD + 2;
   int rows[N];
-#pragma unroll
-  for (int i = 0; i < N; ++i) rows[i] = ring_row(r - P + i, shift);
+  ring_rows<G>(rows, r - P, shift);
   {
     double2 w[N];
 #pragma unroll
@@ -1013,7 +1078,7 @@ __device__ __forceinline__ void pair_terms(
   {
     double2 w[M];
 #pragma unroll
-    for (int i = 0; i < M; ++i) w[i] = cpt[rows[P - HD + i] * kStreamNep];
+    for (int i = 0; i < M; ++i) w[i] = cpt[rows[P - HD + i] * G::kNep];
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       t[j].pt = w[HD + j];
@@ -1023,7 +1088,7 @@ __device__ __forceinline__ void pair_terms(
   if (SC) {
     double2 w[M];
 #pragma unroll
-    for (int i = 0; i < M; ++i) w[i] = cqe[rows[P - HD + i] * kStreamNep];
+    for (int i = 0; i < M; ++i) w[i] = cqe[rows[P - HD + i] * G::kNep];
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       t[j].qe = w[HD + j];
@@ -1035,7 +1100,7 @@ __device__ __forceinline__ void pair_terms(
 }
 
 // Terms of one interior row (the same sums as pair_terms gives it).
-template <int DISC, int SC>
+template <int DISC, int SC, class G = NarrowGeom>
 __device__ __forceinline__ void row_terms(
     StencilTerms& t, const double2* cpsi, const double2* cQ,
     const double2* cP, const double2* cpt, const double2* cqe, const int r,
@@ -1043,8 +1108,7 @@ __device__ __forceinline__ void row_terms(
   using T = DiscTraits<DISC>;
   constexpr int P = T::P, HD = T::HALF, N = 2 * P + 1, M = 2 * HD + 1;
   int rows[N];
-#pragma unroll
-  for (int i = 0; i < N; ++i) rows[i] = ring_row(r - P + i, shift);
+  ring_rows<G>(rows, r - P, shift);
   {
     double2 w[N];
 #pragma unroll
@@ -1070,14 +1134,14 @@ __device__ __forceinline__ void row_terms(
   {
     double2 w[M];
 #pragma unroll
-    for (int i = 0; i < M; ++i) w[i] = cpt[rows[P - HD + i] * kStreamNep];
+    for (int i = 0; i < M; ++i) w[i] = cpt[rows[P - HD + i] * G::kNep];
     t.pt = w[HD];
     t.dpt = taps_derivative<DISC>(w, HD);
   }
   if (SC) {
     double2 w[M];
 #pragma unroll
-    for (int i = 0; i < M; ++i) w[i] = cqe[rows[P - HD + i] * kStreamNep];
+    for (int i = 0; i < M; ++i) w[i] = cqe[rows[P - HD + i] * G::kNep];
     t.qe = w[HD];
     t.dq = taps_derivative<DISC>(w, HD);
   } else {
@@ -1111,7 +1175,7 @@ __device__ __forceinline__ void assemble_interior(
 
 // One thread per (output row pair, ell): all three fields of two adjacent
 // rows, no exchange.
-template <int DISC, int SC>
+template <int DISC, int SC, class G = NarrowGeom>
 __device__ void stream_stencil(const StageLaunch& p,
                                unsigned long long* ready,
                                volatile int* abort_flag,
@@ -1122,13 +1186,15 @@ __device__ void stream_stencil(const StageLaunch& p,
   using T = DiscTraits<DISC>;
   constexpr int P = T::P, HD = T::HALF;
   constexpr int H = SC ? (P > 2 * HD ? P : 2 * HD) : P;
-  const int pair = st / kStreamNep;  // row pair within a 16-row block
-  const int l = st % kStreamNep;
+  const int pair = st / G::kNep;  // row pair of a pass of 2 kPairs rows
+  const int l = st % G::kNep;
+  // threads beyond kPairs pairs (wide geometry) take no rows
+  const bool worker = G::kPairs * G::kNep == kStreamSThreads || pair < G::kPairs;
   int g = 0;
   int published = 0;  // chunks handed back so far
   for (int strip = blockIdx.x; strip < p.strip_count; strip += gridDim.x) {
     const int g0 = g;
-    const StripGeom sg = strip_geom<H, HD>(p, strip, g0);
+    const StripGeom sg = strip_geom<H, HD, G>(p, strip, g0);
     const InstanceDesc& in = p.instances[sg.instance];
     const int ne = sg.ne, nr = sg.nr, rs = sg.rs;
     const double inv_h = in.inv_spacing;
@@ -1148,12 +1214,12 @@ __device__ void stream_stencil(const StageLaunch& p,
     int out_done = sg.r0;
     int rel = g0;  // next chunk of this strip to hand back
     for (int c = 0; c < sg.chunks; ++c, ++g) {
-      const int s = g % kStreamStages;
+      const int s = g % G::kStages;
       const bool done =
-          stream_wait(&ready[s], static_cast<unsigned>(g / kStreamStages) & 1u,
+          stream_wait(&ready[s], static_cast<unsigned>(g / G::kStages) & 1u,
                       abort_flag, p.error, 4);
       if (!named_sync_and(2, kStreamSThreads, done)) return;
-      const int u_end = min(sg.s1, sg.s0 + (c + 1) * kStreamChunk);
+      const int u_end = min(sg.s1, sg.s0 + (c + 1) * G::kChunk);
       int lim = min(sg.r1, computable_end(u_end, nr, T::P, T::SPECIAL + T::P,
                                           T::SPECIAL));
       lim = min(lim, computable_end(u_end, nr, T::HALF, T::W, T::BR));
@@ -1167,68 +1233,96 @@ __device__ void stream_stencil(const StageLaunch& p,
         pe = min(sg.t1, u_end);
       }
       lim = min(lim, computable_end(pe, nr, T::HALF, T::W, T::BR));
-      for (int r = out_done + 2 * pair; r < lim; r += kStreamChunk) {
+      for (int r = out_done + 2 * pair; worker && r < lim;
+           r += 2 * G::kPairs) {
         if (l >= ne) continue;
         const int count = r + 1 < lim ? 2 : 1;  // rows r, r + 1 of this pass
-        auto update = [&](const int q, const double2 kP, const double2 kQ,
-                          const double2 kpsi) {
+        // RK update of row q (ring row rq) from its three slopes (pre: the
+        // row's accumulator values a0, a1, a2 were loaded ahead)
+        auto update_at = [&](const int q, const int rq, const double2 kP,
+                             const double2 kQ, const double2 kpsi,
+                             const bool pre = false,
+                             const double2 a0 = make_double2(0.0, 0.0),
+                             const double2 a1 = make_double2(0.0, 0.0),
+                             const double2 a2 = make_double2(0.0, 0.0)) {
           const long long gi =
               sg.seg_offset + static_cast<long long>(q) * rs + l;
-          const int ri = ring_row(q, sg.shift) * rs + l;
-          stream_rk_update(p, sg, X, A, gi, ri, kP, dt, dt6);
-          stream_rk_update(p, sg, X, A, gi + ne, ri + ne, kQ, dt, dt6);
-          stream_rk_update(p, sg, X, A, gi + 2 * ne, ri + 2 * ne, kpsi, dt,
-                           dt6);
+          const int ri = rq * rs + l;
+          stream_rk_update<G>(p, sg, X, A, gi, ri, kP, dt, dt6, pre, a0);
+          stream_rk_update<G>(p, sg, X, A, gi + ne, ri + ne, kQ, dt, dt6, pre,
+                              a1);
+          stream_rk_update<G>(p, sg, X, A, gi + 2 * ne, ri + 2 * ne, kpsi, dt,
+                              dt6, pre, a2);
+        };
+        auto update = [&](const int q, const double2 kP, const double2 kQ,
+                          const double2 kpsi) {
+          update_at(q, ring_row<G>(q, sg.shift), kP, kQ, kpsi);
         };
         if (count == 2 && r >= T::BR && r + 1 + T::BR < nr) {
           // two interior rows from one register window per field
+          double2 acc_pre[2][3];  // wide: the accumulator values, loaded ahead
+          const bool pre = !G::kRingA && (p.stage == kStage3 || p.stage == kStage4);
+          if constexpr (!G::kRingA) {
+            if (pre) {
+              const long long gi = sg.seg_offset + static_cast<long long>(r) * rs + l;
+#pragma unroll
+              for (int j = 0; j < 2; ++j) {
+#pragma unroll
+                for (int f = 0; f < 3; ++f) {
+                  acc_pre[j][f] = __ldcs(p.acc + gi + j * rs + f * ne);
+                }
+              }
+            }
+          }
           StencilTerms t[2];
-          pair_terms<DISC, SC>(t, cpsi, cQ, cP, cpt, cqe, r, sg.shift, rs);
+          pair_terms<DISC, SC, G>(t, cpsi, cQ, cP, cpt, cqe, r, sg.shift, rs);
+          int rq[2];  // ring rows of r, r + 1
+          ring_rows<G>(rq, r, sg.shift);
 #pragma unroll
           for (int j = 0; j < 2; ++j) {
             double2 kP, kQ, kpsi;
-            assemble_interior<SC>(t[j],
-                                  CF + ring_row(r + j, sg.shift) * kCoefCount,
-                                  mm, lambda, damping, inv_h, diss_scale,
-                                  dissipate, kP, kQ, kpsi);
-            update(r + j, kP, kQ, kpsi);
+            assemble_interior<SC>(t[j], CF + rq[j] * kCoefCount, mm, lambda,
+                                  damping, inv_h, diss_scale, dissipate, kP,
+                                  kQ, kpsi);
+            update_at(r + j, rq[j], kP, kQ, kpsi, pre, acc_pre[j][0],
+                      acc_pre[j][1], acc_pre[j][2]);
           }
           continue;
         }
 #pragma unroll 1
         for (int q = r; q < r + count; ++q) {
-          const int rr = ring_row(q, sg.shift);
+          const int rr = ring_row<G>(q, sg.shift);
           const double* cf = CF + rr * kCoefCount;
           double2 kP, kQ, kpsi;
           if (q >= T::BR && q + T::BR < nr) {
             StencilTerms t;
-            row_terms<DISC, SC>(t, cpsi, cQ, cP, cpt, cqe, q, sg.shift, rs);
+            row_terms<DISC, SC, G>(t, cpsi, cQ, cP, cpt, cqe, q, sg.shift, rs);
             assemble_interior<SC>(t, cf, mm, lambda, damping, inv_h,
                                   diss_scale, dissipate, kP, kQ, kpsi);
           } else {  // closure rows
             const double2 psi = cpsi[rr * rs];
             const double2 Q = cQ[rr * rs];
-            kQ = cadd(cscale(damping, cscale(inv_h, edge_derivative<DISC>(
+            kQ = cadd(cscale(damping, cscale(inv_h, edge_derivative<DISC, G>(
                                                         cpsi, q, nr, sg.shift, rs))),
-                      cscale(inv_h, edge_derivative<DISC>(cpt, q, nr, sg.shift,
-                                                          kStreamNep)));
+                      cscale(inv_h, edge_derivative<DISC, G>(cpt, q, nr, sg.shift,
+                                                             G::kNep)));
             kQ = csub(kQ, cscale(damping, Q));
-            kpsi = cpt[rr * kStreamNep];
+            kpsi = cpt[rr * G::kNep];
             kP = cadd(cmul(make_double2(cf[7], mm * cf[8]), psi),
                       cscale(lambda, psi));
-            const double2 qp = SC ? cqe[rr * kStreamNep] : Q;
+            const double2 qp = SC ? cqe[rr * G::kNep] : Q;
             const double2 dq =
-                SC ? edge_derivative<DISC>(cqe, q, nr, sg.shift, kStreamNep)
-                   : edge_derivative<DISC>(cQ, q, nr, sg.shift, rs);
+                SC ? edge_derivative<DISC, G>(cqe, q, nr, sg.shift, G::kNep)
+                   : edge_derivative<DISC, G>(cQ, q, nr, sg.shift, rs);
             kP = cadd(kP, cadd(cscale(cf[2], cscale(inv_h, dq)),
                                cmul(make_double2(cf[5], mm * cf[6]), qp)));
             if (dissipate) {
               kpsi = cfma(diss_scale,
-                          edge_dissipation<DISC>(cpsi, q, nr, sg.shift, rs), kpsi);
+                          edge_dissipation<DISC, G>(cpsi, q, nr, sg.shift, rs), kpsi);
               kQ = cfma(diss_scale,
-                        edge_dissipation<DISC>(cQ, q, nr, sg.shift, rs), kQ);
+                        edge_dissipation<DISC, G>(cQ, q, nr, sg.shift, rs), kQ);
               kP = cfma(diss_scale,
-                        edge_dissipation<DISC>(cP, q, nr, sg.shift, rs), kP);
+                        edge_dissipation<DISC, G>(cP, q, nr, sg.shift, rs), kP);
             }
           }
           update(q, kP, kQ, kpsi);
@@ -1245,7 +1339,7 @@ __device__ void stream_stencil(const StageLaunch& p,
         bound = min(out_done - H, nr - T::SPECIAL - T::P);
       }
       while (rel <= g &&
-             min(sg.s1, sg.s0 + (rel - g0 + 1) * kStreamChunk) <= bound) {
+             min(sg.s1, sg.s0 + (rel - g0 + 1) * G::kChunk) <= bound) {
         ++rel;
       }
       if (rel > published) {  // the same decision in every stencil thread
@@ -1270,17 +1364,17 @@ __device__ __forceinline__ void set_max_registers() {
 }
 
 // Producer: issues every chunk's copies as soon as its stage is free.
-template <int H, int HD>
+template <int H, int HD, class G = NarrowGeom>
 __device__ void stream_producer(const StageLaunch& p, StreamLoaderState& L,
                                 unsigned long long* full, double2* U,
                                 double2* X, double2* A, double* CF,
                                 double* NI, volatile int* released,
                                 volatile int* abort_flag) {
-  loader_init<H, HD>(p, L);
+  loader_init<H, HD, G>(p, L);
   unsigned long long t_last = global_ns();
   while (L.strip < p.strip_count) {
     const int before = L.g;
-    loader_pump<H, HD>(p, L, full, U, X, A, CF, NI, *released);
+    loader_pump<H, HD, G>(p, L, full, U, X, A, CF, NI, *released);
     if (L.g != before) {
       t_last = global_ns();
       continue;
@@ -1293,7 +1387,7 @@ __device__ void stream_producer(const StageLaunch& p, StreamLoaderState& L,
     }
     __nanosleep(128);
   }
-  if (*abort_flag != 0) loader_drain(L, full);
+  if (*abort_flag != 0) loader_drain<G>(L, full);
 }
 
 template <int DISC, int SC, int PREC>
@@ -1349,22 +1443,395 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
   }
 }
 
+// ------------------------------------------------------------- wide bands
+// The streaming kernel for bands of up to 24 ell and 48 nodes (free-damped
+// reduction, FP64 transforms).  Same roles, chunks and waits as above, with
+// the WideGeom ring (no accumulator or node-row ring): two transform warps
+// share each 4-row block (three node tiles of the synthesis each, from
+// fragments in registers; half of the analysis K steps each, from a
+// shared-memory copy of the band's analysis matrix, partial sums added
+// through `ex`); the stencil warps run the same stencil role with 24 ell
+// lanes (five row pairs per pass).
+constexpr int kWideXs = 36;  // staging strides of the wide transforms
+constexpr int kWideTs = 52;
+constexpr int kWideBlocks = kStreamBlocks;  // 4-row blocks per chunk
+// Register split as in the narrow kernel.
+constexpr int kWideTRegs = kStreamTRegs;
+constexpr int kWideSRegs = kStreamSRegs;
+constexpr int kWidePRegs = kStreamPRegs;
+static_assert(kWidePRegs * 128 + kWideTRegs * 256 + kWideSRegs * 128 <=
+                  kStreamThreads * kStreamLaunchRegs,
+              "wide register split");
+// Named barriers as in the narrow kernel.
+
+struct WideLayout {
+  size_t bars, loader, uring, xring, pring, coef, xw, tw, ex, amat, total;
+  __host__ __device__ WideLayout() {
+    size_t o = 0;
+    bars = o;
+    o += 128;  // 2 x 6 mbarriers, abort flag, released-chunk count
+    loader = o;
+    o += (sizeof(StreamLoaderState) + 127) / 128 * 128;
+    const size_t ring =
+        static_cast<size_t>(WideGeom::kRing) * 3 * WideGeom::kNep * 16;
+    uring = o;
+    o += ring;
+    xring = o;
+    o += ring;
+    pring = o;
+    o += static_cast<size_t>(WideGeom::kRing) * WideGeom::kNep * 16;
+    coef = o;
+    o += static_cast<size_t>(WideGeom::kRing) * kCoefCount * 8;
+    xw = o;
+    o += static_cast<size_t>(kWideBlocks) * 16 * kWideXs * 8;
+    tw = o;
+    o += static_cast<size_t>(kWideBlocks) * 8 * kWideTs * 8;
+    ex = o;  // per block: one warp's analysis sums, 3 tiles x 2 x 32 lanes
+    o += static_cast<size_t>(kWideBlocks) * 6 * 32 * 8;
+    amat = o;  // A(l, j) of the strip's band, [l][j]
+    o += static_cast<size_t>(WideGeom::kNep) * kWideTs * 8;
+    total = o;
+  }
+};
+static_assert(2 * WideGeom::kStages * 8 + 8 <= 128, "barrier area");
+static_assert(2 * static_cast<size_t>(WideGeom::kRing) * 3 * WideGeom::kNep * 16 +
+                      static_cast<size_t>(WideGeom::kRing) *
+                          (WideGeom::kNep * 16 + kCoefCount * 8) +
+                      static_cast<size_t>(kWideBlocks) *
+                          (16 * kWideXs + 8 * kWideTs + 6 * 32) * 8 +
+                      static_cast<size_t>(WideGeom::kNep) * kWideTs * 8 + 512 <=
+                  227 * 1024,
+              "wide shared memory");
+
+// Synthesis fragments of one wide transform warp (h = 0, 1 of its block):
+// node tiles h, h + 2, h + 4 over all 24 ell.  Its analysis covers all
+// three ell tiles over the K steps h, h + 2, ..., h + 10 (nodes 4 k ..
+// 4 k + 3), with the A operand read from the group's copy of A(l, j) in
+// shared memory.  Interleaving splits any node count evenly between the
+// two warps.
+struct PsiWideFragments {
+  double fs[3][6];  // S(j = (h + 2 i) * 8 + group, l = ks * 4 + quad)
+  double gcos[3];   // 2 s a cos(theta_j), j = (h + 2 i) * 8 + group
+};
+
+// psi_t of the 4-row block at q0 (rows >= qlim skipped), this warp's share;
+// the block's two warps synchronise on named barrier `bar`.
+__device__ __forceinline__ void stream_psi_wide(
+    const int q0, const int qlim, const int h, const StripGeom& sg,
+    const double2* U, const double* CF, const double* node_rows, double2* PS,
+    double* xw, double* tw, double* ex, const double* am,
+    const PsiWideFragments& F, const int mts, const int ksa, const int bar,
+    const int lane) {
+  using G = WideGeom;
+  const int quad = lane & 3;
+  const int group = lane >> 2;
+  const int ne = sg.ne;
+  const double mm = static_cast<double>(sg.m);
+  // stage the block's rows: v1 = P + 2K Q - G psi, psi (4 rows x 24 lanes
+  // over the block's 64 threads)
+  for (int it = h * 32 + lane; it < 4 * G::kNep; it += 64) {
+    const int rho = it / G::kNep;
+    const int l = it - rho * G::kNep;
+    const int r = q0 + rho;
+    double2 v1 = make_double2(0.0, 0.0), psi = make_double2(0.0, 0.0);
+    if (r < qlim && l < ne) {
+      const int rr = ring_row<G>(r, sg.shift);
+      const double* cf = CF + rr * kCoefCount;
+      const double2* row = U + rr * sg.rs;
+      const double2 Q = row[ne + l];
+      psi = row[2 * ne + l];
+      v1 = csub(cadd(row[l], cscale(2.0 * cf[1], Q)),
+                cmul(make_double2(cf[3], mm * cf[4]), psi));
+    }
+    xw[(rho * 4 + 0) * kWideXs + l] = v1.x;
+    xw[(rho * 4 + 1) * kWideXs + l] = v1.y;
+    xw[(rho * 4 + 2) * kWideXs + l] = psi.x;
+    xw[(rho * 4 + 3) * kWideXs + l] = psi.y;
+  }
+  named_sync(bar, 64);
+  {
+    double bx[2][6];
+#pragma unroll
+    for (int n = 0; n < 2; ++n) {
+#pragma unroll
+      for (int ks = 0; ks < 6; ++ks) {
+        bx[n][ks] = xw[(n * 8 + group) * kWideXs + ks * 4 + quad];
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const int mt = h + 2 * i;
+      if (mt < mts) {
+        double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+        for (int ks = 0; ks < 6; ++ks) {
+#pragma unroll
+          for (int n = 0; n < 2; ++n) {
+            dmma(acc[n][0], acc[n][1], F.fs[i][ks], bx[n][ks]);
+          }
+        }
+        const int j = mt * 8 + group;
+        double inv[2];  // 1 / C_T(r, theta_j); zero beyond the solve's nodes
+#pragma unroll
+        for (int n = 0; n < 2; ++n) {
+          const int r = q0 + 2 * n + (quad >> 1);
+          inv[n] = r < qlim ? __ldg(node_rows + static_cast<long long>(r) *
+                                                    G::kNodeRec + j)
+                            : 0.0;
+        }
+#pragma unroll
+        for (int n = 0; n < 2; ++n) {
+          // lane quad 0/2 holds a_j of a row, quad 1/3 holds b_j of that row
+          const double o0 = __shfl_xor_sync(0xffffffffu, acc[n][0], 1);
+          const double o1 = __shfl_xor_sync(0xffffffffu, acc[n][1], 1);
+          if ((quad & 1) == 0) {
+            const int rho = 2 * n + (quad >> 1);
+            tw[(rho * 2 + 0) * kWideTs + j] =
+                (acc[n][0] + F.gcos[i] * o1) * inv[n];
+            tw[(rho * 2 + 1) * kWideTs + j] =
+                (acc[n][1] - F.gcos[i] * o0) * inv[n];
+          }
+        }
+      }
+    }
+  }
+  named_sync(bar, 64);
+  double c[3][2][2];
+#pragma unroll
+  for (int t = 0; t < 3; ++t) {
+    c[t][0][0] = c[t][0][1] = c[t][1][0] = c[t][1][1] = 0.0;
+  }
+#pragma unroll
+  for (int ks = 0; ks < 6; ++ks) {
+    const int kg = 2 * ks + h;
+    if (kg < ksa) {
+      const double b = tw[group * kWideTs + kg * 4 + quad];
+#pragma unroll
+      for (int t = 0; t < 3; ++t) {
+        const double a = am[(t * 8 + group) * kWideTs + kg * 4 + quad];
+        dmma(c[t][ks & 1][0], c[t][ks & 1][1], a, b);
+      }
+    }
+  }
+  double sum[3][2];
+#pragma unroll
+  for (int t = 0; t < 3; ++t) {
+    sum[t][0] = c[t][0][0] + c[t][1][0];
+    sum[t][1] = c[t][0][1] + c[t][1][1];
+  }
+  if (h == 1) {
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+      ex[(t * 2 + 0) * 32 + lane] = sum[t][0];
+      ex[(t * 2 + 1) * 32 + lane] = sum[t][1];
+    }
+  }
+  named_sync(bar, 64);
+  if (h == 0) {  // even K steps (this warp) + odd K steps (the partner)
+    const int r = q0 + quad;
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+      const int l = t * 8 + group;
+      if (r < qlim && l < ne) {
+        PS[ring_row<G>(r, sg.shift) * G::kNep + l] =
+            make_double2(sum[t][0] + ex[(t * 2 + 0) * 32 + lane],
+                         sum[t][1] + ex[(t * 2 + 1) * 32 + lane]);
+      }
+    }
+  }
+}
+
+template <int DISC>
+__device__ void stream_transform_wide(const StageLaunch& p,
+                                      unsigned long long* full,
+                                      unsigned long long* ready,
+                                      volatile int* abort_flag, double2* U,
+                                      const double2* X, double2* PS,
+                                      const double* CF, double* xw_all,
+                                      double* tw_all, double* ex_all,
+                                      double* am, const int tt) {
+  using G = WideGeom;
+  using T = DiscTraits<DISC>;
+  constexpr int HD = T::HALF, H = T::P;
+  const int warp = tt >> 5, lane = tt & 31;
+  const int quad = lane & 3, group = lane >> 2;
+  const int blk = warp >> 1, h = warp & 1;
+  double* xw = xw_all + blk * 16 * kWideXs;
+  double* tw = tw_all + blk * 8 * kWideTs;
+  double* ex = ex_all + blk * 6 * 32;
+  // zero the nodal staging once (ordered by the first barrier below):
+  // columns beyond a solve's nodes stay zero
+  for (int i = tt; i < kWideBlocks * 8 * kWideTs; i += kStreamTThreads) {
+    tw_all[i] = 0.0;
+  }
+  int g = 0;
+  for (int strip = blockIdx.x; strip < p.strip_count; strip += gridDim.x) {
+    const StripGeom sg = strip_geom<H, HD, G>(p, strip, g);
+    const InstanceDesc& in = p.instances[sg.instance];
+    const int nt = in.ntheta, ne = sg.ne;
+    const bool kerr = in.spin != 0.0;
+    const double hdt = 0.5 * in.dt;
+    const double mm = static_cast<double>(sg.m);
+    const double* node_rows =
+        p.node_table + static_cast<long long>(sg.node_row0) * G::kNodeRec;
+    PsiWideFragments F;
+    const int mts = (nt + 7) / 8, ksa = (nt + 3) / 4;
+    if (kerr) {
+      const SegmentDesc& seg = p.segments[sg.segment];
+      const double* St = p.matrices + seg.mat_offset;  // St[l][j]
+      const double* At = St + ne * nt;                 // At[j][l]
+      const double sa2 = 2.0 * (static_cast<double>(kSpinWeight) * in.spin);
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const int j = (h + 2 * i) * 8 + group;
+#pragma unroll
+        for (int ks = 0; ks < 6; ++ks) {
+          const int l = ks * 4 + quad;
+          F.fs[i][ks] = (j < nt && l < ne) ? St[l * nt + j] : 0.0;
+        }
+        F.gcos[i] = j < nt ? sa2 * p.trig[in.trig_offset + nt + j] : 0.0;
+      }
+      // the shared copy of A(l, j): every block of the previous strip has
+      // finished reading the old one
+      named_sync(1, kStreamTThreads);
+      for (int i = tt; i < G::kNep * kWideTs; i += kStreamTThreads) {
+        const int l = i / kWideTs;
+        const int j = i - l * kWideTs;
+        am[i] = (j < nt && l < ne) ? At[j * ne + l] : 0.0;
+      }
+      named_sync(1, kStreamTThreads);
+    }
+    for (int c = 0; c < sg.chunks; ++c, ++g) {
+      const int s = g % G::kStages;
+      const unsigned parity = static_cast<unsigned>(g / G::kStages) & 1u;
+      const bool landed = stream_wait(&full[s], parity, abort_flag, p.error, 3);
+      if (!named_sync_and(1, kStreamTThreads, landed)) return;
+      const int a0 = sg.s0 + c * G::kChunk;
+      const int a1 = min(sg.s1, a0 + G::kChunk);
+      if (p.stage == kStage2 || p.stage == kStage3) {  // u = y + dt/2 k
+        const int base = ring_row<G>(a0, sg.shift) * sg.rs;
+        const int count = (a1 - a0) * sg.rs;  // rows never wrap in a chunk
+        double2* u = U + base;
+        const double2* x = X + base;
+        if (p.stage == kStage2) {  // U = y, X = k1
+          for (int i = tt; i < count; i += kStreamTThreads) {
+            u[i] = cfma(hdt, x[i], u[i]);
+          }
+        } else {  // U = k2, X = y
+          for (int i = tt; i < count; i += kStreamTThreads) {
+            u[i] = cfma(hdt, u[i], x[i]);
+          }
+        }
+        named_sync(1, kStreamTThreads);
+      }
+      // psi_t of the chunk's rows (free-damped: pointwise in r)
+      const int q_lo = max(a0, sg.t0), q_hi = min(a1, sg.t1);
+      if (q_hi > q_lo) {
+        if (kerr) {
+          for (int q = q_lo; q < q_hi; q += 4 * kWideBlocks) {
+            stream_psi_wide(q + 4 * blk, q_hi, h, sg, U, CF, node_rows, PS, xw,
+                            tw, ex, am, F, mts, ksa, kStreamBlockBar + blk,
+                            lane);
+          }
+        } else {
+          const int items = (q_hi - q_lo) * G::kNep;
+          for (int i = tt; i < items; i += kStreamTThreads) {
+            const int r = q_lo + i / G::kNep;
+            const int l = i % G::kNep;
+            if (l < ne) {
+              const int rr = ring_row<G>(r, sg.shift);
+              const double* cf = CF + rr * kCoefCount;
+              const double2* row = U + rr * sg.rs;
+              const double2 Q = row[ne + l];
+              const double2 psi = row[2 * ne + l];
+              const double2 num =
+                  csub(cadd(row[l], cscale(2.0 * cf[1], Q)),
+                       cmul(make_double2(cf[3], mm * cf[4]), psi));
+              PS[rr * G::kNep + l] = cscale(cf[9], num);
+            }
+          }
+        }
+      }
+      // the combine wrote ring rows that later bulk copies overwrite
+      fence_proxy_async_smem();
+      mbar_arrive(&ready[s]);
+    }
+  }
+}
+
+template <int DISC>
+__global__ void __launch_bounds__(kStreamThreads, 1)
+    stream_wide_kernel(const StageLaunch p) {
+  using G = WideGeom;
+  using T = DiscTraits<DISC>;
+  extern __shared__ __align__(128) unsigned char stream_smem[];
+  const WideLayout Ls;
+  unsigned long long* full =
+      reinterpret_cast<unsigned long long*>(stream_smem + Ls.bars);
+  unsigned long long* ready = full + G::kStages;
+  volatile int* abort_flag =
+      reinterpret_cast<volatile int*>(ready + G::kStages);
+  volatile int* released = abort_flag + 1;
+  StreamLoaderState& loader =
+      *reinterpret_cast<StreamLoaderState*>(stream_smem + Ls.loader);
+  double2* U = reinterpret_cast<double2*>(stream_smem + Ls.uring);
+  double2* X = reinterpret_cast<double2*>(stream_smem + Ls.xring);
+  double2* PS = reinterpret_cast<double2*>(stream_smem + Ls.pring);
+  double* CF = reinterpret_cast<double*>(stream_smem + Ls.coef);
+  double* xw = reinterpret_cast<double*>(stream_smem + Ls.xw);
+  double* tw = reinterpret_cast<double*>(stream_smem + Ls.tw);
+  double* ex = reinterpret_cast<double*>(stream_smem + Ls.ex);
+  double* am = reinterpret_cast<double*>(stream_smem + Ls.amat);
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < G::kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&ready[s], kStreamTThreads);
+    }
+    *abort_flag = 0;
+    *released = 0;
+    fence_mbarrier_init();
+  }
+  __syncthreads();
+  if (tid < kStreamTThreads) {
+    set_max_registers<kWideTRegs>();
+    stream_transform_wide<DISC>(p, full, ready, abort_flag, U, X, PS, CF, xw,
+                                tw, ex, am, tid);
+  } else if (tid < kStreamTThreads + kStreamSThreads) {
+    set_max_registers<kWideSRegs>();
+    // no accumulator ring (the RK update reads it from global memory) and
+    // no effective-Q ring (free-damped only)
+    stream_stencil<DISC, 0, G>(p, ready, abort_flag, released, U, X, nullptr,
+                               PS, PS, CF, tid - kStreamTThreads);
+  } else {
+    set_max_registers<kWidePRegs>();
+    if (tid == kStreamTThreads + kStreamSThreads) {
+      // no node rows to copy (the transforms read them from global memory)
+      stream_producer<T::P, T::HALF, G>(p, loader, full, U, X, nullptr, CF,
+                                        nullptr, released, abort_flag);
+    }
+  }
+}
+
 // Teukolsky row coefficients of one solve (m = 1 for entries 4, 6, 8) and
 // the inverse of C_T(r, theta_j) = C_T0(r) - a^2 sin^2(theta_j) on its
 // nodes (the diagonal of the implicit ell-coupling, A diag(1/C_T) S).
 __global__ void coefficient_table_kernel(const InstanceDesc* instance,
                                          const double* trig, const int nr,
-                                         double* out, double* node_out) {
+                                         double* out, double* node_out,
+                                         const int node_record) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= nr) return;
   const InstanceDesc in = *instance;
   double cf[kCoefCount];
   row_coefficients(in, 1, r, cf);
+  if (out != nullptr) {
 #pragma unroll
-  for (int k = 0; k < kCoefCount; ++k) out[r * kCoefCount + k] = cf[k];
+    for (int k = 0; k < kCoefCount; ++k) out[r * kCoefCount + k] = cf[k];
+  }
   const double a2 = in.spin * in.spin;
-  double* inv = node_out + static_cast<long long>(r) * kNodeRecord;
-  for (int j = 0; j < kNodeRecord; ++j) {
+  double* inv = node_out + static_cast<long long>(r) * node_record;
+  for (int j = 0; j < node_record; ++j) {
     double v = 0.0;
     if (j < in.ntheta) {
       const double s = trig[in.trig_offset + j];
