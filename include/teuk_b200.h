@@ -411,10 +411,11 @@ int teuk_b200_batch_synchronize(teuk_b200_batch* batch);
 /* Kernel launches issued per RK4 step (for launch accounting). */
 int teuk_b200_batch_launches_per_step(const teuk_b200_batch* batch,
                                       int* launches);
-/* Launch groups (one per discretization and reduction) whose stages run the
- * streaming kernel (persistent CTAs over radial strips; n_ell <= 16 and at
- * most 32 Gauss-Legendre nodes) and those that run the tile kernel.  No
- * counterpart in the reference: kernel selection of this engine. */
+/* Launch groups (per discretization, reduction and kernel) whose stages run
+ * a streaming kernel (persistent CTAs over radial strips: n_ell <= 16 and at
+ * most 32 Gauss-Legendre nodes, or, free-damped, n_ell <= 24 and at most 48
+ * nodes) and those that run the tile kernel.  No counterpart in the
+ * reference: kernel selection of this engine. */
 int teuk_b200_batch_stage_kernels(const teuk_b200_batch* batch,
                                   int* streaming_groups, int* tile_groups);
 
