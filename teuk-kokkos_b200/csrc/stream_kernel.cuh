@@ -1527,6 +1527,21 @@ __device__ __forceinline__ void stream_psi_wide(
   const int group = lane >> 2;
   const int ne = sg.ne;
   const double mm = static_cast<double>(sg.m);
+  // 1 / C_T(r, theta_j) of this lane's outputs of the synthesis, loaded
+  // first so the loads overlap the staging and the MMAs; zero beyond the
+  // solve's nodes and the block's rows
+  double inv[3][2];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll
+    for (int n = 0; n < 2; ++n) {
+      const int r = q0 + 2 * n + (quad >> 1);
+      const int j = (h + 2 * i) * 8 + group;
+      inv[i][n] = (h + 2 * i < mts && r < qlim)
+                      ? __ldg(node_rows + static_cast<long long>(r) * G::kNodeRec + j)
+                      : 0.0;
+    }
+  }
   // stage the block's rows: v1 = P + 2K Q - G psi, psi (4 rows x 24 lanes
   // over the block's 64 threads)
   for (int it = h * 32 + lane; it < 4 * G::kNep; it += 64) {
@@ -1571,14 +1586,6 @@ __device__ __forceinline__ void stream_psi_wide(
           }
         }
         const int j = mt * 8 + group;
-        double inv[2];  // 1 / C_T(r, theta_j); zero beyond the solve's nodes
-#pragma unroll
-        for (int n = 0; n < 2; ++n) {
-          const int r = q0 + 2 * n + (quad >> 1);
-          inv[n] = r < qlim ? __ldg(node_rows + static_cast<long long>(r) *
-                                                    G::kNodeRec + j)
-                            : 0.0;
-        }
 #pragma unroll
         for (int n = 0; n < 2; ++n) {
           // lane quad 0/2 holds a_j of a row, quad 1/3 holds b_j of that row
@@ -1587,9 +1594,9 @@ __device__ __forceinline__ void stream_psi_wide(
           if ((quad & 1) == 0) {
             const int rho = 2 * n + (quad >> 1);
             tw[(rho * 2 + 0) * kWideTs + j] =
-                (acc[n][0] + F.gcos[i] * o1) * inv[n];
+                (acc[n][0] + F.gcos[i] * o1) * inv[i][n];
             tw[(rho * 2 + 1) * kWideTs + j] =
-                (acc[n][1] - F.gcos[i] * o0) * inv[n];
+                (acc[n][1] - F.gcos[i] * o0) * inv[i][n];
           }
         }
       }
