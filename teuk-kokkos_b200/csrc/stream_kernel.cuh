@@ -80,10 +80,10 @@ constexpr int kStreamTs = 36;
 // Ring geometry of a streaming launch.  NarrowGeom: n_ell <= 16, at most 32
 // nodes, 16-row chunks in a 4-stage ring that also holds the RK
 // accumulator rows.  WideGeom: n_ell <= 24, at most 48 nodes (free-damped
-// reduction), the same chunks and stages; the RK update reads the
-// accumulator, and the transforms the 1 / C_T node values, straight from
-// global memory (three 24-lane rings of 64 rows do not fit in shared memory,
-// two do).
+// reduction), the same chunks and stages; three 24-lane rings of 64 rows do
+// not fit in shared memory, two do: stage 4 copies the accumulator rows
+// into the free X ring, stage 3's RK update reads them from global memory,
+// and the transforms read the 1 / C_T node values from global memory.
 struct NarrowGeom {
   static constexpr int kNep = kStreamNep;        // ell lanes per row
   static constexpr int kChunk = kStreamChunk;    // rows per copy
@@ -481,9 +481,12 @@ __device__ void loader_pump(const StageLaunch& p, StreamLoaderState& state,
     const unsigned bytes_u = static_cast<unsigned>(a1 - a0) * row_bytes;
     const unsigned bytes_x = L.src_x != nullptr ? bytes_u : 0u;
     const int o0 = max(a0, sg.r0), o1 = min(a1, sg.r1);
-    const unsigned bytes_a = (G::kRingA && L.src_a != nullptr && o1 > o0)
-                                 ? static_cast<unsigned>(o1 - o0) * row_bytes
-                                 : 0u;
+    // the accumulator rows of the outputs: into the A ring, or (WideGeom,
+    // stage 4, where the X ring is free) into the X ring
+    const bool a_rows =
+        L.src_a != nullptr && o1 > o0 && (G::kRingA || p.stage == kStage4);
+    const unsigned bytes_a =
+        a_rows ? static_cast<unsigned>(o1 - o0) * row_bytes : 0u;
     const unsigned bytes_c =
         static_cast<unsigned>(a1 - a0) * kCoefCount * sizeof(double);
     const unsigned bytes_n = (G::kRingA && sg.kerr)
@@ -501,7 +504,7 @@ __device__ void loader_pump(const StageLaunch& p, StreamLoaderState& state,
         bulk_copy_g2s(X + ra0 * sg.rs, L.src_x + gsrc, bytes_x, &full[s]);
       }
       if (bytes_a != 0u) {
-        bulk_copy_g2s(A + ring_row<G>(o0, sg.shift) * sg.rs,
+        bulk_copy_g2s((G::kRingA ? A : X) + ring_row<G>(o0, sg.shift) * sg.rs,
                       L.src_a + sg.seg_offset + static_cast<long long>(o0) * sg.rs,
                       bytes_a, &full[s]);
       }
@@ -993,8 +996,8 @@ __device__ __forceinline__ void stream_rk_update(
       p.kA[gi] = cfma(dt, k, y0);
       break;
     }
-    case kStage4:  // A = y + dt/6 (k1 + 2 k2 + 2 k3)
-      p.y[gi] = cfma(dt6, k, G::kRingA ? A[ri] : (pre ? a_pre : p.acc[gi]));
+    case kStage4:  // A (WideGeom: X) = y + dt/6 (k1 + 2 k2 + 2 k3)
+      p.y[gi] = cfma(dt6, k, G::kRingA ? A[ri] : X[ri]);
       break;
     default:  // stage 1 and the RHS-only evaluation
       p.kA[gi] = k;
@@ -1261,7 +1264,7 @@ __device__ void stream_stencil(const StageLaunch& p,
         if (count == 2 && r >= T::BR && r + 1 + T::BR < nr) {
           // two interior rows from one register window per field
           double2 acc_pre[2][3];  // wide: the accumulator values, loaded ahead
-          const bool pre = !G::kRingA && (p.stage == kStage3 || p.stage == kStage4);
+          const bool pre = !G::kRingA && p.stage == kStage3;
           if constexpr (!G::kRingA) {
             if (pre) {
               const long long gi = sg.seg_offset + static_cast<long long>(r) * rs + l;
