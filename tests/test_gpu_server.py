@@ -38,6 +38,15 @@ SECOND_ORDER = {
         normalized_constraint_tolerance=1e30, required_consecutive_passes=2),
 }
 
+# near-extremal linear solve with bands on the wide streaming kernel
+# (ell <= 24, 37 nodes)
+WIDE = {
+    "kerr_wide": tb.SolveConfig(
+        mass=1.0, spin=0.99, compactification_length=1.0, radial_points=160,
+        theta_nodes=37, ell_max_first=24, ell_max_second=24,
+        modes=(-2, -1, 0, 1, 2), dissipation=0.005, discretization=tb.D105),
+}
+
 # linear solves of different shapes, discretizations and reductions
 MIX = [
     ("kerr_d105", 7, 12),
@@ -47,6 +56,7 @@ MIX = [
     ("kerr_d105", 11, 5),
     ("so_unrestricted_d84", 12, 6),
     ("so_constraint_d42", 13, 4),
+    ("kerr_wide", 14, 7),
 ]
 
 
@@ -72,7 +82,10 @@ def test_second_order_requests_match_alone_exactly(require_gpu):
 
 
 def _config(name):
-    return CASES[name] if name in CASES else SECOND_ORDER[name]
+    for table in (CASES, SECOND_ORDER, WIDE):
+        if name in table:
+            return table[name]
+    raise KeyError(name)
 
 
 def _alone(config, pulse, dt, steps):

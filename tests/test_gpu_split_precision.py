@@ -153,6 +153,34 @@ def test_split_batch_member_equals_solo(require_gpu):
         assert np.array_equal(batch.get_state(i), solo.get_state()), i
 
 
+def test_split_batch_runs_wide_bands_in_fp64(require_gpu):
+    """Bands on the wide streaming kernel transform in FP64 in every
+    precision: in a split-precision batch, a solve whose bands are all wide
+    equals the same solve in an FP64 batch bit for bit, beside a narrow
+    split-precision solve."""
+    from cases import pulse_for, step_size
+    narrow = tb.SolveConfig(
+        mass=1.0, spin=0.7, compactification_length=1.0, radial_points=200,
+        theta_nodes=25, ell_max_first=16, ell_max_second=16,
+        modes=tuple(range(-4, 5)), dissipation=0.005, discretization=tb.D105)
+    wide = replace(narrow, radial_points=240, spin=0.95, theta_nodes=37,
+                   ell_max_first=24, ell_max_second=24, modes=(-2, 2))
+    configs = [narrow, wide]
+    pulses = [pulse_for(c, 41 + i) for i, c in enumerate(configs)]
+    dts = [step_size(c, 0.1) for c in configs]
+    states = []
+    for options in (SPLIT, None):
+        batch = tb.Batch(configs, options)
+        assert batch.stage_kernels() == (2, 0)  # narrow and wide groups
+        for i, p in enumerate(pulses):
+            batch.initialize_gaussian(i, p)
+        batch.step(dts, 6)
+        states.append([batch.get_state(i) for i in range(2)])
+    assert np.array_equal(states[0][1], states[1][1])
+    assert not np.array_equal(states[0][0], states[1][0])
+    assert relative_error(states[0][0][:, :3], states[1][0][:, :3]) < SPLIT_TOL
+
+
 def test_split_second_order_checkpoint_loads_into_the_reference(require_gpu, tmp_path):
     """Projections run the FP64 two-GEMM path in every precision, so a
     split-precision pipeline's state stays band limited to the reference's
