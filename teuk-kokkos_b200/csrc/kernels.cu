@@ -1000,10 +1000,10 @@ class KernelSetups {
 static_assert(kSplitRecord == kSplitRecordUint4, "split record size");
 static_assert(kSplitScales == kSplitScaleDoubles, "split scale count");
 
-template <int DISC, int SC, int PREC>
-cudaError_t launch_stream_typed(const StageLaunch& p, cudaStream_t stream) {
+template <int DISC, int SC, int PREC, int STAGE>
+cudaError_t launch_stream_stage(const StageLaunch& p, cudaStream_t stream) {
   const size_t bytes = StreamLayout(SC).total;
-  auto kernel = stream_stage_kernel<DISC, SC, PREC>;
+  auto kernel = stream_stage_kernel<DISC, SC, PREC, STAGE>;
   static KernelSetups setups;
   int sms = 0;
   const cudaError_t setup_err = setups.with([&](KernelSetup& k, const int device) {
@@ -1038,6 +1038,17 @@ cudaError_t launch_stream_typed(const StageLaunch& p, cudaStream_t stream) {
   const int grid = p.strip_count < sms ? p.strip_count : sms;
   kernel<<<grid, kStreamThreads, bytes, stream>>>(p);
   return cudaGetLastError();
+}
+
+template <int DISC, int SC, int PREC>
+cudaError_t launch_stream_typed(const StageLaunch& p, cudaStream_t stream) {
+  switch (p.stage) {
+    case kStage1: return launch_stream_stage<DISC, SC, PREC, kStage1>(p, stream);
+    case kStage2: return launch_stream_stage<DISC, SC, PREC, kStage2>(p, stream);
+    case kStage3: return launch_stream_stage<DISC, SC, PREC, kStage3>(p, stream);
+    case kStage4: return launch_stream_stage<DISC, SC, PREC, kStage4>(p, stream);
+    default: return launch_stream_stage<DISC, SC, PREC, kRhsOnly>(p, stream);
+  }
 }
 
 template <int DISC>

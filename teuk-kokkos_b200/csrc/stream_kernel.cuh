@@ -978,13 +978,14 @@ __device__ void stream_transform(const StageLaunch& p,
 // RK update of field f of one row from the stage slope k (global stores).
 // (WideGeom: with `pre` the caller loaded this entry's accumulator value
 // `a_pre` ahead, else it is read from global memory here.)
-template <class G = NarrowGeom>
+// (STAGE: the stage as a compile-time constant, 0: read p.stage)
+template <class G = NarrowGeom, int STAGE = 0>
 __device__ __forceinline__ void stream_rk_update(
     const StageLaunch& p, const StripGeom& sg, const double2* X,
     const double2* A, const long long gi, const int ri, const double2 k,
     const double dt, const double dt6, const bool pre = false,
     const double2 a_pre = make_double2(0.0, 0.0)) {
-  switch (p.stage) {
+  switch (STAGE != 0 ? STAGE : p.stage) {
     case kStage2:  // X = k1
       p.kB[gi] = k;
       p.acc[gi] = cfma(2.0, k, X[ri]);
@@ -1178,7 +1179,7 @@ __device__ __forceinline__ void assemble_interior(
 
 // One thread per (output row pair, ell): all three fields of two adjacent
 // rows, no exchange.
-template <int DISC, int SC, class G = NarrowGeom>
+template <int DISC, int SC, class G = NarrowGeom, int STAGE = 0>
 __device__ void stream_stencil(const StageLaunch& p,
                                unsigned long long* ready,
                                volatile int* abort_flag,
@@ -1251,11 +1252,12 @@ __device__ void stream_stencil(const StageLaunch& p,
           const long long gi =
               sg.seg_offset + static_cast<long long>(q) * rs + l;
           const int ri = rq * rs + l;
-          stream_rk_update<G>(p, sg, X, A, gi, ri, kP, dt, dt6, pre, a0);
-          stream_rk_update<G>(p, sg, X, A, gi + ne, ri + ne, kQ, dt, dt6, pre,
-                              a1);
-          stream_rk_update<G>(p, sg, X, A, gi + 2 * ne, ri + 2 * ne, kpsi, dt,
-                              dt6, pre, a2);
+          stream_rk_update<G, STAGE>(p, sg, X, A, gi, ri, kP, dt, dt6, pre,
+                                     a0);
+          stream_rk_update<G, STAGE>(p, sg, X, A, gi + ne, ri + ne, kQ, dt,
+                                     dt6, pre, a1);
+          stream_rk_update<G, STAGE>(p, sg, X, A, gi + 2 * ne, ri + 2 * ne,
+                                     kpsi, dt, dt6, pre, a2);
         };
         auto update = [&](const int q, const double2 kP, const double2 kQ,
                           const double2 kpsi) {
@@ -1393,7 +1395,8 @@ __device__ void stream_producer(const StageLaunch& p, StreamLoaderState& L,
   if (*abort_flag != 0) loader_drain<G>(L, full);
 }
 
-template <int DISC, int SC, int PREC>
+// STAGE: p.stage as a compile-time constant (the RK update's branch).
+template <int DISC, int SC, int PREC, int STAGE>
 __global__ void __launch_bounds__(kStreamThreads, 1)
     stream_stage_kernel(const StageLaunch p) {
   extern __shared__ __align__(128) unsigned char stream_smem[];
@@ -1435,8 +1438,9 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
                                      CF, NI, xw, tw, ex, tid);
   } else if (tid < kStreamTThreads + kStreamSThreads) {
     set_max_registers<kStreamSRegs>();
-    stream_stencil<DISC, SC>(p, ready, abort_flag, released, U, X, A, PS, QE,
-                             CF, tid - kStreamTThreads);
+    stream_stencil<DISC, SC, NarrowGeom, STAGE>(p, ready, abort_flag, released,
+                                                U, X, A, PS, QE, CF,
+                                                tid - kStreamTThreads);
   } else {
     set_max_registers<kStreamPRegs>();
     if (tid == kStreamTThreads + kStreamSThreads) {
