@@ -1051,10 +1051,10 @@ cudaError_t launch_stream_typed(const StageLaunch& p, cudaStream_t stream) {
   }
 }
 
-template <int DISC>
-cudaError_t launch_wide_typed(const StageLaunch& p, cudaStream_t stream) {
+template <int DISC, int STAGE>
+cudaError_t launch_wide_stage(const StageLaunch& p, cudaStream_t stream) {
   const size_t bytes = WideLayout().total;
-  auto kernel = stream_wide_kernel<DISC>;
+  auto kernel = stream_wide_kernel<DISC, STAGE>;
   static KernelSetups setups;
   int sms = 0;
   const cudaError_t setup_err = setups.with([&](KernelSetup& k, const int device) {
@@ -1085,6 +1085,17 @@ cudaError_t launch_wide_typed(const StageLaunch& p, cudaStream_t stream) {
   const int grid = p.strip_count < sms ? p.strip_count : sms;
   kernel<<<grid, kStreamThreads, bytes, stream>>>(p);
   return cudaGetLastError();
+}
+
+template <int DISC>
+cudaError_t launch_wide_typed(const StageLaunch& p, cudaStream_t stream) {
+  switch (p.stage) {
+    case kStage1: return launch_wide_stage<DISC, kStage1>(p, stream);
+    case kStage2: return launch_wide_stage<DISC, kStage2>(p, stream);
+    case kStage3: return launch_wide_stage<DISC, kStage3>(p, stream);
+    case kStage4: return launch_wide_stage<DISC, kStage4>(p, stream);
+    default: return launch_wide_stage<DISC, kRhsOnly>(p, stream);
+  }
 }
 
 template <int DISC, int SC>

@@ -812,7 +812,7 @@ __device__ __forceinline__ void stream_psi_split(
   }
 }
 
-template <int DISC, int SC, int PREC>
+template <int DISC, int SC, int PREC, int STAGE = 0>
 __device__ void stream_transform(const StageLaunch& p,
                                  unsigned long long* full,
                                  unsigned long long* ready,
@@ -898,12 +898,14 @@ __device__ void stream_transform(const StageLaunch& p,
       const int a0 = sg.s0 + c * kStreamChunk;
       const int a1 = min(sg.s1, a0 + kStreamChunk);
       // stage input u = y + dt/2 k, in place
-      if (p.stage == kStage2 || p.stage == kStage3) {
+      constexpr bool kFixed = STAGE != 0;
+      const int stage = kFixed ? STAGE : p.stage;
+      if (stage == kStage2 || stage == kStage3) {
         const int base = ring_row(a0, sg.shift) * sg.rs;
         const int count = (a1 - a0) * sg.rs;
         double2* u = U + base;
         const double2* x = X + base;
-        if (p.stage == kStage2) {  // U = y, X = k1
+        if (stage == kStage2) {  // U = y, X = k1
           for (int i = tt; i < count; i += kStreamTThreads) {
             u[i] = cfma(hdt, x[i], u[i]);
           }
@@ -1266,7 +1268,8 @@ __device__ void stream_stencil(const StageLaunch& p,
         if (count == 2 && r >= T::BR && r + 1 + T::BR < nr) {
           // two interior rows from one register window per field
           double2 acc_pre[2][3];  // wide: the accumulator values, loaded ahead
-          const bool pre = !G::kRingA && p.stage == kStage3;
+          const bool pre =
+              !G::kRingA && (STAGE != 0 ? STAGE : p.stage) == kStage3;
           if constexpr (!G::kRingA) {
             if (pre) {
               const long long gi = sg.seg_offset + static_cast<long long>(r) * rs + l;
@@ -1434,8 +1437,8 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
   constexpr int H = SC ? (T::P > 2 * T::HALF ? T::P : 2 * T::HALF) : T::P;
   if (tid < kStreamTThreads) {
     set_max_registers<kStreamTRegs>();
-    stream_transform<DISC, SC, PREC>(p, full, ready, abort_flag, U, X, PS, QE,
-                                     CF, NI, xw, tw, ex, tid);
+    stream_transform<DISC, SC, PREC, STAGE>(p, full, ready, abort_flag, U, X,
+                                            PS, QE, CF, NI, xw, tw, ex, tid);
   } else if (tid < kStreamTThreads + kStreamSThreads) {
     set_max_registers<kStreamSRegs>();
     stream_stencil<DISC, SC, NarrowGeom, STAGE>(p, ready, abort_flag, released,
@@ -1655,7 +1658,7 @@ __device__ __forceinline__ void stream_psi_wide(
   }
 }
 
-template <int DISC>
+template <int DISC, int STAGE = 0>
 __device__ void stream_transform_wide(const StageLaunch& p,
                                       unsigned long long* full,
                                       unsigned long long* ready,
@@ -1722,12 +1725,13 @@ __device__ void stream_transform_wide(const StageLaunch& p,
       if (!named_sync_and(1, kStreamTThreads, landed)) return;
       const int a0 = sg.s0 + c * G::kChunk;
       const int a1 = min(sg.s1, a0 + G::kChunk);
-      if (p.stage == kStage2 || p.stage == kStage3) {  // u = y + dt/2 k
+      const int stage = STAGE != 0 ? STAGE : p.stage;
+      if (stage == kStage2 || stage == kStage3) {  // u = y + dt/2 k
         const int base = ring_row<G>(a0, sg.shift) * sg.rs;
         const int count = (a1 - a0) * sg.rs;  // rows never wrap in a chunk
         double2* u = U + base;
         const double2* x = X + base;
-        if (p.stage == kStage2) {  // U = y, X = k1
+        if (stage == kStage2) {  // U = y, X = k1
           for (int i = tt; i < count; i += kStreamTThreads) {
             u[i] = cfma(hdt, x[i], u[i]);
           }
@@ -1773,7 +1777,8 @@ __device__ void stream_transform_wide(const StageLaunch& p,
   }
 }
 
-template <int DISC>
+// STAGE: p.stage as a compile-time constant.
+template <int DISC, int STAGE>
 __global__ void __launch_bounds__(kStreamThreads, 1)
     stream_wide_kernel(const StageLaunch p) {
   using G = WideGeom;
@@ -1809,14 +1814,14 @@ __global__ void __launch_bounds__(kStreamThreads, 1)
   __syncthreads();
   if (tid < kStreamTThreads) {
     set_max_registers<kWideTRegs>();
-    stream_transform_wide<DISC>(p, full, ready, abort_flag, U, X, PS, CF, xw,
-                                tw, ex, am, tid);
+    stream_transform_wide<DISC, STAGE>(p, full, ready, abort_flag, U, X, PS,
+                                       CF, xw, tw, ex, am, tid);
   } else if (tid < kStreamTThreads + kStreamSThreads) {
     set_max_registers<kWideSRegs>();
     // no accumulator ring (the RK update reads it from global memory) and
     // no effective-Q ring (free-damped only)
-    stream_stencil<DISC, 0, G>(p, ready, abort_flag, released, U, X, nullptr,
-                               PS, PS, CF, tid - kStreamTThreads);
+    stream_stencil<DISC, 0, G, STAGE>(p, ready, abort_flag, released, U, X,
+                                      nullptr, PS, PS, CF, tid - kStreamTThreads);
   } else {
     set_max_registers<kWidePRegs>();
     if (tid == kStreamTThreads + kStreamSThreads) {
