@@ -17,6 +17,7 @@
 // All arithmetic is binary64.
 #include <cstdio>
 #include <mutex>
+#include <type_traits>
 #include <unordered_map>
 
 #include "kernels.h"

@@ -1198,14 +1198,16 @@ __device__ void stream_stencil(const StageLaunch& p,
   const bool worker = G::kPairs * G::kNep == kStreamSThreads || pair < G::kPairs;
   int g = 0;
   int published = 0;  // chunks handed back so far
-  for (int strip = blockIdx.x; strip < p.strip_count; strip += gridDim.x) {
+  // one strip, with the dissipation switch a compile-time constant (false:
+  // the CTA is aborting)
+  auto run_strip = [&](const int strip, auto dissipation) -> bool {
+    constexpr bool dissipate = decltype(dissipation)::value;
     const int g0 = g;
     const StripGeom sg = strip_geom<H, HD, G>(p, strip, g0);
     const InstanceDesc& in = p.instances[sg.instance];
     const int ne = sg.ne, nr = sg.nr, rs = sg.rs;
     const double inv_h = in.inv_spacing;
     const double diss_scale = in.dissipation * inv_h;
-    const bool dissipate = in.dissipation > 0.0;
     const double damping = in.damping;
     const double dt = in.dt, dt6 = in.dt / 6.0;
     const double mm = static_cast<double>(sg.m);
@@ -1224,7 +1226,7 @@ __device__ void stream_stencil(const StageLaunch& p,
       const bool done =
           stream_wait(&ready[s], static_cast<unsigned>(g / G::kStages) & 1u,
                       abort_flag, p.error, 4);
-      if (!named_sync_and(2, kStreamSThreads, done)) return;
+      if (!named_sync_and(2, kStreamSThreads, done)) return false;
       const int u_end = min(sg.s1, sg.s0 + (c + 1) * G::kChunk);
       int lim = min(sg.r1, computable_end(u_end, nr, T::P, T::SPECIAL + T::P,
                                           T::SPECIAL));
@@ -1356,6 +1358,14 @@ __device__ void stream_stencil(const StageLaunch& p,
         published = rel;
       }
     }
+    return true;
+  };
+  for (int strip = blockIdx.x; strip < p.strip_count; strip += gridDim.x) {
+    const int instance = p.segments[p.strips[strip].segment].instance;
+    const bool ok = p.instances[instance].dissipation > 0.0
+                        ? run_strip(strip, std::true_type{})
+                        : run_strip(strip, std::false_type{});
+    if (!ok) return;
   }
 }
 
